@@ -1,0 +1,321 @@
+"""albedo_b200: a B200-native (sm_100a) path tracer with albedo's render API.
+
+The Python surface mirrors the reference's render entry points over the C ABI
+of include/albedo_b200.h:
+
+    read_scene / load_scene   readScene            (src/albedo/scene/scene_file.hpp:142-146)
+    Scene builder methods     Scene::add*, setSky  (src/albedo/scene/scene.hpp:31-62)
+    RenderJob                 RenderJob            (src/albedo/render/render_image.hpp:17-32)
+    PixelBuffer               PixelBuffer          (src/albedo/image/pixel_buffer.hpp:17-65)
+    render_image              renderImage          (src/albedo/render/render_image.hpp:36-49)
+    Scene.intersect/occluded  Scene::intersect / occluded (src/albedo/scene/scene.hpp:69-88)
+
+Errors raise the Python counterpart of the reference's exception: ValueError for
+std::invalid_argument, SceneParseError for SceneParseError, OSError for
+std::runtime_error (unreadable files), IndexError for std::out_of_range, and
+DeviceError for CUDA failures. There is no CPU fallback: without the built
+library, or without a CUDA device when one is needed, calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_double, c_float, c_int32, c_uint32, c_void_p
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from ._lib import Accumulator, BasicMaterialC, MaterialC, RenderJobC, SceneInfoC, library
+
+ACCUMULATOR_DTYPE = np.dtype([("r", "<f8"), ("g", "<f8"), ("b", "<f8"), ("count", "<i8")])
+
+PATH, SCATTER_ONLY, NORMALS = 0, 1, 2
+MEGAKERNEL, WAVEFRONT = 0, 1
+
+
+class SceneParseError(ValueError):
+    """A scene file the reader rejects; the message names the line."""
+
+
+class DeviceError(RuntimeError):
+    """A CUDA call failed, or a kernel reported an error."""
+
+
+class Unsupported(RuntimeError):
+    """The scene exceeds a limit of the device layout."""
+
+
+def _raise(status: int) -> None:
+    if status == 0:
+        return
+    message = library().albedo_last_error().decode("utf-8", "replace")
+    if status == 1:
+        raise ValueError(message)
+    if status == 2:
+        raise SceneParseError(message)
+    if status == 3:
+        raise OSError(message)
+    if status == 4:
+        raise IndexError(message)
+    if status == 6:
+        raise MemoryError(message)
+    if status == 7:
+        raise Unsupported(message)
+    raise DeviceError(message)
+
+
+def _d3(values) -> ctypes.Array:
+    return (c_double * 3)(*[float(v) for v in values])
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_float))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(POINTER(c_int32))
+
+
+@dataclass
+class BasicMaterial:
+    """BasicMaterial: kind "diffuse" (texture constant/checker/perlin), "conductor", "dielectric"."""
+
+    kind: str = "diffuse"
+    texture: str = "constant"
+    a: tuple = (0.0, 0.0, 0.0)  # color / even / low, or conductor eta
+    b: tuple = (0.0, 0.0, 0.0)  # odd / high, or conductor k
+    frequency_or_scale: float = 1.0
+    veins: float = 0.0
+    ior: float = 1.5
+    roughness: float = 0.0
+
+    def to_c(self) -> BasicMaterialC:
+        kinds = {"diffuse": 0, "conductor": 1, "dielectric": 2}
+        textures = {"constant": 0, "checker": 1, "perlin": 2}
+        c = BasicMaterialC()
+        c.kind = kinds[self.kind]
+        c.texture = textures[self.texture]
+        c.a = (c_double * 3)(*self.a)
+        c.b = (c_double * 3)(*self.b)
+        c.frequency_or_scale = self.frequency_or_scale
+        c.veins = self.veins
+        c.ior = self.ior
+        c.roughness = self.roughness
+        return c
+
+
+@dataclass
+class RenderJob:
+    """RenderJob without its camera and scene references; PathEstimator defaults."""
+
+    width: int
+    height: int
+    samples_per_axis: int = 1
+    seed: int = 0
+    estimator: int = PATH
+    max_depth: int = 64
+    roulette_start: int = 3
+    method: int = MEGAKERNEL
+
+    def to_c(self) -> RenderJobC:
+        return RenderJobC(self.width, self.height, self.samples_per_axis, self.estimator, self.seed, self.max_depth,
+                          self.roulette_start, self.method, 0)
+
+
+class PixelBuffer:
+    """Per-pixel FP64 sums and sample counts, accumulated in place like PixelBuffer."""
+
+    def __init__(self, width: int, height: int):
+        if width <= 0 or height <= 0 or width * height > (1 << 28):
+            raise ValueError(f"invalid image size {width}x{height}")
+        self.width = width
+        self.height = height
+        self.pixels = np.zeros(width * height, dtype=ACCUMULATOR_DTYPE)
+
+    def average(self) -> np.ndarray:
+        """(H, W, 3) means; black where a pixel has no samples."""
+        count = self.pixels["count"].astype(np.float64)
+        rgb = np.stack([self.pixels["r"], self.pixels["g"], self.pixels["b"]], axis=-1)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            avg = np.where(count[:, None] > 0, rgb / count[:, None], 0.0)
+        return avg.reshape(self.height, self.width, 3)
+
+
+class Scene:
+    """A scene built on the host and, once committed, resident on the device."""
+
+    def __init__(self, handle: int):
+        self._handle = c_void_p(handle)
+
+    @classmethod
+    def create(cls) -> "Scene":
+        handle = c_void_p()
+        _raise(library().albedo_scene_create(byref(handle)))
+        return cls(handle.value)
+
+    @classmethod
+    def read(cls, path) -> "Scene":
+        """Parses a scene file and builds it on the host only (no device)."""
+        handle = c_void_p()
+        _raise(library().albedo_scene_read(str(path).encode(), byref(handle)))
+        return cls(handle.value)
+
+    @classmethod
+    def load(cls, path) -> "Scene":
+        """readScene and upload to the current CUDA device."""
+        handle = c_void_p()
+        _raise(library().albedo_scene_load(str(path).encode(), byref(handle)))
+        return cls(handle.value)
+
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            library().albedo_scene_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> c_void_p:
+        return self._handle
+
+    # Scene building (mirrors Scene::add*, setSky and CameraSettings).
+    def set_camera(self, look_from, look_at, up=(0.0, 1.0, 0.0), fov=60.0) -> None:
+        _raise(library().albedo_scene_set_camera(self._handle, _d3(look_from), _d3(look_at), _d3(up), fov))
+
+    def add_material(self, first: BasicMaterial, second: BasicMaterial | None = None, scale: float = 1.0,
+                     veins: float = 0.0, threshold: float = 0.5) -> int:
+        m = MaterialC()
+        m.mix = 1 if second is not None else 0
+        m.first = first.to_c()
+        m.second = (second or first).to_c()
+        m.scale, m.veins, m.threshold = scale, veins, threshold
+        out = c_uint32()
+        _raise(library().albedo_scene_add_material(self._handle, byref(m), byref(out)))
+        return out.value
+
+    def add_sphere(self, center, radius: float, material: int) -> int:
+        out = c_uint32()
+        _raise(library().albedo_scene_add_sphere(self._handle, _d3(center), radius, material, byref(out)))
+        return out.value
+
+    def add_area_light(self, center, radius: float, radiance, material: int) -> int:
+        out = c_uint32()
+        _raise(library().albedo_scene_add_area_light(self._handle, _d3(center), radius, _d3(radiance), material,
+                                                     byref(out)))
+        return out.value
+
+    def add_point_light(self, position, intensity) -> None:
+        _raise(library().albedo_scene_add_point_light(self._handle, _d3(position), _d3(intensity)))
+
+    def set_sky(self, nadir, zenith=None) -> None:
+        _raise(library().albedo_scene_set_sky(self._handle, _d3(nadir), _d3(zenith if zenith is not None else nadir)))
+
+    def add_mesh(self, positions, faces, uvs=None, texture_faces=None, smooth=False) -> int:
+        p = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        f = np.ascontiguousarray(faces, dtype=np.uint32).reshape(-1, 3)
+        uv = np.ascontiguousarray(uvs if uvs is not None else np.zeros((0, 2)), dtype=np.float64).reshape(-1, 2)
+        tf = np.ascontiguousarray(texture_faces if texture_faces is not None else np.zeros((0, 3)),
+                                  dtype=np.uint32).reshape(-1, 3)
+        out = c_uint32()
+        _raise(library().albedo_scene_add_mesh(
+            self._handle, p.ctypes.data_as(POINTER(c_double)), len(p), f.ctypes.data_as(POINTER(c_uint32)), len(f),
+            uv.ctypes.data_as(POINTER(c_double)), len(uv), tf.ctypes.data_as(POINTER(c_uint32)), len(tf),
+            1 if smooth else 0, byref(out)))
+        return out.value
+
+    def add_instance(self, mesh: int, to_world, to_object, material: int) -> int:
+        w = (c_double * 12)(*np.asarray(to_world, dtype=np.float64).reshape(12))
+        o = (c_double * 12)(*np.asarray(to_object, dtype=np.float64).reshape(12))
+        out = c_uint32()
+        _raise(library().albedo_scene_add_instance(self._handle, mesh, w, o, material, byref(out)))
+        return out.value
+
+    def add_triangles(self, positions, faces, material: int) -> None:
+        p = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        f = np.ascontiguousarray(faces, dtype=np.uint32).reshape(-1, 3)
+        _raise(library().albedo_scene_add_triangles(self._handle, p.ctypes.data_as(POINTER(c_double)), len(p),
+                                                    f.ctypes.data_as(POINTER(c_uint32)), len(f), material))
+
+    def prepare(self) -> None:
+        _raise(library().albedo_scene_prepare(self._handle))
+
+    def commit(self) -> None:
+        _raise(library().albedo_scene_commit(self._handle))
+
+    def info(self) -> dict:
+        info = SceneInfoC()
+        _raise(library().albedo_scene_get_info(self._handle, byref(info)))
+        return {name: getattr(info, name) for name, _ in SceneInfoC._fields_}
+
+    # Ray queries.
+    def intersect(self, rays: np.ndarray, t_min: float = 0.0, t_max: float = float("inf"), geometry: bool = False):
+        """Closest hits of (N, 6) float32 rays: dict of hit, t, object, triangle [, point, normal, ...]."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        n = len(rays)
+        out = {"hit": np.zeros(n, np.int32), "t": np.zeros(n, np.float32), "object": np.full(n, -1, np.int32),
+               "triangle": np.full(n, -1, np.int32)}
+        extra = {}
+        if geometry:
+            extra = {"point": np.zeros((n, 3), np.float32), "normal": np.zeros((n, 3), np.float32),
+                     "shading_normal": np.zeros((n, 3), np.float32), "front": np.zeros(n, np.int32)}
+        _raise(library().albedo_trace_host(
+            self._handle, _fptr(rays), n, t_min, t_max, _iptr(out["hit"]), _fptr(out["t"]), _iptr(out["object"]),
+            _iptr(out["triangle"]), _fptr(extra["point"]) if geometry else None,
+            _fptr(extra["normal"]) if geometry else None, _fptr(extra["shading_normal"]) if geometry else None,
+            _iptr(extra["front"]) if geometry else None))
+        out.update(extra)
+        return out
+
+    def occluded(self, rays: np.ndarray, t_max: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+        t_max = np.ascontiguousarray(t_max, dtype=np.float32).reshape(-1)
+        out = np.zeros(len(rays), np.int32)
+        _raise(library().albedo_occluded_host(self._handle, _fptr(rays), _fptr(t_max), len(rays), _iptr(out)))
+        return out
+
+    def check(self) -> None:
+        """Collects a kernel-reported error after asynchronous renders."""
+        _raise(library().albedo_scene_check(self._handle))
+
+
+def read_scene(path) -> Scene:
+    """readScene(path), resident on the current CUDA device."""
+    return Scene.load(path)
+
+
+def render_image(scene: Scene, job: RenderJob, image: PixelBuffer) -> None:
+    """renderImage: adds samples_per_axis^2 samples to every pixel of `image`."""
+    if (image.width, image.height) != (job.width, job.height):
+        raise ValueError("image size does not match the job")
+    c = job.to_c()
+    _raise(library().albedo_render_host(scene.handle, byref(c), image.pixels.ctypes.data_as(c_void_p)))
+
+
+def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: int = 0) -> None:
+    """Stream-ordered render into a device array of width*height accumulators."""
+    c = job.to_c()
+    _raise(library().albedo_render(scene.handle, byref(c), c_void_p(accumulators_ptr), c_void_p(stream)))
+
+
+def render_pixels(scene: Scene, job: RenderJob, pixels: np.ndarray, with_squares: bool = False):
+    """Renders only the listed (x, y) pixels; returns accumulators (and sums of squares)."""
+    pixels = np.ascontiguousarray(pixels, dtype=np.int32).reshape(-1, 2)
+    acc = np.zeros(len(pixels), dtype=ACCUMULATOR_DTYPE)
+    squares = np.zeros((len(pixels), 3), np.float64) if with_squares else None
+    c = job.to_c()
+    _raise(library().albedo_render_pixels_host(
+        scene.handle, byref(c), _iptr(pixels), len(pixels), acc.ctypes.data_as(c_void_p),
+        squares.ctypes.data_as(POINTER(c_double)) if with_squares else None))
+    return (acc, squares) if with_squares else acc
+
+
+__all__ = [
+    "ACCUMULATOR_DTYPE", "BasicMaterial", "DeviceError", "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer",
+    "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError", "Unsupported", "WAVEFRONT", "read_scene",
+    "render_device", "render_image", "render_pixels", "Accumulator",
+]

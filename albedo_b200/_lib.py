@@ -1,0 +1,92 @@
+"""Loads libalbedo_b200.so (built in-tree) and declares the C ABI of include/albedo_b200.h."""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libalbedo_b200.so"
+
+
+class Accumulator(ctypes.Structure):
+    _fields_ = [("r", c_double), ("g", c_double), ("b", c_double), ("count", c_int64)]
+
+
+class RenderJobC(ctypes.Structure):
+    _fields_ = [("width", c_int32), ("height", c_int32), ("samples_per_axis", c_int32), ("estimator", c_int32),
+                ("seed", c_uint64), ("max_depth", c_int32), ("roulette_start", c_int32), ("method", c_int32),
+                ("reserved", c_int32)]
+
+
+class BasicMaterialC(ctypes.Structure):
+    _fields_ = [("kind", c_int32), ("texture", c_int32), ("a", c_double * 3), ("b", c_double * 3),
+                ("frequency_or_scale", c_double), ("veins", c_double), ("ior", c_double), ("roughness", c_double)]
+
+
+class MaterialC(ctypes.Structure):
+    _fields_ = [("mix", c_int32), ("reserved", c_int32), ("first", BasicMaterialC), ("second", BasicMaterialC),
+                ("scale", c_double), ("veins", c_double), ("threshold", c_double)]
+
+
+class SceneInfoC(ctypes.Structure):
+    _fields_ = [("objects", c_int64), ("lights", c_int64), ("triangles", c_int64), ("nodes", c_int64),
+                ("device_bytes", c_int64), ("stack_need", c_int32), ("stack_capacity", c_int32)]
+
+
+_D3 = POINTER(c_double)
+_F = POINTER(c_float)
+_I = POINTER(c_int32)
+_U = POINTER(c_uint32)
+
+# name -> (restype, argtypes); every symbol include/albedo_b200.h declares.
+PROTOTYPES: dict[str, tuple] = {
+    "albedo_last_error": (c_char_p, []),
+    "albedo_scene_load": (c_int32, [c_char_p, POINTER(c_void_p)]),
+    "albedo_scene_read": (c_int32, [c_char_p, POINTER(c_void_p)]),
+    "albedo_scene_create": (c_int32, [POINTER(c_void_p)]),
+    "albedo_scene_destroy": (None, [c_void_p]),
+    "albedo_scene_set_camera": (c_int32, [c_void_p, _D3, _D3, _D3, c_double]),
+    "albedo_scene_add_material": (c_int32, [c_void_p, POINTER(MaterialC), _U]),
+    "albedo_scene_add_sphere": (c_int32, [c_void_p, _D3, c_double, c_uint32, _U]),
+    "albedo_scene_add_area_light": (c_int32, [c_void_p, _D3, c_double, _D3, c_uint32, _U]),
+    "albedo_scene_add_point_light": (c_int32, [c_void_p, _D3, _D3]),
+    "albedo_scene_set_sky": (c_int32, [c_void_p, _D3, _D3]),
+    "albedo_scene_add_mesh": (c_int32, [c_void_p, _D3, c_int64, _U, c_int64, _D3, c_int64, _U, c_int64, c_int32, _U]),
+    "albedo_scene_add_instance": (c_int32, [c_void_p, c_uint32, _D3, _D3, c_uint32, _U]),
+    "albedo_scene_add_triangles": (c_int32, [c_void_p, _D3, c_int64, _U, c_int64, c_uint32]),
+    "albedo_scene_prepare": (c_int32, [c_void_p]),
+    "albedo_scene_commit": (c_int32, [c_void_p]),
+    "albedo_scene_host_view": (c_void_p, [c_void_p]),
+    "albedo_scene_get_info": (c_int32, [c_void_p, POINTER(SceneInfoC)]),
+    "albedo_render": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
+    "albedo_render_host": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p]),
+    "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
+    "albedo_scene_check": (c_int32, [c_void_p]),
+    "albedo_trace_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, _I, _F, _I, _I, _F, _F, _F, _I]),
+    "albedo_occluded_host": (c_int32, [c_void_p, _F, _F, c_int64, _I]),
+    "albedo_probe_pixel_stream": (c_int32, [c_uint64, c_int32, c_int32, c_int32, c_int32, _U, _F]),
+    "albedo_probe_lobe_eval": (c_int32, [c_int32, _F, _F, c_int32, _F, _F]),
+    "albedo_probe_lobe_sample": (c_int32, [c_int32, _F, _F, c_int32, _I, _F, _F, _F, _I]),
+    "albedo_probe_perlin": (c_int32, [_F, c_int32, _F, _F]),
+    "albedo_probe_camera_rays": (c_int32, [c_void_p, c_int32, c_int32, _F, c_int32, _F]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def library() -> ctypes.CDLL:
+    """The loaded library; raises if it has not been built (no fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY_PATH.exists():
+            raise RuntimeError(
+                f"{LIBRARY_PATH} is missing: build it with `python albedo_b200/build.py` "
+                "(the CUDA path is the only implementation)")
+        lib = ctypes.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib

@@ -1,0 +1,734 @@
+// The C ABI (include/albedo_b200.h): scene building and upload, renders and ray
+// queries. Exceptions from the host scene code become status codes with a
+// thread-local message; CUDA errors become ALBEDO_DEVICE_ERROR.
+#include "../../include/albedo_b200.h"
+
+#include "host/flatten.hpp"
+#include "host/scene_file.hpp"
+#include "kernels/launch.hpp"
+
+#include <cuda_runtime_api.h>
+
+#include <cstring>
+#include <format>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace albedo_b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+class DeviceError : public std::runtime_error {
+public:
+    explicit DeviceError(const std::string& what) : std::runtime_error{what} {}
+};
+class Unsupported : public std::runtime_error {
+public:
+    explicit Unsupported(const std::string& what) : std::runtime_error{what} {}
+};
+class TraversalError : public std::runtime_error {
+public:
+    explicit TraversalError(const std::string& what) : std::runtime_error{what} {}
+};
+
+void check(cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation) {
+        throw std::bad_alloc{};
+    }
+    if (e != cudaSuccess) {
+        throw DeviceError{std::format("{}: {}", what, cudaGetErrorString(e))};
+    }
+}
+
+template <typename F>
+int guarded(F&& body)
+{
+    try {
+        body();
+        return ALBEDO_OK;
+    } catch (const SceneParseError& e) {
+        g_last_error = e.what();
+        return ALBEDO_PARSE_ERROR;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return ALBEDO_INVALID_ARGUMENT;
+    } catch (const std::out_of_range& e) {
+        g_last_error = e.what();
+        return ALBEDO_OUT_OF_RANGE;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "out of memory";
+        return ALBEDO_OUT_OF_MEMORY;
+    } catch (const DeviceError& e) {
+        g_last_error = e.what();
+        return ALBEDO_DEVICE_ERROR;
+    } catch (const Unsupported& e) {
+        g_last_error = e.what();
+        return ALBEDO_UNSUPPORTED;
+    } catch (const TraversalError& e) {
+        g_last_error = e.what();
+        return ALBEDO_TRAVERSAL_ERROR;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return ALBEDO_IO_ERROR;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return ALBEDO_IO_ERROR;
+    }
+}
+
+// A device allocation freed on destruction.
+struct DeviceBuffer {
+    void* ptr{nullptr};
+    std::size_t bytes{0};
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(std::size_t n) : bytes{n}
+    {
+        if (n > 0) {
+            check(cudaMalloc(&ptr, n), "cudaMalloc");
+        }
+    }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr{o.ptr}, bytes{o.bytes}
+    {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept
+    {
+        std::swap(ptr, o.ptr);
+        std::swap(bytes, o.bytes);
+        return *this;
+    }
+    ~DeviceBuffer()
+    {
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+        }
+    }
+    template <typename T>
+    T* as() const
+    {
+        return static_cast<T*>(ptr);
+    }
+};
+
+template <typename T>
+DeviceBuffer upload(const std::vector<T>& host)
+{
+    DeviceBuffer buffer{host.size() * sizeof(T)};
+    if (!host.empty()) {
+        check(cudaMemcpy(buffer.ptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    }
+    return buffer;
+}
+
+template <typename T>
+DeviceBuffer uploadRaw(const T* data, std::size_t count)
+{
+    DeviceBuffer buffer{count * sizeof(T)};
+    if (count > 0) {
+        check(cudaMemcpy(buffer.ptr, data, count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    }
+    return buffer;
+}
+
+template <typename T>
+void download(T* host, const DeviceBuffer& buffer, std::size_t count)
+{
+    if (count > 0 && host != nullptr) {
+        check(cudaMemcpy(host, buffer.ptr, count * sizeof(T), cudaMemcpyDeviceToHost), "download");
+    }
+}
+
+Vec3 vec(const double* v) { return {v[0], v[1], v[2]}; }
+Rgb rgb(const double* v) { return {v[0], v[1], v[2]}; }
+
+BasicMaterialDesc basicFrom(const albedo_basic_material& m)
+{
+    BasicMaterialDesc b;
+    if (m.kind < 0 || m.kind > 2 || m.texture < 0 || m.texture > 2) {
+        throw std::invalid_argument{"unknown material or texture kind"};
+    }
+    b.kind = static_cast<BasicKind>(m.kind);
+    b.texture.kind = static_cast<TextureKind>(m.texture);
+    b.texture.a = rgb(m.a);
+    b.texture.b = rgb(m.b);
+    b.texture.frequency_or_scale = m.frequency_or_scale;
+    b.texture.veins = m.veins;
+    b.eta = rgb(m.a);
+    b.k = rgb(m.b);
+    b.ior = m.ior;
+    b.roughness = m.roughness;
+    return b;
+}
+
+} // namespace
+
+struct albedo_scene {
+    HostScene host;
+    bool prepared{false};
+    bool committed{false};
+    DeviceImage image;
+    DevScene dev{};
+    int stack_capacity{0};
+    std::vector<DeviceBuffer> buffers;
+    DeviceBuffer error_flag;
+
+    void requireOpen() const
+    {
+        if (committed || prepared) {
+            throw std::invalid_argument{"the scene is committed and can no longer change"};
+        }
+    }
+    void requireCommitted() const
+    {
+        if (!committed) {
+            throw std::invalid_argument{"the scene has not been committed"};
+        }
+    }
+
+    // Builds the TLAS and the device tables on the host.
+    void prepare()
+    {
+        if (prepared) {
+            return;
+        }
+        host.finalize();
+        image = flattenScene(host);
+        stack_capacity = stackCapacityFor(image.stack_need);
+        if (stack_capacity == 0) {
+            throw Unsupported{std::format("scene hierarchy needs {} traversal stack entries; the device kernels hold 64",
+                                          image.stack_need)};
+        }
+        prepared = true;
+    }
+
+    void commit()
+    {
+        prepare();
+        commitPrepared();
+    }
+
+    // Uploads the prepared tables to the current device.
+    void commitPrepared()
+    {
+        const auto add = [&](DeviceBuffer&& b) -> void* {
+            buffers.push_back(std::move(b));
+            return buffers.back().ptr;
+        };
+        dev.nodes = static_cast<const DevNode*>(add(upload(image.nodes)));
+        dev.objects = static_cast<const DevObject*>(add(upload(image.objects)));
+        dev.spheres = static_cast<const DevSphere*>(add(upload(image.spheres)));
+        dev.triangles = static_cast<const DevTriangle*>(add(upload(image.triangles)));
+        dev.attrs = static_cast<const DevTriangleAttr*>(add(upload(image.attrs)));
+        dev.instances = static_cast<const DevInstance*>(add(upload(image.instances)));
+        dev.materials = static_cast<const DevMaterial*>(add(upload(image.materials)));
+        dev.lights = static_cast<const DevLight*>(add(upload(image.lights)));
+        dev.object_light = static_cast<const std::int32_t*>(add(upload(image.object_light)));
+        dev.tlas_root = image.tlas_root;
+        dev.light_count = static_cast<std::uint32_t>(image.lights.size());
+        dev.sky_light = image.sky_light;
+        dev.object_count = static_cast<std::uint32_t>(image.objects.size());
+        error_flag = DeviceBuffer{sizeof(unsigned int)};
+        check(cudaMemset(error_flag.ptr, 0, sizeof(unsigned int)), "cudaMemset");
+        committed = true;
+    }
+
+    std::size_t deviceBytes() const
+    {
+        std::size_t total{0};
+        for (const DeviceBuffer& b : buffers) {
+            total += b.bytes;
+        }
+        return total;
+    }
+
+    // Reads and clears the kernel error flag.
+    void collectKernelError() const
+    {
+        unsigned int flag{0};
+        check(cudaMemcpy(&flag, error_flag.ptr, sizeof(flag), cudaMemcpyDeviceToHost), "error flag");
+        if (flag != 0) {
+            check(cudaMemset(error_flag.ptr, 0, sizeof(flag)), "cudaMemset");
+            throw TraversalError{"a traversal stack overflowed; the affected rays were ended"};
+        }
+    }
+};
+
+namespace {
+
+// renderImage's argument checks (render/render_image.cpp:60-67) and
+// PixelBuffer's size check (image/pixel_buffer.hpp:30-38).
+RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job)
+{
+    scene.requireCommitted();
+    if (job.samples_per_axis <= 0) {
+        throw std::invalid_argument{std::format("samples per axis must be positive, got {}", job.samples_per_axis)};
+    }
+    if (job.width <= 0 || job.height <= 0 ||
+        static_cast<std::uint64_t>(job.width) > (std::uint64_t{1} << 28) / static_cast<std::uint64_t>(job.height)) {
+        throw std::invalid_argument{std::format(
+            "invalid image size {}x{}: dimensions must be positive and the image at most {} pixels", job.width,
+            job.height, std::uint64_t{1} << 28)};
+    }
+    if (job.max_depth < 0 || job.roulette_start < 0) {
+        throw std::invalid_argument{"path limits must not be negative"};
+    }
+    if (job.estimator < 0 || job.estimator > 2) {
+        throw std::invalid_argument{"unknown estimator"};
+    }
+    if (!scene.host.has_camera) {
+        throw std::invalid_argument{"the scene has no camera"};
+    }
+    RenderArgs args{};
+    args.width = job.width;
+    args.height = job.height;
+    args.samples_per_axis = job.samples_per_axis;
+    args.estimator = job.estimator;
+    args.seed = job.seed;
+    args.max_depth = job.max_depth;
+    args.roulette_start = job.roulette_start;
+    return args;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* albedo_last_error(void) { return g_last_error.c_str(); }
+
+int albedo_scene_read(const char* path, albedo_scene** out)
+{
+    *out = nullptr;
+    return guarded([&] {
+        auto scene{std::make_unique<albedo_scene>()};
+        scene->host = readSceneFile(path);
+        scene->prepare();
+        *out = scene.release();
+    });
+}
+
+const void* albedo_scene_host_view(const albedo_scene* scene) { return &scene->host; }
+
+int albedo_scene_create(albedo_scene** out)
+{
+    return guarded([&] { *out = new albedo_scene{}; });
+}
+
+int albedo_scene_load(const char* path, albedo_scene** out)
+{
+    *out = nullptr;
+    return guarded([&] {
+        auto scene{std::make_unique<albedo_scene>()};
+        scene->host = readSceneFile(path);
+        scene->commit();
+        *out = scene.release();
+    });
+}
+
+void albedo_scene_destroy(albedo_scene* scene) { delete scene; }
+
+int albedo_scene_set_camera(albedo_scene* scene, const double look_from[3], const double look_at[3],
+                            const double up[3], double vertical_fov_degrees)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        CameraSettings settings{vec(look_from), vec(look_at), vec(up), vertical_fov_degrees};
+        static_cast<void>(buildCameraFrame(settings, 16.0 / 9.0));
+        scene->host.camera = settings;
+        scene->host.has_camera = true;
+    });
+}
+
+int albedo_scene_add_material(albedo_scene* scene, const albedo_material* material, uint32_t* out_material)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        MaterialDesc m;
+        m.mix = material->mix != 0;
+        m.first = basicFrom(material->first);
+        m.second = m.mix ? basicFrom(material->second) : m.first;
+        m.scale = material->scale;
+        m.veins = material->veins;
+        m.threshold = material->threshold;
+        const std::uint32_t id{scene->host.addMaterial(m)};
+        if (out_material != nullptr) {
+            *out_material = id;
+        }
+    });
+}
+
+namespace {
+void requireMaterial(const albedo_scene* scene, uint32_t material)
+{
+    if (material >= scene->host.materials.size()) {
+        throw std::invalid_argument{std::format("material {} is not defined", material)};
+    }
+}
+} // namespace
+
+int albedo_scene_add_sphere(albedo_scene* scene, const double center[3], double radius, uint32_t material,
+                            uint32_t* out_object)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        requireMaterial(scene, material);
+        const std::uint32_t id{scene->host.addSphere(vec(center), radius, material)};
+        if (out_object != nullptr) {
+            *out_object = id;
+        }
+    });
+}
+
+int albedo_scene_add_area_light(albedo_scene* scene, const double center[3], double radius, const double radiance[3],
+                                uint32_t material, uint32_t* out_object)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        requireMaterial(scene, material);
+        const std::uint32_t id{scene->host.addAreaLight(vec(center), radius, rgb(radiance), material)};
+        if (out_object != nullptr) {
+            *out_object = id;
+        }
+    });
+}
+
+int albedo_scene_add_point_light(albedo_scene* scene, const double position[3], const double intensity[3])
+{
+    return guarded([&] {
+        scene->requireOpen();
+        scene->host.addPointLight(vec(position), rgb(intensity));
+    });
+}
+
+int albedo_scene_set_sky(albedo_scene* scene, const double nadir[3], const double zenith[3])
+{
+    return guarded([&] {
+        scene->requireOpen();
+        scene->host.setSky(rgb(nadir), rgb(zenith));
+    });
+}
+
+namespace {
+std::vector<Vec3> positionsFrom(const double* positions, int64_t count)
+{
+    std::vector<Vec3> out(static_cast<std::size_t>(count));
+    for (int64_t i{0}; i < count; ++i) {
+        out[static_cast<std::size_t>(i)] = vec(positions + 3 * i);
+    }
+    return out;
+}
+std::vector<std::array<std::uint32_t, 3>> facesFrom(const uint32_t* faces, int64_t count)
+{
+    std::vector<std::array<std::uint32_t, 3>> out(static_cast<std::size_t>(count));
+    for (int64_t i{0}; i < count; ++i) {
+        out[static_cast<std::size_t>(i)] = {faces[3 * i], faces[3 * i + 1], faces[3 * i + 2]};
+    }
+    return out;
+}
+} // namespace
+
+int albedo_scene_add_mesh(albedo_scene* scene, const double* positions, int64_t position_count, const uint32_t* faces,
+                          int64_t face_count, const double* texture_coordinates, int64_t texture_coordinate_count,
+                          const uint32_t* texture_faces, int64_t texture_face_count, int32_t smooth, uint32_t* out_mesh)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        std::vector<std::array<double, 2>> uvs(static_cast<std::size_t>(texture_coordinate_count));
+        for (int64_t i{0}; i < texture_coordinate_count; ++i) {
+            uvs[static_cast<std::size_t>(i)] = {texture_coordinates[2 * i], texture_coordinates[2 * i + 1]};
+        }
+        const std::uint32_t id{scene->host.addMesh(positionsFrom(positions, position_count),
+                                                   facesFrom(faces, face_count), uvs,
+                                                   facesFrom(texture_faces, texture_face_count), smooth != 0)};
+        if (out_mesh != nullptr) {
+            *out_mesh = id;
+        }
+    });
+}
+
+int albedo_scene_add_instance(albedo_scene* scene, uint32_t mesh, const double to_world[12],
+                              const double to_object[12], uint32_t material, uint32_t* out_object)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        requireMaterial(scene, material);
+        Affine forward;
+        Affine backward;
+        for (int row{0}; row < 3; ++row) {
+            for (int col{0}; col < 3; ++col) {
+                forward.linear[row][col] = to_world[4 * row + col];
+                backward.linear[row][col] = to_object[4 * row + col];
+            }
+        }
+        forward.offset = {to_world[3], to_world[7], to_world[11]};
+        backward.offset = {to_object[3], to_object[7], to_object[11]};
+        const std::uint32_t id{
+            scene->host.addInstance(mesh, Transform::fromMaps(forward, backward), material)};
+        if (out_object != nullptr) {
+            *out_object = id;
+        }
+    });
+}
+
+int albedo_scene_add_triangles(albedo_scene* scene, const double* positions, int64_t position_count,
+                               const uint32_t* faces, int64_t face_count, uint32_t material)
+{
+    return guarded([&] {
+        scene->requireOpen();
+        requireMaterial(scene, material);
+        scene->host.addTriangles(positionsFrom(positions, position_count), facesFrom(faces, face_count), {}, {},
+                                 material);
+    });
+}
+
+int albedo_scene_prepare(albedo_scene* scene)
+{
+    return guarded([&] { scene->prepare(); });
+}
+
+int albedo_scene_commit(albedo_scene* scene)
+{
+    return guarded([&] {
+        if (scene->committed) {
+            throw std::invalid_argument{"the scene is already committed"};
+        }
+        scene->prepare();
+        scene->commitPrepared();
+    });
+}
+
+int albedo_scene_get_info(const albedo_scene* scene, albedo_scene_info* out)
+{
+    return guarded([&] {
+        if (!scene->prepared) {
+            throw std::invalid_argument{"the scene has not been prepared"};
+        }
+        out->objects = static_cast<int64_t>(scene->host.objects.size());
+        out->lights = static_cast<int64_t>(scene->host.lights.size());
+        out->triangles = static_cast<int64_t>(scene->image.triangles.size());
+        out->nodes = static_cast<int64_t>(scene->image.nodes.size());
+        out->device_bytes = static_cast<int64_t>(scene->deviceBytes());
+        out->stack_need = static_cast<int32_t>(scene->image.stack_need);
+        out->stack_capacity = scene->stack_capacity;
+    });
+}
+
+int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
+                  void* stream)
+{
+    return guarded([&] {
+        const RenderArgs args{renderArgsFor(*scene, *job)};
+        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
+        check(launchMegakernel(scene->dev, camera, args, reinterpret_cast<PixelAccum*>(accumulators),
+                               scene->error_flag.as<unsigned int>(), scene->stack_capacity,
+                               static_cast<cudaStream_t>(stream)),
+              "render launch");
+    });
+}
+
+int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators)
+{
+    return guarded([&] {
+        const RenderArgs args{renderArgsFor(*scene, *job)};
+        const std::size_t pixels{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height)};
+        DeviceBuffer device{uploadRaw(accumulators, pixels)};
+        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
+        check(launchMegakernel(scene->dev, camera, args, device.as<PixelAccum>(), scene->error_flag.as<unsigned int>(),
+                               scene->stack_capacity, nullptr),
+              "render launch");
+        check(cudaDeviceSynchronize(), "render");
+        download(accumulators, device, pixels);
+        scene->collectKernelError();
+    });
+}
+
+int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
+                              int64_t pixel_count, albedo_accumulator* accumulators, double* sum_squares)
+{
+    return guarded([&] {
+        RenderArgs args{renderArgsFor(*scene, *job)};
+        for (int64_t i{0}; i < pixel_count; ++i) {
+            if (pixels[2 * i] < 0 || pixels[2 * i] >= job->width || pixels[2 * i + 1] < 0 ||
+                pixels[2 * i + 1] >= job->height) {
+                throw std::invalid_argument{std::format("pixel {} lies outside the image", i)};
+            }
+        }
+        const auto count{static_cast<std::size_t>(pixel_count)};
+        DeviceBuffer device_pixels{uploadRaw(pixels, 2 * count)};
+        DeviceBuffer device_accum{uploadRaw(accumulators, count)};
+        DeviceBuffer device_squares;
+        if (sum_squares != nullptr) {
+            device_squares = uploadRaw(sum_squares, 3 * count);
+        }
+        args.pixels = device_pixels.as<int2>();
+        args.pixel_count = static_cast<int>(pixel_count);
+        args.sum_squares = sum_squares != nullptr ? device_squares.as<double>() : nullptr;
+        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
+        check(launchMegakernel(scene->dev, camera, args, device_accum.as<PixelAccum>(),
+                               scene->error_flag.as<unsigned int>(), scene->stack_capacity, nullptr),
+              "render launch");
+        check(cudaDeviceSynchronize(), "render");
+        download(accumulators, device_accum, count);
+        if (sum_squares != nullptr) {
+            download(sum_squares, device_squares, 3 * count);
+        }
+        scene->collectKernelError();
+    });
+}
+
+int albedo_scene_check(const albedo_scene* scene)
+{
+    return guarded([&] {
+        check(cudaDeviceSynchronize(), "synchronize");
+        scene->collectKernelError();
+    });
+}
+
+int albedo_trace_host(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                      int32_t* hit, float* t, int32_t* object, int32_t* triangle, float* point, float* normal,
+                      float* shading_normal, int32_t* front)
+{
+    return guarded([&] {
+        scene->requireCommitted();
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer d_rays{uploadRaw(rays, 6 * n)};
+        DeviceBuffer d_hit{n * sizeof(int)};
+        DeviceBuffer d_t{n * sizeof(float)};
+        DeviceBuffer d_object{n * sizeof(int)};
+        DeviceBuffer d_triangle{n * sizeof(int)};
+        const bool geometry{point != nullptr};
+        DeviceBuffer d_point{geometry ? 3 * n * sizeof(float) : 0};
+        DeviceBuffer d_normal{geometry ? 3 * n * sizeof(float) : 0};
+        DeviceBuffer d_shading{geometry ? 3 * n * sizeof(float) : 0};
+        DeviceBuffer d_front{geometry ? n * sizeof(int) : 0};
+        TraceOutputs out{d_hit.as<int>(),   d_t.as<float>(),      d_object.as<int>(),   d_triangle.as<int>(),
+                         d_point.as<float>(), d_normal.as<float>(), d_shading.as<float>(), d_front.as<int>()};
+        check(launchTrace(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max, out,
+                          scene->error_flag.as<unsigned int>(), scene->stack_capacity, nullptr),
+              "trace launch");
+        check(cudaDeviceSynchronize(), "trace");
+        download(hit, d_hit, n);
+        download(t, d_t, n);
+        download(object, d_object, n);
+        download(triangle, d_triangle, n);
+        if (geometry) {
+            download(point, d_point, 3 * n);
+            download(normal, d_normal, 3 * n);
+            download(shading_normal, d_shading, 3 * n);
+            download(front, d_front, n);
+        }
+        scene->collectKernelError();
+    });
+}
+
+int albedo_occluded_host(const albedo_scene* scene, const float* rays, const float* t_max, int64_t count,
+                         int32_t* occluded)
+{
+    return guarded([&] {
+        scene->requireCommitted();
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer d_rays{uploadRaw(rays, 6 * n)};
+        DeviceBuffer d_tmax{uploadRaw(t_max, n)};
+        DeviceBuffer d_out{n * sizeof(int)};
+        check(launchOccluded(scene->dev, d_rays.as<float>(), d_tmax.as<float>(), static_cast<int>(count),
+                             d_out.as<int>(), scene->error_flag.as<unsigned int>(), scene->stack_capacity, nullptr),
+              "occluded launch");
+        check(cudaDeviceSynchronize(), "occluded");
+        download(occluded, d_out, n);
+        scene->collectKernelError();
+    });
+}
+
+int albedo_probe_pixel_stream(uint64_t seed, int32_t x, int32_t y, int32_t width, int32_t count, uint32_t* out_u32,
+                              float* out_real)
+{
+    return guarded([&] {
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer u{n * sizeof(unsigned int)};
+        DeviceBuffer r{n * sizeof(float)};
+        check(launchPixelStream(seed, x, y, width, count, u.as<unsigned int>(), r.as<float>(), nullptr), "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_u32, u, n);
+        download(out_real, r, n);
+    });
+}
+
+int albedo_probe_lobe_eval(int32_t kind, const float* params, const float* wo_wi, int32_t count, float* out_f,
+                           float* out_pdf)
+{
+    return guarded([&] {
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer p{uploadRaw(params, 8)};
+        DeviceBuffer in{uploadRaw(wo_wi, 6 * n)};
+        DeviceBuffer f{3 * n * sizeof(float)};
+        DeviceBuffer pdf{n * sizeof(float)};
+        check(launchLobeEval(kind, p.as<float>(), in.as<float>(), count, f.as<float>(), pdf.as<float>(), nullptr),
+              "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_f, f, 3 * n);
+        download(out_pdf, pdf, n);
+    });
+}
+
+int albedo_probe_lobe_sample(int32_t kind, const float* params, const float* inputs, int32_t count, int32_t* out_valid,
+                             float* out_direction, float* out_weight, float* out_pdf, int32_t* out_specular)
+{
+    return guarded([&] {
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer p{uploadRaw(params, 8)};
+        DeviceBuffer in{uploadRaw(inputs, 6 * n)};
+        DeviceBuffer valid{n * sizeof(int)};
+        DeviceBuffer dir{3 * n * sizeof(float)};
+        DeviceBuffer weight{3 * n * sizeof(float)};
+        DeviceBuffer pdf{n * sizeof(float)};
+        DeviceBuffer spec{n * sizeof(int)};
+        check(cudaMemset(valid.ptr, 0, n * sizeof(int)), "memset");
+        check(launchLobeSample(kind, p.as<float>(), in.as<float>(), count, valid.as<int>(), dir.as<float>(),
+                               weight.as<float>(), pdf.as<float>(), spec.as<int>(), nullptr),
+              "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_valid, valid, n);
+        download(out_direction, dir, 3 * n);
+        download(out_weight, weight, 3 * n);
+        download(out_pdf, pdf, n);
+        download(out_specular, spec, n);
+    });
+}
+
+int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, float* out_turbulence)
+{
+    return guarded([&] {
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer in{uploadRaw(points, 3 * n)};
+        DeviceBuffer noise{n * sizeof(float)};
+        DeviceBuffer turb{n * sizeof(float)};
+        check(launchPerlin(in.as<float>(), count, noise.as<float>(), turb.as<float>(), nullptr), "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_noise, noise, n);
+        download(out_turbulence, turb, n);
+    });
+}
+
+int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film, int32_t count,
+                             float* out_rays)
+{
+    return guarded([&] {
+        const auto n{static_cast<std::size_t>(count)};
+        const DevCamera camera{deviceCamera(scene->host, width, height)};
+        DeviceBuffer in{uploadRaw(film, 2 * n)};
+        DeviceBuffer out{6 * n * sizeof(float)};
+        check(launchCameraRays(camera, in.as<float>(), count, out.as<float>(), nullptr), "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_rays, out, 6 * n);
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,211 @@
+// Binned-SAH BVH build; each helper restates the accel/bvh.cpp function named beside it.
+#include "bvh_build.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cstddef>
+#include <format>
+#include <optional>
+#include <stdexcept>
+
+namespace albedo_b200 {
+
+namespace {
+
+constexpr std::size_t kBins{12};            // accel/bvh.cpp:27
+constexpr double kTraversalCost{0.125};     // accel/bvh.cpp:30
+constexpr std::size_t kMaxLeaf{4};          // accel/bvh.cpp:32
+constexpr std::size_t kSahDepthLimit{32};   // accel/bvh.cpp:35
+
+struct Prim {
+    Box3 bounds{};
+    Vec3 centroid{};
+    std::size_t index{};
+};
+
+// centroidOf, accel/bvh.cpp:45-50: halved before adding.
+Vec3 centroidOf(const Box3& box)
+{
+    return {box.min.x / 2 + box.max.x / 2, box.min.y / 2 + box.max.y / 2, box.min.z / 2 + box.max.z / 2};
+}
+
+struct Extents {
+    Box3 bounds{};
+    Box3 centroids{};
+};
+
+// extentsOf, accel/bvh.cpp:70-78.
+Extents extentsOf(std::span<const Prim> prims)
+{
+    Extents e;
+    for (const Prim& p : prims) {
+        e.bounds = merged(e.bounds, p.bounds);
+        e.centroids = merged(e.centroids, p.centroid);
+    }
+    return e;
+}
+
+// widestAxis, accel/bvh.cpp:80-87.
+std::size_t widestAxis(const Box3& box)
+{
+    const Vec3 extent{box.extent()};
+    if (extent.x >= extent.y && extent.x >= extent.z) {
+        return 0;
+    }
+    return extent.y >= extent.z ? 1 : 2;
+}
+
+// halfDistance / halfSpread, accel/bvh.cpp:91-100.
+double halfDistance(double low, double high) { return high / 2 - low / 2; }
+double halfSpread(const Box3& centroids, std::size_t axis)
+{
+    return halfDistance(axisOf(centroids.min, axis), axisOf(centroids.max, axis));
+}
+
+// binOf, accel/bvh.cpp:107-118.
+std::size_t binOf(Vec3 centroid, const Box3& centroids, std::size_t axis)
+{
+    const double low{axisOf(centroids.min, axis)};
+    const double fraction{halfDistance(low, axisOf(centroid, axis)) / halfSpread(centroids, axis)};
+    const double limited{fraction > 0 ? std::min(fraction, 1.0) : 0.0};
+    const double scaled{limited * static_cast<double>(kBins)};
+    return std::min(static_cast<std::size_t>(scaled), kBins - 1);
+}
+
+struct Bin {
+    Box3 bounds{};
+    std::size_t count{};
+};
+
+struct Split {
+    std::size_t axis{};
+    std::size_t last_left_bin{};
+    double cost{std::numeric_limits<double>::infinity()};
+};
+
+// bestSplitAlong, accel/bvh.cpp:134-160: bin, sweep from the right, then scan left.
+Split bestSplitAlong(std::span<const Prim> prims, const Extents& extents, std::size_t axis)
+{
+    std::array<Bin, kBins> bins{};
+    for (const Prim& p : prims) {
+        Bin& bin{bins[binOf(p.centroid, extents.centroids, axis)]};
+        bin.bounds = merged(bin.bounds, p.bounds);
+        ++bin.count;
+    }
+    std::array<Bin, kBins> right_of{};
+    for (std::size_t bin{kBins - 1}; bin > 0; --bin) {
+        const Bin next{bin + 1 < kBins ? right_of[bin] : Bin{}};
+        right_of[bin - 1] = {merged(next.bounds, bins[bin].bounds), next.count + bins[bin].count};
+    }
+    Split best{.axis = axis};
+    Bin left{};
+    for (std::size_t bin{0}; bin + 1 < kBins; ++bin) {
+        left = {merged(left.bounds, bins[bin].bounds), left.count + bins[bin].count};
+        const Bin& right{right_of[bin]};
+        const double cost{left.bounds.surfaceArea() * static_cast<double>(left.count) +
+                          right.bounds.surfaceArea() * static_cast<double>(right.count)};
+        if (cost < best.cost) {
+            best = {.axis = axis, .last_left_bin = bin, .cost = cost};
+        }
+    }
+    return best;
+}
+
+// bestSplit, accel/bvh.cpp:163-176.
+std::optional<Split> bestSplit(std::span<const Prim> prims, const Extents& extents)
+{
+    std::optional<Split> best;
+    for (std::size_t axis{0}; axis < 3; ++axis) {
+        if (!(halfSpread(extents.centroids, axis) > 0)) {
+            continue;
+        }
+        const Split split{bestSplitAlong(prims, extents, axis)};
+        if (!best || split.cost < best->cost) {
+            best = split;
+        }
+    }
+    return best;
+}
+
+struct Partition {
+    std::size_t left_count{};
+    std::size_t axis{};
+};
+
+// partitionForSplit, accel/bvh.cpp:186-220.
+Partition partitionForSplit(std::span<Prim> prims, const Extents& extents, std::size_t depth)
+{
+    const std::size_t count{prims.size()};
+    if (depth < kSahDepthLimit) {
+        if (const auto split{bestSplit(prims, extents)}) {
+            const double area{extents.bounds.surfaceArea()};
+            const bool leaf_is_cheaper{static_cast<double>(count) * area <= kTraversalCost * area + split->cost};
+            if (count <= kMaxLeaf && leaf_is_cheaper) {
+                return {};
+            }
+            const auto middle{std::partition(prims.begin(), prims.end(), [&](const Prim& p) {
+                return binOf(p.centroid, extents.centroids, split->axis) <= split->last_left_bin;
+            })};
+            return {static_cast<std::size_t>(middle - prims.begin()), split->axis};
+        }
+    }
+    if (count <= kMaxLeaf) {
+        return {};
+    }
+    const std::size_t axis{widestAxis(extents.centroids)};
+    const std::size_t half{count / 2};
+    const auto middle{prims.begin() + static_cast<std::ptrdiff_t>(half)};
+    std::nth_element(prims.begin(), middle, prims.end(), [&](const Prim& a, const Prim& b) {
+        return axisOf(a.centroid, axis) < axisOf(b.centroid, axis);
+    });
+    return {half, axis};
+}
+
+// buildSubtree, accel/bvh.cpp:224-244 (recursion depth is bounded by 32 + log2 n).
+std::size_t buildSubtree(BuiltBvh& bvh, std::span<Prim> prims, std::size_t first, std::size_t depth)
+{
+    const std::size_t index{bvh.nodes.size()};
+    const Extents extents{extentsOf(prims)};
+    bvh.nodes.push_back({.bounds = extents.bounds});
+    bvh.max_depth = std::max<std::uint32_t>(bvh.max_depth, static_cast<std::uint32_t>(depth));
+    const Partition partition{prims.size() == 1 ? Partition{} : partitionForSplit(prims, extents, depth)};
+    if (partition.left_count == 0) {
+        bvh.nodes[index].offset = first;
+        bvh.nodes[index].count = static_cast<std::uint32_t>(prims.size());
+        return index;
+    }
+    buildSubtree(bvh, prims.first(partition.left_count), first, depth + 1);
+    const std::size_t second{
+        buildSubtree(bvh, prims.subspan(partition.left_count), first + partition.left_count, depth + 1)};
+    bvh.nodes[index].offset = second;
+    bvh.nodes[index].axis = static_cast<std::uint8_t>(partition.axis);
+    return index;
+}
+
+} // namespace
+
+BuiltBvh buildBvh(std::span<const Box3> primitive_bounds)
+{
+    BuiltBvh bvh;
+    if (primitive_bounds.empty()) {
+        return bvh;
+    }
+    std::vector<Prim> prims;
+    prims.reserve(primitive_bounds.size());
+    for (std::size_t index{0}; index < primitive_bounds.size(); ++index) {
+        const Box3& box{primitive_bounds[index]};
+        if (!isFinite(box.min) || !isFinite(box.max) || box.isEmpty()) {
+            throw std::invalid_argument{std::format("BVH primitive {} has an empty or non-finite box", index)};
+        }
+        prims.push_back({box, centroidOf(box), index});
+    }
+    bvh.nodes.reserve(2 * prims.size() - 1);
+    buildSubtree(bvh, prims, 0, 0);
+    bvh.order.reserve(prims.size());
+    for (const Prim& p : prims) {
+        bvh.order.push_back(static_cast<std::uint32_t>(p.index));
+    }
+    return bvh;
+}
+
+} // namespace albedo_b200

@@ -1,0 +1,37 @@
+// HostScene -> device tables (host copies), ready for one upload.
+#pragma once
+
+#include "../device_layout.hpp"
+#include "host_scene.hpp"
+
+#include <vector>
+
+namespace albedo_b200 {
+
+struct DeviceImage {
+    std::vector<DevNode> nodes;
+    std::vector<DevObject> objects;
+    std::vector<DevSphere> spheres;
+    std::vector<DevTriangle> triangles;
+    std::vector<DevTriangleAttr> attrs;
+    std::vector<DevInstance> instances;
+    std::vector<DevMaterial> materials;
+    std::vector<DevLight> lights;
+    std::vector<std::int32_t> object_light;
+    // Leaf position of each object id, and the triangle-table base of each mesh.
+    std::vector<std::uint32_t> object_position;
+    std::vector<std::uint32_t> mesh_triangle_base;
+    std::uint32_t tlas_root{kEmptyChild};
+    std::int32_t sky_light{-1};
+    // Traversal stack entries a query can need: TLAS depth + deepest BLAS + 2.
+    std::uint32_t stack_need{0};
+};
+
+// Throws std::invalid_argument if the scene exceeds the device layout's limits
+// (leaf positions must fit 28 bits).
+DeviceImage flattenScene(const HostScene& scene);
+
+// The camera frame for an image of the given size, rounded to FP32.
+DevCamera deviceCamera(const HostScene& scene, int width, int height);
+
+} // namespace albedo_b200

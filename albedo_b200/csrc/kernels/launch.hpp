@@ -1,0 +1,74 @@
+// Host-callable launchers for the CUDA kernels (defined in the .cu files).
+#pragma once
+
+#include "../device_layout.hpp"
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace albedo_b200 {
+
+// Per-pixel accumulator, laid out as the reference's PixelBuffer::Accumulator
+// (image/pixel_buffer.hpp:53-57): FP64 RGB sum and an int64 sample count.
+struct PixelAccum {
+    double r, g, b;
+    long long count;
+};
+
+enum Estimator : int { kEstimatorPath = 0, kEstimatorScatterOnly = 1, kEstimatorNormals = 2 };
+
+struct RenderArgs {
+    int width;
+    int height;
+    int samples_per_axis;
+    int estimator;
+    unsigned long long seed;
+    int max_depth;       // PathEstimator::max_depth / ScatterOnlyEstimator::max_scatter_count
+    int roulette_start;
+    const int2* pixels;  // optional pixel subset (x, y); null renders the whole image
+    int pixel_count;
+    double* sum_squares; // optional per-pixel (or per-listed-pixel) sums of squared samples, 3 doubles each
+};
+
+// Stack capacity (entries per thread) of the kernel chosen for a scene, or 0 if
+// the scene's hierarchy is deeper than every compiled variant supports.
+int stackCapacityFor(std::uint32_t stack_need);
+
+// The plain megakernel: one thread per pixel, serial over that pixel's n x n
+// stratified samples so each pixel's PCG32 stream is consumed as the
+// reference consumes it. Adds into `accum` (one PixelAccum per pixel, or per
+// listed pixel when args.pixels is set).
+cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
+                             unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
+
+// Ray queries: rays are 6 floats (origin, direction). Closest hit in (t_min,
+// t_max): hit flag, t, object id, triangle id within its mesh (-1 for spheres),
+// point, geometric normal facing the ray, shading normal, front-face flag.
+struct TraceOutputs {
+    int* hit;
+    float* t;
+    int* object;
+    int* triangle;
+    float* point;
+    float* normal;
+    float* shading_normal;
+    int* front;
+};
+cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
+                        const TraceOutputs& out, unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
+// Any hit in (0, t_max[i]).
+cudaError_t launchOccluded(const DevScene& scene, const float* rays, const float* t_max, int count, int* occluded,
+                           unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
+
+// Probe kernels for parity tests of device arithmetic.
+cudaError_t launchPixelStream(unsigned long long seed, int x, int y, int width, int count, unsigned int* out_u32,
+                              float* out_real, cudaStream_t stream);
+cudaError_t launchLobeEval(int kind, const float* params, const float* wo_wi, int count, float* out_f, float* out_pdf,
+                           cudaStream_t stream);
+cudaError_t launchLobeSample(int kind, const float* params, const float* inputs, int count, int* out_valid,
+                             float* out_dir, float* out_weight, float* out_pdf, int* out_specular, cudaStream_t stream);
+cudaError_t launchPerlin(const float* points, int count, float* out_noise, float* out_turbulence, cudaStream_t stream);
+cudaError_t launchCameraRays(const DevCamera& camera, const float* film, int count, float* out_rays,
+                             cudaStream_t stream);
+
+} // namespace albedo_b200

@@ -1,0 +1,154 @@
+// Probe kernels: run one piece of device arithmetic over arrays of inputs so the
+// parity tests can compare it, input for input, with the reference: the pixel
+// random stream, the BSDF lobes, Perlin noise and camera rays.
+#include "estimator.cuh"
+
+namespace albedo_b200 {
+
+namespace {
+
+constexpr int kProbeBlock = 256;
+
+int probeBlocks(int count) { return (count + kProbeBlock - 1) / kProbeBlock; }
+
+__global__ void pixelStreamKernel(unsigned long long seed, int x, int y, int width, int count, unsigned int* out_u32,
+                                  float* out_real)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) {
+        return;
+    }
+    Pcg32 g = pixelGenerator(seed, static_cast<std::uint32_t>(x), static_cast<std::uint32_t>(y),
+                             static_cast<std::uint32_t>(width));
+    for (int i = 0; i < count; ++i) {
+        const std::uint32_t u = g.next();
+        out_u32[i] = u;
+        out_real[i] = static_cast<float>(u >> 8u) * 5.9604644775390625e-8f;
+    }
+}
+
+ALB_DEV Lobe probeLobe(int kind, const float* p)
+{
+    if (kind == kLobeLambert) {
+        return {kLobeLambert, mk(p[0], p[1], p[2]), gray(0.0f), 0.0f, 1.0f};
+    }
+    if (kind == kLobeConductor) {
+        return {kLobeConductor, mk(p[0], p[1], p[2]), mk(p[3], p[4], p[5]), p[6], 1.0f};
+    }
+    return {kLobeDielectric, gray(0.0f), gray(0.0f), p[1], p[0]};
+}
+
+__global__ void lobeEvalKernel(int kind, const float* params, const float* wo_wi, int count, float* out_f,
+                               float* out_pdf)
+{
+    const int i = blockIdx.x * kProbeBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    const Lobe lobe = probeLobe(kind, params);
+    const float3 wo = mk(wo_wi[6 * i], wo_wi[6 * i + 1], wo_wi[6 * i + 2]);
+    const float3 wi = mk(wo_wi[6 * i + 3], wo_wi[6 * i + 4], wo_wi[6 * i + 5]);
+    const float3 f = lobeEvaluate(lobe, wo, wi);
+    out_f[3 * i] = f.x;
+    out_f[3 * i + 1] = f.y;
+    out_f[3 * i + 2] = f.z;
+    out_pdf[i] = lobePdf(lobe, wo, wi);
+}
+
+__global__ void lobeSampleKernel(int kind, const float* params, const float* inputs, int count, int* out_valid,
+                                 float* out_dir, float* out_weight, float* out_pdf, int* out_specular)
+{
+    const int i = blockIdx.x * kProbeBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    const Lobe lobe = probeLobe(kind, params);
+    const float* v = inputs + 6 * i;
+    ScatterSample s;
+    const bool ok = lobeSample(lobe, mk(v[0], v[1], v[2]), v[3], v[4], v[5], s);
+    out_valid[i] = ok ? 1 : 0;
+    if (!ok) {
+        return;
+    }
+    out_dir[3 * i] = s.dir.x;
+    out_dir[3 * i + 1] = s.dir.y;
+    out_dir[3 * i + 2] = s.dir.z;
+    out_weight[3 * i] = s.weight.x;
+    out_weight[3 * i + 1] = s.weight.y;
+    out_weight[3 * i + 2] = s.weight.z;
+    out_pdf[i] = s.pdf;
+    out_specular[i] = s.specular ? 1 : 0;
+}
+
+__global__ void perlinKernel(const float* points, int count, float* out_noise, float* out_turbulence)
+{
+    const int i = blockIdx.x * kProbeBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    const float3 p = mk(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+    out_noise[i] = perlinNoise(p);
+    out_turbulence[i] = turbulence(p);
+}
+
+__global__ void cameraRaysKernel(const DevCamera camera, const float* film, int count, float* out_rays)
+{
+    const int i = blockIdx.x * kProbeBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    float3 o, d;
+    cameraRay(camera, film[2 * i], film[2 * i + 1], o, d);
+    out_rays[6 * i] = o.x;
+    out_rays[6 * i + 1] = o.y;
+    out_rays[6 * i + 2] = o.z;
+    out_rays[6 * i + 3] = d.x;
+    out_rays[6 * i + 4] = d.y;
+    out_rays[6 * i + 5] = d.z;
+}
+
+} // namespace
+
+cudaError_t launchPixelStream(unsigned long long seed, int x, int y, int width, int count, unsigned int* out_u32,
+                              float* out_real, cudaStream_t stream)
+{
+    pixelStreamKernel<<<1, 1, 0, stream>>>(seed, x, y, width, count, out_u32, out_real);
+    return cudaGetLastError();
+}
+
+cudaError_t launchLobeEval(int kind, const float* params, const float* wo_wi, int count, float* out_f, float* out_pdf,
+                           cudaStream_t stream)
+{
+    if (count > 0) {
+        lobeEvalKernel<<<probeBlocks(count), kProbeBlock, 0, stream>>>(kind, params, wo_wi, count, out_f, out_pdf);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchLobeSample(int kind, const float* params, const float* inputs, int count, int* out_valid,
+                             float* out_dir, float* out_weight, float* out_pdf, int* out_specular, cudaStream_t stream)
+{
+    if (count > 0) {
+        lobeSampleKernel<<<probeBlocks(count), kProbeBlock, 0, stream>>>(kind, params, inputs, count, out_valid,
+                                                                          out_dir, out_weight, out_pdf, out_specular);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchPerlin(const float* points, int count, float* out_noise, float* out_turbulence, cudaStream_t stream)
+{
+    if (count > 0) {
+        perlinKernel<<<probeBlocks(count), kProbeBlock, 0, stream>>>(points, count, out_noise, out_turbulence);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launchCameraRays(const DevCamera& camera, const float* film, int count, float* out_rays,
+                             cudaStream_t stream)
+{
+    if (count > 0) {
+        cameraRaysKernel<<<probeBlocks(count), kProbeBlock, 0, stream>>>(camera, film, count, out_rays);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace albedo_b200

@@ -1,0 +1,267 @@
+// The plain per-pixel megakernel and the ray-query kernels.
+//
+// renderPixel (render/render_image.cpp:27-44): each pixel owns one PCG32 stream
+// and draws its n x n stratified samples from it in row-major order, so one
+// thread runs one pixel's samples serially. Blocks cover 16 x 8 pixel tiles so a
+// warp's camera rays start coherent. The traversal stack of every thread sits in
+// shared memory (STACK entries of 8 bytes).
+#include "estimator.cuh"
+
+namespace albedo_b200 {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kTileW = 16;
+constexpr int kTileH = 8;
+
+template <int STACK, int EST>
+__global__ void __launch_bounds__(kBlock) megakernel(const DevScene scene, const DevCamera camera,
+                                                     const RenderArgs args, PixelAccum* accum,
+                                                     unsigned int* error_flag)
+{
+    extern __shared__ uint2 stack[];
+    const TraceContext ctx{stack + threadIdx.x, kBlock, STACK, error_flag};
+    int x, y, slot;
+    if (args.pixels != nullptr) {
+        slot = blockIdx.x * kBlock + threadIdx.x;
+        if (slot >= args.pixel_count) {
+            return;
+        }
+        x = args.pixels[slot].x;
+        y = args.pixels[slot].y;
+    } else {
+        const int tiles_x = (args.width + kTileW - 1) / kTileW;
+        x = (blockIdx.x % tiles_x) * kTileW + static_cast<int>(threadIdx.x % kTileW);
+        y = (blockIdx.x / tiles_x) * kTileH + static_cast<int>(threadIdx.x / kTileW);
+        if (x >= args.width || y >= args.height) {
+            return;
+        }
+        slot = y * args.width + x;
+    }
+    Pcg32 g = pixelGenerator(args.seed, static_cast<std::uint32_t>(x), static_cast<std::uint32_t>(y),
+                             static_cast<std::uint32_t>(args.width));
+    const int n = args.samples_per_axis;
+    const float inv_n = 1.0f / static_cast<float>(n);
+    const float width = static_cast<float>(args.width);
+    const float height = static_cast<float>(args.height);
+    double sr = 0.0, sg = 0.0, sb = 0.0;
+    double qr = 0.0, qg = 0.0, qb = 0.0;
+    for (int sy = 0; sy < n; ++sy) {
+        for (int sx = 0; sx < n; ++sx) {
+            const float jx = g.next1D();
+            const float jy = g.next1D();
+            const float fx = (static_cast<float>(x) + (static_cast<float>(sx) + jx) * inv_n) / width;
+            const float fy = (static_cast<float>(y) + (static_cast<float>(sy) + jy) * inv_n) / height;
+            float3 o, d;
+            cameraRay(camera, fx, fy, o, d);
+            const float3 L = estimateRadiance<EST>(scene, ctx, o, d, g, args);
+            sr += L.x;
+            sg += L.y;
+            sb += L.z;
+            qr += static_cast<double>(L.x) * L.x;
+            qg += static_cast<double>(L.y) * L.y;
+            qb += static_cast<double>(L.z) * L.z;
+        }
+    }
+    PixelAccum& a = accum[slot];
+    a.r += sr;
+    a.g += sg;
+    a.b += sb;
+    a.count += static_cast<long long>(n) * n;
+    if (args.sum_squares != nullptr) {
+        args.sum_squares[3 * slot] += qr;
+        args.sum_squares[3 * slot + 1] += qg;
+        args.sum_squares[3 * slot + 2] += qb;
+    }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(kBlock) traceKernel(const DevScene scene, const float* rays, int count, float t_min,
+                                                      float t_max, TraceOutputs out, unsigned int* error_flag)
+{
+    extern __shared__ uint2 stack[];
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    const float3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+    const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+    TraceHit hit;
+    float tmax = t_max;
+    const bool found = traceScene<false>(scene, o, d, t_min, tmax, SkipRule::none(), hit, stack + threadIdx.x, kBlock,
+                                         STACK, error_flag);
+    out.hit[i] = found ? 1 : 0;
+    if (!found) {
+        return;
+    }
+    Surface sf;
+    resolveHit(scene, o, d, hit, sf);
+    out.t[i] = hit.t;
+    out.object[i] = static_cast<int>(sf.object_id);
+    out.triangle[i] = -1;
+    const DevObject obj = scene.objects[hit.obj_pos];
+    if (obj.kind == kObjInstance) {
+        out.triangle[i] = static_cast<int>(__float_as_uint(scene.triangles[hit.tri_pos].v0w));
+    }
+    if (out.point != nullptr) {
+        out.point[3 * i] = sf.p.x;
+        out.point[3 * i + 1] = sf.p.y;
+        out.point[3 * i + 2] = sf.p.z;
+        out.normal[3 * i] = sf.n.x;
+        out.normal[3 * i + 1] = sf.n.y;
+        out.normal[3 * i + 2] = sf.n.z;
+        out.shading_normal[3 * i] = sf.ns.x;
+        out.shading_normal[3 * i + 1] = sf.ns.y;
+        out.shading_normal[3 * i + 2] = sf.ns.z;
+        out.front[i] = sf.front ? 1 : 0;
+    }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(kBlock) occludedKernel(const DevScene scene, const float* rays, const float* t_max,
+                                                         int count, int* occluded_out, unsigned int* error_flag)
+{
+    extern __shared__ uint2 stack[];
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    const float3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+    const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+    TraceHit hit;
+    float tmax = t_max[i];
+    occluded_out[i] = traceScene<true>(scene, o, d, 0.0f, tmax, SkipRule::none(), hit, stack + threadIdx.x, kBlock,
+                                       STACK, error_flag)
+                          ? 1
+                          : 0;
+}
+
+constexpr std::size_t stackBytes(int stack) { return static_cast<std::size_t>(stack) * kBlock * sizeof(uint2); }
+
+// Opts a kernel into the dynamic shared memory its stack needs (above the 48 KB
+// default for 64-entry stacks); done once per kernel.
+template <typename Kernel>
+cudaError_t launchWithStack(Kernel kernel, int stack, int blocks, cudaStream_t stream, bool& configured)
+{
+    if (!configured) {
+        const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(stackBytes(stack)));
+        if (e != cudaSuccess) {
+            return e;
+        }
+        configured = true;
+    }
+    (void)blocks;
+    (void)stream;
+    return cudaSuccess;
+}
+
+template <int STACK>
+cudaError_t launchMegaStack(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
+                            unsigned int* error_flag, cudaStream_t stream)
+{
+    int blocks;
+    if (args.pixels != nullptr) {
+        blocks = (args.pixel_count + kBlock - 1) / kBlock;
+    } else {
+        blocks = ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
+    }
+    if (blocks == 0) {
+        return cudaSuccess;
+    }
+    static bool configured[3] = {false, false, false};
+    const std::size_t smem = stackBytes(STACK);
+    cudaError_t e = cudaSuccess;
+    switch (args.estimator) {
+    case kEstimatorScatterOnly:
+        e = launchWithStack(megakernel<STACK, kEstimatorScatterOnly>, STACK, blocks, stream, configured[1]);
+        if (e == cudaSuccess) {
+            megakernel<STACK, kEstimatorScatterOnly><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
+        }
+        break;
+    case kEstimatorNormals:
+        e = launchWithStack(megakernel<STACK, kEstimatorNormals>, STACK, blocks, stream, configured[2]);
+        if (e == cudaSuccess) {
+            megakernel<STACK, kEstimatorNormals><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
+        }
+        break;
+    default:
+        e = launchWithStack(megakernel<STACK, kEstimatorPath>, STACK, blocks, stream, configured[0]);
+        if (e == cudaSuccess) {
+            megakernel<STACK, kEstimatorPath><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
+        }
+        break;
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+} // namespace
+
+int stackCapacityFor(std::uint32_t stack_need)
+{
+    if (stack_need <= 32u) {
+        return 32;
+    }
+    if (stack_need <= 64u) {
+        return 64;
+    }
+    return 0;
+}
+
+cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
+                             unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
+{
+    if (stack_capacity == 32) {
+        return launchMegaStack<32>(scene, camera, args, accum, error_flag, stream);
+    }
+    return launchMegaStack<64>(scene, camera, args, accum, error_flag, stream);
+}
+
+cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
+                        const TraceOutputs& out, unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
+{
+    const int blocks = (count + kBlock - 1) / kBlock;
+    if (blocks == 0) {
+        return cudaSuccess;
+    }
+    static bool configured[2] = {false, false};
+    cudaError_t e;
+    if (stack_capacity == 32) {
+        e = launchWithStack(traceKernel<32>, 32, blocks, stream, configured[0]);
+        if (e == cudaSuccess) {
+            traceKernel<32><<<blocks, kBlock, stackBytes(32), stream>>>(scene, rays, count, t_min, t_max, out, error_flag);
+        }
+    } else {
+        e = launchWithStack(traceKernel<64>, 64, blocks, stream, configured[1]);
+        if (e == cudaSuccess) {
+            traceKernel<64><<<blocks, kBlock, stackBytes(64), stream>>>(scene, rays, count, t_min, t_max, out, error_flag);
+        }
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t launchOccluded(const DevScene& scene, const float* rays, const float* t_max, int count, int* occluded_out,
+                           unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
+{
+    const int blocks = (count + kBlock - 1) / kBlock;
+    if (blocks == 0) {
+        return cudaSuccess;
+    }
+    static bool configured[2] = {false, false};
+    cudaError_t e;
+    if (stack_capacity == 32) {
+        e = launchWithStack(occludedKernel<32>, 32, blocks, stream, configured[0]);
+        if (e == cudaSuccess) {
+            occludedKernel<32><<<blocks, kBlock, stackBytes(32), stream>>>(scene, rays, t_max, count, occluded_out, error_flag);
+        }
+    } else {
+        e = launchWithStack(occludedKernel<64>, 64, blocks, stream, configured[1]);
+        if (e == cudaSuccess) {
+            occludedKernel<64><<<blocks, kBlock, stackBytes(64), stream>>>(scene, rays, t_max, count, occluded_out, error_flag);
+        }
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+} // namespace albedo_b200

@@ -1,0 +1,407 @@
+// Ray queries over the two-level BVH: TLAS over objects, BLAS per shared mesh.
+//
+// Restates, in FP32 over the device layout, the reference's query path:
+//   Bvh::traverse / nearestHit / anyHit   accel/bvh.hpp:211-267
+//   clipToSlab with Ize's exit widening    accel/bvh.hpp:80-103
+//   orderedChildren (near child by sign)   accel/bvh.hpp:118-129
+//   Sphere::intersect (Haines)             geometry/sphere.cpp:92-135
+//   Triangle::intersect (watertight)       geometry/triangle.cpp:132-176
+//   MeshInstance::intersect                geometry/mesh_instance.cpp:32-48
+// The node order, the near/far rule and "a later hit must be strictly nearer"
+// are the reference's, so ties resolve the same way. Boxes are FP32 rounded
+// outward, which can only add box hits, never lose one.
+//
+// The traversal stack lives in shared memory: entry i of thread `lane` is at
+// stack[i * stride + lane] (entry-major, so a warp touching the same depth hits
+// consecutive banks). Each entry is (child reference, entry distance).
+#pragma once
+
+#include "common.cuh"
+
+namespace albedo_b200 {
+
+// 1 + 2 gamma(3) for FP32 (u = 2^-24), rounded up: Ize 2013 as in accel/bvh.hpp:80-84.
+constexpr float kBoxExitWidening = 1.00000036f;
+constexpr std::uint32_t kExitMarker = 0x7FFFFFFFu; // stack entry: leave the current instance
+constexpr std::uint32_t kNoPrim = 0xFFFFFFFFu;
+
+enum SphereSkip : int { kSphereTestBoth = 0, kSphereSkipAll = 1, kSphereFarOnly = 2 };
+
+// What a ray leaving a surface must not hit again. A triangle cannot be hit
+// again by a ray leaving it; a sphere left outward cannot be hit again, and one
+// left inward only at its far root. This replaces the reference's FP64-scale
+// 1e-7 origin offset (estimator/surface_ray.hpp:18-31), which FP32 cannot
+// resolve, with the exact statement it approximates.
+struct SkipRule {
+    std::uint32_t object_pos;  // TLAS leaf position of the object left, or kNoPrim
+    std::uint32_t tri_pos;     // triangle table position left (instances), or kNoPrim
+    int sphere_mode;           // SphereSkip for a sphere object
+    std::uint32_t light_object_pos; // shadow rays: the area light's own object, or kNoPrim
+
+    ALB_DEV static SkipRule none() { return {kNoPrim, kNoPrim, kSphereTestBoth, kNoPrim}; }
+};
+
+struct TraceHit {
+    float t;
+    std::uint32_t obj_pos; // TLAS leaf position of the object hit
+    std::uint32_t tri_pos; // triangle table position, or kNoPrim for spheres
+    float b0, b1, b2;      // barycentric weights of a triangle hit
+};
+
+// The ray as traversal and the watertight test need it (accel/bvh.hpp:60-78,
+// geometry/triangle.cpp:81-106).
+struct TravRay {
+    float3 o, d, inv;
+    std::uint32_t neg; // bit a set when d[a] < 0
+    int kx, ky, kz;
+    float sx, sy, sz;
+    bool usable; // |d|^2 is a normal number
+
+    ALB_DEV void setup(float3 origin, float3 dir)
+    {
+        o = origin;
+        d = dir;
+        inv = mk(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
+        neg = (dir.x < 0.0f ? 1u : 0u) | (dir.y < 0.0f ? 2u : 0u) | (dir.z < 0.0f ? 4u : 0u);
+        usable = isNormalF(lengthSquared(dir));
+        const float mx = fabsf(dir.x);
+        const float my = fabsf(dir.y);
+        const float mz = fabsf(dir.z);
+        kz = mx > my ? (mx > mz ? 0 : 2) : (my > mz ? 1 : 2);
+        kx = kz == 2 ? 0 : kz + 1;
+        ky = kx == 2 ? 0 : kx + 1;
+        const float dz = comp(dir, kz);
+        if (dz < 0.0f) {
+            const int t = kx;
+            kx = ky;
+            ky = t;
+        }
+        sx = comp(dir, kx) / dz;
+        sy = comp(dir, ky) / dz;
+        sz = 1.0f / dz;
+    }
+};
+
+// clipToSlab on all three axes for one box; returns whether [tmin, tmax]
+// survives and the clipped entry distance (accel/bvh.hpp:93-114).
+ALB_DEV bool slabTest(float lox, float hix, float loy, float hiy, float loz, float hiz, const TravRay& r, float tmin,
+                      float tmax, float& entry)
+{
+    float lo = tmin;
+    float hi = tmax;
+    float n, f;
+#define ALB_CLIP(LO, HI, O, INV)                                                                                       \
+    n = ((LO) - (O)) * (INV);                                                                                          \
+    f = ((HI) - (O)) * (INV);                                                                                          \
+    if (n > f) {                                                                                                       \
+        const float s_ = n;                                                                                            \
+        n = f;                                                                                                         \
+        f = s_;                                                                                                        \
+    }                                                                                                                  \
+    f *= f < 0.0f ? 2.0f - kBoxExitWidening : kBoxExitWidening;                                                        \
+    lo = n > lo ? n : lo;                                                                                              \
+    hi = f < hi ? f : hi;
+    ALB_CLIP(lox, hix, r.o.x, r.inv.x)
+    ALB_CLIP(loy, hiy, r.o.y, r.inv.y)
+    ALB_CLIP(loz, hiz, r.o.z, r.inv.z)
+#undef ALB_CLIP
+    entry = lo;
+    return lo <= hi;
+}
+
+// Haines' sphere test in precision T (geometry/sphere.cpp:92-135), returning the
+// nearest root strictly inside (tmin, tmax), honouring the skip mode.
+template <typename T>
+ALB_DEV bool sphereRoot(T ox, T oy, T oz, T dx, T dy, T dz, T cx, T cy, T cz, T radius, T tmin, T tmax, int mode,
+                        T& t_out)
+{
+    const T ocx = ox - cx;
+    const T ocy = oy - cy;
+    const T ocz = oz - cz;
+    const T a = dx * dx + dy * dy + dz * dz;
+    const T h = dx * ocx + dy * ocy + dz * ocz;
+    const T r2 = radius * radius;
+    const T c = (ocx * ocx + ocy * ocy + ocz * ocz) - r2;
+    const T k = h / a;
+    const T lx = ocx - dx * k;
+    const T ly = ocy - dy * k;
+    const T lz = ocz - dz * k;
+    const T disc = a * (r2 - (lx * lx + ly * ly + lz * lz));
+    if (disc < T(0)) {
+        return false;
+    }
+    const T q = -(h + copysign(sqrt(disc), h));
+    T near_root = T(0);
+    T far_root = T(0);
+    if (q != T(0)) {
+        near_root = q / a;
+        far_root = c / q;
+        if (near_root > far_root) {
+            const T s = near_root;
+            near_root = far_root;
+            far_root = s;
+        }
+    }
+    T t = near_root;
+    if (mode == kSphereFarOnly || !(tmin < t && t < tmax)) {
+        t = far_root;
+        if (!(tmin < t && t < tmax)) {
+            return false;
+        }
+    }
+    // A hit point that rounds onto the center has no normal: a miss (geometry/sphere.cpp:121-126).
+    const T px = ox + dx * t - cx;
+    const T py = oy + dy * t - cy;
+    const T pz = oz + dz * t - cz;
+    if (!(px * px + py * py + pz * pz > T(0))) {
+        return false;
+    }
+    t_out = t;
+    return true;
+}
+
+ALB_DEV bool intersectSphere(const TravRay& r, const DevSphere& s, bool wide, float tmin, float tmax, int mode,
+                             float& t)
+{
+    if (!r.usable) {
+        return false;
+    }
+    if (wide) {
+        // Coordinates of order 1e4 (room-sized walls): o - c and |o - c|^2 - r^2
+        // cancel catastrophically in FP32, so the quadratic runs in FP64.
+        double td;
+        if (!sphereRoot<double>(r.o.x, r.o.y, r.o.z, r.d.x, r.d.y, r.d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, td)) {
+            return false;
+        }
+        const float tf = static_cast<float>(td);
+        if (!(tmin < tf && tf < tmax)) {
+            return false;
+        }
+        t = tf;
+        return true;
+    }
+    return sphereRoot<float>(r.o.x, r.o.y, r.o.z, r.d.x, r.d.y, r.d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, t);
+}
+
+// Woop-Benthin-Wald watertight test (geometry/triangle.cpp:132-176). Every
+// product is rounded on its own (no FMA), so edge functions of triangles sharing
+// an edge are exact negations; zero edge functions are recomputed in FP64.
+ALB_DEV bool intersectTriangle(const TravRay& r, const float4& p0, const float4& p1, const float4& p2, float tmin,
+                               float tmax, float& t, float& b0, float& b1, float& b2)
+{
+    const float3 A = mk(__fsub_rn(p0.x, r.o.x), __fsub_rn(p0.y, r.o.y), __fsub_rn(p0.z, r.o.z));
+    const float3 B = mk(__fsub_rn(p1.x, r.o.x), __fsub_rn(p1.y, r.o.y), __fsub_rn(p1.z, r.o.z));
+    const float3 C = mk(__fsub_rn(p2.x, r.o.x), __fsub_rn(p2.y, r.o.y), __fsub_rn(p2.z, r.o.z));
+    const float az = comp(A, r.kz);
+    const float bz = comp(B, r.kz);
+    const float cz = comp(C, r.kz);
+    const float ax = __fsub_rn(comp(A, r.kx), __fmul_rn(r.sx, az));
+    const float ay = __fsub_rn(comp(A, r.ky), __fmul_rn(r.sy, az));
+    const float bx = __fsub_rn(comp(B, r.kx), __fmul_rn(r.sx, bz));
+    const float by = __fsub_rn(comp(B, r.ky), __fmul_rn(r.sy, bz));
+    const float cx = __fsub_rn(comp(C, r.kx), __fmul_rn(r.sx, cz));
+    const float cy = __fsub_rn(comp(C, r.ky), __fmul_rn(r.sy, cz));
+    float u = __fsub_rn(__fmul_rn(cx, by), __fmul_rn(cy, bx));
+    float v = __fsub_rn(__fmul_rn(ax, cy), __fmul_rn(ay, cx));
+    float w = __fsub_rn(__fmul_rn(bx, ay), __fmul_rn(by, ax));
+    if (u == 0.0f || v == 0.0f || w == 0.0f) {
+        const double du = static_cast<double>(cx) * by - static_cast<double>(cy) * bx;
+        const double dv = static_cast<double>(ax) * cy - static_cast<double>(ay) * cx;
+        const double dw = static_cast<double>(bx) * ay - static_cast<double>(by) * ax;
+        u = static_cast<float>(du);
+        v = static_cast<float>(dv);
+        w = static_cast<float>(dw);
+    }
+    const bool inside = (u >= 0.0f && v >= 0.0f && w >= 0.0f) || (u <= 0.0f && v <= 0.0f && w <= 0.0f);
+    if (!inside) {
+        return false;
+    }
+    const float det = __fadd_rn(__fadd_rn(u, v), w);
+    if (det == 0.0f) {
+        return false;
+    }
+    const float tz = __fadd_rn(__fadd_rn(__fmul_rn(u, __fmul_rn(r.sz, az)), __fmul_rn(v, __fmul_rn(r.sz, bz))),
+                               __fmul_rn(w, __fmul_rn(r.sz, cz)));
+    const float tt = __fdiv_rn(tz, det);
+    if (!(tmin < tt && tt < tmax)) {
+        return false;
+    }
+    t = tt;
+    b0 = __fdiv_rn(u, det);
+    b1 = __fdiv_rn(v, det);
+    b2 = __fdiv_rn(w, det);
+    return true;
+}
+
+ALB_DEV float3 affinePoint(const float* m, float3 p)
+{
+    return mk(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
+              m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+}
+ALB_DEV float3 affineVector(const float* m, float3 v)
+{
+    return mk(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
+              m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+// Transpose of the linear part times v: how a normal maps under the inverse map.
+ALB_DEV float3 affineTransposedVector(const float* m, float3 v)
+{
+    return mk(m[0] * v.x + m[4] * v.y + m[8] * v.z, m[1] * v.x + m[5] * v.y + m[9] * v.z,
+              m[2] * v.x + m[6] * v.y + m[10] * v.z);
+}
+
+ALB_DEV std::uint32_t leafRef(std::uint32_t first, std::uint32_t count)
+{
+    return kLeafBit | ((count - 1u) << 28) | first;
+}
+
+// Traverses the scene for the nearest hit in (tmin, tmax) (ANY = false), or for
+// any hit (ANY = true). On return `tmax` is the nearest hit distance. The stack
+// overflow bound (TLAS depth + BLAS depth + 2) is checked on the host before
+// launch, so pushes never exceed `stack_size`.
+template <bool ANY>
+ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
+                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag)
+{
+    if (s.tlas_root == kEmptyChild) {
+        return false;
+    }
+    TravRay r;
+    r.setup(origin, dir);
+    bool found = false;
+    int sp = 0;
+    std::uint32_t inst_pos = kNoPrim; // TLAS leaf position of the instance being traversed
+    std::uint32_t ref = s.tlas_root;
+    for (;;) {
+        if ((ref & kLeafBit) == 0u) {
+            const float4* np = reinterpret_cast<const float4*>(s.nodes + ref);
+            const float4 n0 = __ldg(np);
+            const float4 n1 = __ldg(np + 1);
+            const float4 n2 = __ldg(np + 2);
+            const uint4 n3 = __ldg(reinterpret_cast<const uint4*>(np + 3));
+            float e0, e1;
+            const bool h0 = n3.x != kEmptyChild && slabTest(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tmin, tmax, e0);
+            const bool h1 = n3.y != kEmptyChild && slabTest(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tmin, tmax, e1);
+            if (h0 && h1) {
+                if (sp >= stack_size) {
+                    atomicOr(error_flag, 1u);
+                    return found;
+                }
+                const bool second_first = ((r.neg >> n3.z) & 1u) != 0u;
+                const std::uint32_t near_ref = second_first ? n3.y : n3.x;
+                const std::uint32_t far_ref = second_first ? n3.x : n3.y;
+                const float far_entry = second_first ? e0 : e1;
+                stack[sp * stride] = make_uint2(far_ref, __float_as_uint(far_entry));
+                ++sp;
+                ref = near_ref;
+                continue;
+            }
+            if (h0 || h1) {
+                ref = h0 ? n3.x : n3.y;
+                continue;
+            }
+        } else {
+            const std::uint32_t first = ref & kLeafFirstMask;
+            const std::uint32_t count = ((ref >> 28) & 7u) + 1u;
+            if (inst_pos == kNoPrim) {
+                // TLAS leaf: spheres, scene triangles and instances, in leaf order.
+                bool entered = false;
+                for (std::uint32_t k = 0; k < count; ++k) {
+                    const std::uint32_t pos = first + k;
+                    const DevObject obj = s.objects[pos];
+                    if (pos == skip.light_object_pos) {
+                        continue;
+                    }
+                    if (obj.kind == kObjInstance) {
+                        if (sp + 2 > stack_size) {
+                            atomicOr(error_flag, 1u);
+                            return found;
+                        }
+                        if (k + 1 < count) {
+                            stack[sp * stride] = make_uint2(leafRef(pos + 1, count - k - 1), __float_as_uint(-INFINITY));
+                            ++sp;
+                        }
+                        stack[sp * stride] = make_uint2(kExitMarker, 0u);
+                        ++sp;
+                        const DevInstance& inst = s.instances[obj.index];
+                        r.setup(affinePoint(inst.to_object, origin), affineVector(inst.to_object, dir));
+                        inst_pos = pos;
+                        ref = inst.root;
+                        entered = true;
+                        break;
+                    }
+                    float t;
+                    float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
+                    bool h;
+                    if (obj.kind == kObjTriangle) {
+                        if (pos == skip.object_pos) {
+                            continue;
+                        }
+                        const float4* tp = reinterpret_cast<const float4*>(s.triangles + obj.index);
+                        h = r.usable && intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2);
+                    } else {
+                        int mode = kSphereTestBoth;
+                        if (pos == skip.object_pos) {
+                            if (skip.sphere_mode == kSphereSkipAll) {
+                                continue;
+                            }
+                            mode = skip.sphere_mode;
+                        }
+                        h = intersectSphere(r, s.spheres[obj.index], obj.kind == kObjSphereWide, tmin, tmax, mode, t);
+                    }
+                    if (h) {
+                        found = true;
+                        tmax = t;
+                        hit = {t, pos, obj.kind == kObjTriangle ? obj.index : kNoPrim, b0, b1, b2};
+                        if (ANY) {
+                            return true;
+                        }
+                    }
+                }
+                if (entered) {
+                    continue;
+                }
+            } else {
+                // BLAS leaf: triangles of the current instance's mesh.
+                if (r.usable) {
+                    for (std::uint32_t k = 0; k < count; ++k) {
+                        const std::uint32_t pos = first + k;
+                        if (pos == skip.tri_pos && inst_pos == skip.object_pos) {
+                            continue;
+                        }
+                        const float4* tp = reinterpret_cast<const float4*>(s.triangles + pos);
+                        float t, b0, b1, b2;
+                        if (intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2)) {
+                            found = true;
+                            tmax = t;
+                            hit = {t, inst_pos, pos, b0, b1, b2};
+                            if (ANY) {
+                                return true;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // Pop the next entry still worth visiting.
+        for (;;) {
+            if (sp == 0) {
+                return found;
+            }
+            --sp;
+            const uint2 e = stack[sp * stride];
+            if (e.x == kExitMarker) {
+                r.setup(origin, dir);
+                inst_pos = kNoPrim;
+                continue;
+            }
+            if (__uint_as_float(e.y) > tmax) {
+                continue;
+            }
+            ref = e.x;
+            break;
+        }
+    }
+}
+
+} // namespace albedo_b200

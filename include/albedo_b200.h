@@ -1,0 +1,203 @@
+/*
+ * albedo_b200: the C ABI of the B200 path tracer.
+ *
+ * A drop-in for the render path of anazli/albedo. The reference has no C or FFI
+ * API of its own; these entry points replace the C++ calls its app and tests
+ * make, one for one:
+ *
+ *   albedo_scene_load           readScene(path)                    src/albedo/scene/scene_file.hpp:142-146
+ *   albedo_scene_create/...     Scene::add / addAreaLight /        src/albedo/scene/scene.hpp:31-62
+ *                               addLight / setSky, TriangleMesh,   src/albedo/geometry/triangle_mesh.hpp:29-41
+ *                               MeshGeometry, MeshInstance,        src/albedo/geometry/mesh_geometry.hpp:30-33
+ *                               Transform factories                src/albedo/geometry/mesh_instance.hpp:24-27
+ *                                                                  src/albedo/core/transform.hpp:45-66
+ *   albedo_scene_set_camera     CameraSettings                     src/albedo/camera/perspective_camera.hpp:13-26
+ *   albedo_render               renderImage(RenderJob, PixelBuffer) src/albedo/render/render_image.hpp:36-49
+ *   albedo_render_host          renderImage with a host PixelBuffer src/albedo/render/render_image.hpp:36-49
+ *   albedo_trace_host           Scene::intersect                   src/albedo/scene/scene.hpp:69-75
+ *   albedo_occluded_host        Scene::occluded                    src/albedo/scene/scene.hpp:86-88
+ *
+ * Exceptions never cross the ABI: every call returns an albedo_status and leaves
+ * a message in a thread-local string (albedo_last_error). Status values map to
+ * the reference's exception types (std::invalid_argument, SceneParseError,
+ * std::runtime_error, std::out_of_range) plus device failures.
+ *
+ * Scenes are immutable once committed; any number of renders may then run on
+ * them concurrently on different streams. Accumulators follow PixelBuffer's
+ * Accumulator (src/albedo/image/pixel_buffer.hpp:53-57): an FP64 RGB sum and an
+ * int64 sample count per pixel, row-major from the top-left pixel; renders ADD
+ * samples to them, as renderImage adds to a PixelBuffer.
+ */
+#ifndef ALBEDO_B200_H
+#define ALBEDO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct albedo_scene albedo_scene;
+
+typedef enum albedo_status {
+    ALBEDO_OK = 0,
+    ALBEDO_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    ALBEDO_PARSE_ERROR = 2,      /* SceneParseError, with the line number in the message */
+    ALBEDO_IO_ERROR = 3,         /* std::runtime_error: a file cannot be opened or read */
+    ALBEDO_OUT_OF_RANGE = 4,     /* std::out_of_range: a mesh index past its table */
+    ALBEDO_DEVICE_ERROR = 5,     /* a CUDA call failed */
+    ALBEDO_OUT_OF_MEMORY = 6,    /* device or host allocation failed */
+    ALBEDO_UNSUPPORTED = 7,      /* beyond the device layout's limits (see message) */
+    ALBEDO_TRAVERSAL_ERROR = 8   /* a kernel reported a traversal stack overflow */
+} albedo_status;
+
+/* One per pixel; 32 bytes, as PixelBuffer's Accumulator. */
+typedef struct albedo_accumulator {
+    double r;
+    double g;
+    double b;
+    int64_t count;
+} albedo_accumulator;
+
+typedef enum albedo_estimator {
+    ALBEDO_PATH = 0,         /* PathEstimator: NEE + MIS + Russian roulette */
+    ALBEDO_SCATTER_ONLY = 1, /* ScatterOnlyEstimator (max_depth = max_scatter_count) */
+    ALBEDO_NORMALS = 2       /* NormalsEstimator */
+} albedo_estimator;
+
+typedef enum albedo_method {
+    ALBEDO_MEGAKERNEL = 0, /* one thread per pixel, samples in sequence */
+    ALBEDO_WAVEFRONT = 1   /* path slots advanced bounce by bounce through compacted queues */
+} albedo_method;
+
+/* RenderJob (src/albedo/render/render_image.hpp:17-32) minus the camera and scene. */
+typedef struct albedo_render_job {
+    int32_t width;
+    int32_t height;
+    int32_t samples_per_axis; /* n: n x n stratified samples per pixel */
+    int32_t estimator;        /* albedo_estimator */
+    uint64_t seed;
+    int32_t max_depth;        /* PathEstimator::max_depth (default 64) */
+    int32_t roulette_start;   /* PathEstimator::roulette_start (default 3) */
+    int32_t method;           /* albedo_method */
+    int32_t reserved;
+} albedo_render_job;
+
+/* BasicMaterial: kind 0 diffuse (texture 0 constant color a, 1 checker even a /
+ * odd b / frequency, 2 Perlin low a / high b / scale / veins), kind 1 conductor
+ * (eta a, k b, roughness), kind 2 dielectric (ior, roughness). */
+typedef struct albedo_basic_material {
+    int32_t kind;
+    int32_t texture;
+    double a[3];
+    double b[3];
+    double frequency_or_scale;
+    double veins;
+    double ior;
+    double roughness;
+} albedo_basic_material;
+
+/* Material: a basic material, or (mix != 0) MixMaterial of two basic ones. */
+typedef struct albedo_material {
+    int32_t mix;
+    int32_t reserved;
+    albedo_basic_material first;
+    albedo_basic_material second;
+    double scale;
+    double veins;
+    double threshold;
+} albedo_material;
+
+typedef struct albedo_scene_info {
+    int64_t objects;
+    int64_t lights;
+    int64_t triangles;       /* scene triangles plus every mesh's triangles */
+    int64_t nodes;           /* device BVH nodes (child-box form) */
+    int64_t device_bytes;    /* device memory held by the committed scene */
+    int32_t stack_need;      /* traversal stack entries a query can need */
+    int32_t stack_capacity;  /* entries of the kernel variant chosen */
+} albedo_scene_info;
+
+const char* albedo_last_error(void);
+
+/* Scene input. albedo_scene_load = albedo_scene_read + albedo_scene_commit. */
+int albedo_scene_load(const char* path, albedo_scene** out);
+/* Reads a scene file and builds its hierarchy and device tables on the host
+ * only (no device needed); commit uploads it. */
+int albedo_scene_read(const char* path, albedo_scene** out);
+int albedo_scene_create(albedo_scene** out);
+void albedo_scene_destroy(albedo_scene* scene);
+int albedo_scene_set_camera(albedo_scene* scene, const double look_from[3], const double look_at[3],
+                            const double up[3], double vertical_fov_degrees);
+int albedo_scene_add_material(albedo_scene* scene, const albedo_material* material, uint32_t* out_material);
+int albedo_scene_add_sphere(albedo_scene* scene, const double center[3], double radius, uint32_t material,
+                            uint32_t* out_object);
+int albedo_scene_add_area_light(albedo_scene* scene, const double center[3], double radius,
+                                const double radiance[3], uint32_t material, uint32_t* out_object);
+int albedo_scene_add_point_light(albedo_scene* scene, const double position[3], const double intensity[3]);
+int albedo_scene_set_sky(albedo_scene* scene, const double nadir[3], const double zenith[3]);
+/* A shared mesh (TriangleMesh + MeshGeometry): positions (3 per vertex), faces
+ * (3 indices each), optional texture coordinates (2 each) and texture faces
+ * (0 or face_count of them). smooth != 0 shades with averaged vertex normals. */
+int albedo_scene_add_mesh(albedo_scene* scene, const double* positions, int64_t position_count,
+                          const uint32_t* faces, int64_t face_count, const double* texture_coordinates,
+                          int64_t texture_coordinate_count, const uint32_t* texture_faces,
+                          int64_t texture_face_count, int32_t smooth, uint32_t* out_mesh);
+/* A MeshInstance: object-to-world as a 3x4 row-major affine matrix and its exact
+ * inverse, as Transform keeps both. */
+int albedo_scene_add_instance(albedo_scene* scene, uint32_t mesh, const double to_world[12],
+                              const double to_object[12], uint32_t material, uint32_t* out_object);
+/* Scene::add(TriangleMesh, material): every triangle its own object. */
+int albedo_scene_add_triangles(albedo_scene* scene, const double* positions, int64_t position_count,
+                               const uint32_t* faces, int64_t face_count, uint32_t material);
+/* Builds the TLAS and the device tables on the host (idempotent; no device). */
+int albedo_scene_prepare(albedo_scene* scene);
+/* Prepares if needed, then uploads the scene to the current CUDA device. */
+int albedo_scene_commit(albedo_scene* scene);
+/* The host-side scene tables (an albedo_b200::HostScene) of a prepared scene,
+ * for test code built against the same headers; valid until destroy. */
+const void* albedo_scene_host_view(const albedo_scene* scene);
+int albedo_scene_get_info(const albedo_scene* scene, albedo_scene_info* out);
+
+/* Rendering. albedo_render is stream-ordered and asynchronous: `accumulators`
+ * is a device array of width*height entries; `stream` is a cudaStream_t (NULL:
+ * the default stream). Call albedo_scene_check after synchronizing to collect a
+ * kernel-reported error. albedo_render_host takes a host array, copies it in,
+ * renders, copies it back and synchronizes. */
+int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
+                  void* stream);
+int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators);
+/* Renders only the listed pixels (x, y pairs) into one host accumulator each,
+ * optionally also returning per-pixel sums of squared samples (3 doubles each). */
+int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
+                              int64_t pixel_count, albedo_accumulator* accumulators, double* sum_squares);
+/* Reads and clears the scene's kernel error flag (synchronizes the device). */
+int albedo_scene_check(const albedo_scene* scene);
+
+/* Ray queries over host arrays of rays (origin xyz, direction xyz as floats).
+ * trace: hit flag, t, object id (add order), triangle id within its mesh (-1 if
+ * none), and optionally point / normal / shading normal (3 floats each) and
+ * front-face flags. occluded: any hit in (0, t_max[i]). */
+int albedo_trace_host(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                      int32_t* hit, float* t, int32_t* object, int32_t* triangle, float* point, float* normal,
+                      float* shading_normal, int32_t* front);
+int albedo_occluded_host(const albedo_scene* scene, const float* rays, const float* t_max, int64_t count,
+                         int32_t* occluded);
+
+/* Probes of device arithmetic for parity tests (host arrays). */
+int albedo_probe_pixel_stream(uint64_t seed, int32_t x, int32_t y, int32_t width, int32_t count, uint32_t* out_u32,
+                              float* out_real);
+int albedo_probe_lobe_eval(int32_t kind, const float* params, const float* wo_wi, int32_t count, float* out_f,
+                           float* out_pdf);
+int albedo_probe_lobe_sample(int32_t kind, const float* params, const float* inputs, int32_t count,
+                             int32_t* out_valid, float* out_direction, float* out_weight, float* out_pdf,
+                             int32_t* out_specular);
+int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, float* out_turbulence);
+int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film,
+                             int32_t count, float* out_rays);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ALBEDO_B200_H */
