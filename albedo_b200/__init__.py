@@ -296,10 +296,31 @@ def render_image(scene: Scene, job: RenderJob, image: PixelBuffer) -> None:
     _raise(library().albedo_render_host(scene.handle, byref(c), image.pixels.ctypes.data_as(c_void_p)))
 
 
+def render_image_ptr(scene: Scene, job: RenderJob, host_accumulators_ptr: int) -> None:
+    """renderImage into a host array (pinned or pageable) of width*height accumulators."""
+    c = job.to_c()
+    _raise(library().albedo_render_host(scene.handle, byref(c), c_void_p(host_accumulators_ptr)))
+
+
 def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: int = 0) -> None:
     """Stream-ordered render into a device array of width*height accumulators."""
     c = job.to_c()
     _raise(library().albedo_render(scene.handle, byref(c), c_void_p(accumulators_ptr), c_void_p(stream)))
+
+
+def work_counts(scene: Scene, job: RenderJob) -> dict:
+    """Traversal work of one render of `job` (path estimator), counted on the device."""
+    out = (ctypes.c_int64 * 5)()
+    c = job.to_c()
+    _raise(library().albedo_render_work_counts(scene.handle, byref(c), out))
+    return dict(zip(["boxes", "triangles", "spheres", "instances", "rays"], [int(v) for v in out]))
+
+
+def algorithmic_bytes(counts: dict) -> int:
+    """Bytes a traversal must read for the counted work: 32 per box tested, 48 per
+    triangle, 32 per sphere (its 16-byte record and its object entry), 96 per
+    instance entered (its two 3x4 FP32 transforms)."""
+    return 32 * counts["boxes"] + 48 * counts["triangles"] + 32 * counts["spheres"] + 96 * counts["instances"]
 
 
 def render_pixels(scene: Scene, job: RenderJob, pixels: np.ndarray, with_squares: bool = False):

@@ -63,6 +63,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render_host": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p]),
     "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
     "albedo_scene_check": (c_int32, [c_void_p]),
+    "albedo_render_work_counts": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(c_int64)]),
     "albedo_trace_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, _I, _F, _I, _I, _F, _F, _F, _I]),
     "albedo_occluded_host": (c_int32, [c_void_p, _F, _F, c_int64, _I]),
     "albedo_probe_pixel_stream": (c_int32, [c_uint64, c_int32, c_int32, c_int32, c_int32, _U, _F]),

@@ -584,6 +584,30 @@ int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job
     });
 }
 
+int albedo_render_work_counts(const albedo_scene* scene, const albedo_render_job* job, int64_t* out_counts)
+{
+    return guarded([&] {
+        const RenderArgs args{renderArgsFor(*scene, *job)};
+        const std::size_t pixels{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height)};
+        DeviceBuffer accum{pixels * sizeof(PixelAccum)};
+        DeviceBuffer totals{5 * sizeof(unsigned long long)};
+        check(cudaMemset(accum.ptr, 0, accum.bytes), "cudaMemset");
+        check(cudaMemset(totals.ptr, 0, totals.bytes), "cudaMemset");
+        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
+        check(launchMegakernelCounting(scene->dev, camera, args, accum.as<PixelAccum>(),
+                                       scene->error_flag.as<unsigned int>(), scene->stack_capacity,
+                                       totals.as<unsigned long long>(), nullptr),
+              "counting launch");
+        check(cudaDeviceSynchronize(), "counting");
+        unsigned long long host[5]{};
+        check(cudaMemcpy(host, totals.ptr, sizeof(host), cudaMemcpyDeviceToHost), "download");
+        for (int i{0}; i < 5; ++i) {
+            out_counts[i] = static_cast<int64_t>(host[i]);
+        }
+        scene->collectKernelError();
+    });
+}
+
 int albedo_scene_check(const albedo_scene* scene)
 {
     return guarded([&] {

@@ -20,19 +20,20 @@ struct TraceContext {
     int stride;
     int capacity;
     unsigned int* error_flag;
+    TraversalCounts* counts; // null except in the counting variants
 };
 
 ALB_DEV bool closestHit(const DevScene& s, const TraceContext& c, float3 o, float3 d, const SkipRule& skip,
                         TraceHit& hit)
 {
     float tmax = INFINITY;
-    return traceScene<false>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag);
+    return traceScene<false>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag, c.counts);
 }
 
 ALB_DEV bool occluded(const DevScene& s, const TraceContext& c, float3 o, float3 d, float tmax, const SkipRule& skip)
 {
     TraceHit hit;
-    return traceScene<true>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag);
+    return traceScene<true>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag, c.counts);
 }
 
 // Next-event estimation from one uniformly chosen light, MIS-weighted, scaled

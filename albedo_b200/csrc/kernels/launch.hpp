@@ -41,6 +41,13 @@ int stackCapacityFor(std::uint32_t stack_need);
 cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
                              unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
 
+// The megakernel (path estimator) counting its traversal work into
+// totals[0..4] = child boxes tested, triangles tested, spheres tested,
+// instances entered, queries traced. Not used for timing.
+cudaError_t launchMegakernelCounting(const DevScene& scene, const DevCamera& camera, const RenderArgs& args,
+                                     PixelAccum* accum, unsigned int* error_flag, int stack_capacity,
+                                     unsigned long long* totals, cudaStream_t stream);
+
 // Ray queries: rays are 6 floats (origin, direction). Closest hit in (t_min,
 // t_max): hit flag, t, object id, triangle id within its mesh (-1 for spheres),
 // point, geometric normal facing the ray, shading normal, front-face flag.

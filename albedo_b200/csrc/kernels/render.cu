@@ -15,13 +15,15 @@ constexpr int kBlock = 128;
 constexpr int kTileW = 16;
 constexpr int kTileH = 8;
 
-template <int STACK, int EST>
+template <int STACK, int EST, bool COUNT = false>
 __global__ void __launch_bounds__(kBlock) megakernel(const DevScene scene, const DevCamera camera,
                                                      const RenderArgs args, PixelAccum* accum,
-                                                     unsigned int* error_flag)
+                                                     unsigned int* error_flag,
+                                                     unsigned long long* totals = nullptr)
 {
     extern __shared__ uint2 stack[];
-    const TraceContext ctx{stack + threadIdx.x, kBlock, STACK, error_flag};
+    TraversalCounts counts{0, 0, 0, 0, 0};
+    const TraceContext ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
         slot = blockIdx.x * kBlock + threadIdx.x;
@@ -74,6 +76,13 @@ __global__ void __launch_bounds__(kBlock) megakernel(const DevScene scene, const
         args.sum_squares[3 * slot + 1] += qg;
         args.sum_squares[3 * slot + 2] += qb;
     }
+    if constexpr (COUNT) {
+        atomicAdd(totals + 0, counts.boxes);
+        atomicAdd(totals + 1, counts.triangles);
+        atomicAdd(totals + 2, counts.spheres);
+        atomicAdd(totals + 3, counts.instances);
+        atomicAdd(totals + 4, counts.rays);
+    }
 }
 
 template <int STACK>
@@ -97,7 +106,7 @@ __global__ void __launch_bounds__(kBlock) traceKernel(const DevScene scene, cons
     }
     Surface sf;
     resolveHit(scene, o, d, hit, sf);
-    out.t[i] = hit.t;
+    out.t[i] = static_cast<float>(refinedDistance(scene, o, d, hit));
     out.object[i] = static_cast<int>(sf.object_id);
     out.triangle[i] = -1;
     const DevObject obj = scene.objects[hit.obj_pos];
@@ -197,6 +206,37 @@ cudaError_t launchMegaStack(const DevScene& scene, const DevCamera& camera, cons
 }
 
 } // namespace
+
+cudaError_t launchMegakernelCounting(const DevScene& scene, const DevCamera& camera, const RenderArgs& args,
+                                     PixelAccum* accum, unsigned int* error_flag, int stack_capacity,
+                                     unsigned long long* totals, cudaStream_t stream)
+{
+    int blocks;
+    if (args.pixels != nullptr) {
+        blocks = (args.pixel_count + kBlock - 1) / kBlock;
+    } else {
+        blocks = ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
+    }
+    if (blocks == 0) {
+        return cudaSuccess;
+    }
+    static bool configured[2] = {false, false};
+    cudaError_t e;
+    if (stack_capacity == 32) {
+        e = launchWithStack(megakernel<32, kEstimatorPath, true>, 32, blocks, stream, configured[0]);
+        if (e == cudaSuccess) {
+            megakernel<32, kEstimatorPath, true>
+                <<<blocks, kBlock, stackBytes(32), stream>>>(scene, camera, args, accum, error_flag, totals);
+        }
+    } else {
+        e = launchWithStack(megakernel<64, kEstimatorPath, true>, 64, blocks, stream, configured[1]);
+        if (e == cudaSuccess) {
+            megakernel<64, kEstimatorPath, true>
+                <<<blocks, kBlock, stackBytes(64), stream>>>(scene, camera, args, accum, error_flag, totals);
+        }
+    }
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
 
 int stackCapacityFor(std::uint32_t stack_need)
 {

@@ -52,6 +52,70 @@ ALB_DEV float3 blendedNormal(const DevTriangle& tri, const DevTriangleAttr& at, 
     return normalized(blended);
 }
 
+// The reported hit's distance recomputed once in FP64 (traversal decided which
+// primitive is nearest in FP32): the sphere root closest to the FP32 one, or the
+// watertight triangle distance, with instance rays taken to object space in FP64.
+ALB_DEV double refinedDistance(const DevScene& s, float3 origin, float3 dir, const TraceHit& h)
+{
+    const DevObject obj = s.objects[h.obj_pos];
+    const double ox = origin.x, oy = origin.y, oz = origin.z;
+    const double dx = dir.x, dy = dir.y, dz = dir.z;
+    if (obj.kind == kObjSphere || obj.kind == kObjSphereWide) {
+        const DevSphere sp = s.spheres[obj.index];
+        const double cx = ox - sp.cx, cy = oy - sp.cy, cz = oz - sp.cz;
+        const double a = dx * dx + dy * dy + dz * dz;
+        const double hh = dx * cx + dy * cy + dz * cz;
+        const double r2 = static_cast<double>(sp.r) * sp.r;
+        const double c = (cx * cx + cy * cy + cz * cz) - r2;
+        const double k = hh / a;
+        const double lx = cx - dx * k, ly = cy - dy * k, lz = cz - dz * k;
+        const double disc = fmax(a * (r2 - (lx * lx + ly * ly + lz * lz)), 0.0);
+        const double q = -(hh + copysign(sqrt(disc), hh));
+        if (q == 0.0) {
+            return 0.0;
+        }
+        const double r0 = q / a;
+        const double r1 = c / q;
+        return fabs(r0 - h.t) < fabs(r1 - h.t) ? r0 : r1;
+    }
+    double px = ox, py = oy, pz = oz, qx = dx, qy = dy, qz = dz;
+    if (obj.kind == kObjInstance) {
+        const float* m = s.instances[obj.index].to_object;
+        px = m[0] * ox + m[1] * oy + m[2] * oz + m[3];
+        py = m[4] * ox + m[5] * oy + m[6] * oz + m[7];
+        pz = m[8] * ox + m[9] * oy + m[10] * oz + m[11];
+        qx = m[0] * dx + m[1] * dy + m[2] * dz;
+        qy = m[4] * dx + m[5] * dy + m[6] * dz;
+        qz = m[8] * dx + m[9] * dy + m[10] * dz;
+    }
+    const DevTriangle tri = s.triangles[h.tri_pos];
+    const double mx = fabs(qx), my = fabs(qy), mz = fabs(qz);
+    const int kz = mx > my ? (mx > mz ? 0 : 2) : (my > mz ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const double q3[3] = {qx, qy, qz};
+    if (q3[kz] < 0.0) {
+        const int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    const double sx = q3[kx] / q3[kz], sy = q3[ky] / q3[kz], sz = 1.0 / q3[kz];
+    const double A[3] = {tri.v0x - px, tri.v0y - py, tri.v0z - pz};
+    const double B[3] = {tri.v1x - px, tri.v1y - py, tri.v1z - pz};
+    const double C[3] = {tri.v2x - px, tri.v2y - py, tri.v2z - pz};
+    const double ax = A[kx] - sx * A[kz], ay = A[ky] - sy * A[kz];
+    const double bx = B[kx] - sx * B[kz], by = B[ky] - sy * B[kz];
+    const double cx = C[kx] - sx * C[kz], cy = C[ky] - sy * C[kz];
+    const double u = cx * by - cy * bx;
+    const double v = ax * cy - ay * cx;
+    const double w = bx * ay - by * ax;
+    const double det = u + v + w;
+    if (det == 0.0) {
+        return h.t;
+    }
+    return (u * (sz * A[kz]) + v * (sz * B[kz]) + w * (sz * C[kz])) / det;
+}
+
 // Scene::intersect's record (scene/scene.cpp:107-133) for a TraceHit.
 ALB_DEV void resolveHit(const DevScene& s, float3 origin, float3 dir, const TraceHit& h, Surface& out)
 {
@@ -67,8 +131,13 @@ ALB_DEV void resolveHit(const DevScene& s, float3 origin, float3 dir, const Trac
     float3 ns;
     if (obj.kind == kObjSphere || obj.kind == kObjSphereWide) {
         const DevSphere sp = s.spheres[obj.index];
-        out.p = origin + dir * h.t;
-        n = normalized(out.p - mk(sp.cx, sp.cy, sp.cz));
+        // The hit point from the FP64 distance: FP32 o + t d loses the walls' 1e4-scale digits.
+        const double t = refinedDistance(s, origin, dir, h);
+        out.p = mk(static_cast<float>(origin.x + dir.x * t), static_cast<float>(origin.y + dir.y * t),
+                   static_cast<float>(origin.z + dir.z * t));
+        n = normalized(mk(static_cast<float>(origin.x + dir.x * t - sp.cx),
+                          static_cast<float>(origin.y + dir.y * t - sp.cy),
+                          static_cast<float>(origin.z + dir.z * t - sp.cz)));
         ns = n;
         out.sphere_outward = n;
         out.is_sphere = true;

@@ -41,6 +41,16 @@ struct SkipRule {
     ALB_DEV static SkipRule none() { return {kNoPrim, kNoPrim, kSphereTestBoth, kNoPrim}; }
 };
 
+// Work one query did, for the algorithmic-bytes figure: child boxes tested,
+// triangles and spheres tested, instances entered, queries traced.
+struct TraversalCounts {
+    unsigned long long boxes;
+    unsigned long long triangles;
+    unsigned long long spheres;
+    unsigned long long instances;
+    unsigned long long rays;
+};
+
 struct TraceHit {
     float t;
     std::uint32_t obj_pos; // TLAS leaf position of the object hit
@@ -261,8 +271,12 @@ ALB_DEV std::uint32_t leafRef(std::uint32_t first, std::uint32_t count)
 // launch, so pushes never exceed `stack_size`.
 template <bool ANY>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
-                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag)
+                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
+                        TraversalCounts* counts = nullptr)
 {
+    if (counts != nullptr) {
+        counts->rays += 1;
+    }
     if (s.tlas_root == kEmptyChild) {
         return false;
     }
@@ -279,6 +293,9 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
             const float4 n1 = __ldg(np + 1);
             const float4 n2 = __ldg(np + 2);
             const uint4 n3 = __ldg(reinterpret_cast<const uint4*>(np + 3));
+            if (counts != nullptr) {
+                counts->boxes += (n3.x != kEmptyChild ? 1u : 0u) + (n3.y != kEmptyChild ? 1u : 0u);
+            }
             float e0, e1;
             const bool h0 = n3.x != kEmptyChild && slabTest(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tmin, tmax, e0);
             const bool h1 = n3.y != kEmptyChild && slabTest(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tmin, tmax, e1);
@@ -324,6 +341,9 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
                         stack[sp * stride] = make_uint2(kExitMarker, 0u);
                         ++sp;
                         const DevInstance& inst = s.instances[obj.index];
+                        if (counts != nullptr) {
+                            counts->instances += 1;
+                        }
                         r.setup(affinePoint(inst.to_object, origin), affineVector(inst.to_object, dir));
                         inst_pos = pos;
                         ref = inst.root;
@@ -338,6 +358,9 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
                             continue;
                         }
                         const float4* tp = reinterpret_cast<const float4*>(s.triangles + obj.index);
+                        if (counts != nullptr) {
+                            counts->triangles += 1;
+                        }
                         h = r.usable && intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2);
                     } else {
                         int mode = kSphereTestBoth;
@@ -346,6 +369,9 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
                                 continue;
                             }
                             mode = skip.sphere_mode;
+                        }
+                        if (counts != nullptr) {
+                            counts->spheres += 1;
                         }
                         h = intersectSphere(r, s.spheres[obj.index], obj.kind == kObjSphereWide, tmin, tmax, mode, t);
                     }
@@ -371,6 +397,9 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
                         }
                         const float4* tp = reinterpret_cast<const float4*>(s.triangles + pos);
                         float t, b0, b1, b2;
+                        if (counts != nullptr) {
+                            counts->triangles += 1;
+                        }
                         if (intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2)) {
                             found = true;
                             tmax = t;

@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Throughput of the path-tracing hot path on one or more B200s.
+
+Workload (the instanced-mesh configuration): three instances of a seeded trefoil
+tube (256 x 32 ring vertices, 16,384 smooth triangles, uniform scale 0.8-1.2,
+seeded y-rotation) in gold, glass and copper on a 2-triangle checker floor inside
+a room of radius-1e4 wall spheres, with an area light, a point light and a sky;
+960 x 540 pixels, 8 x 8 = 64 stratified samples per pixel, PathEstimator
+max_depth 10, roulette_start 3, seed 0. One step renders the full frame:
+33,177,600 paths.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--method megakernel|wavefront]
+
+Prints one JSON line. `value` is whole-job Mpaths/s with the scene and the
+accumulators resident in HBM, timed with CUDA events per step and L2 flushed
+(a 256 MiB write) between steps. `e2e` is the same metric through the C-ABI
+call that takes host (pinned) accumulators: the host-to-device copy, the render
+and the device-to-host copy of the frame's accumulators are inside each timed
+step. `roofline` divides the algorithmic bytes of one launch (32 B per BVH box
+tested, 48 B per triangle, 32 B per sphere, 96 B per instance entered, counted
+on the device in an untimed counting launch) by the launch's measured time.
+`cpu_baseline` is the reference renderer, built from its own sources, timed on
+this machine's host cores over a band of rows of the same frame.
+
+Under torchrun (N > 1) every rank renders its own replica of the frame (the path
+does not shard across GPUs without changing per-pixel random streams, so the
+runs are replicas); the time is the maximum over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WIDTH, HEIGHT, SAMPLES_PER_AXIS, MAX_DEPTH, ROULETTE_START, SEED = 960, 540, 8, 10, 3, 0
+PATHS_PER_STEP = WIDTH * HEIGHT * SAMPLES_PER_AXIS * SAMPLES_PER_AXIS
+METRIC = "Mpaths/s at matched RMSE vs plain GPU + host CPU; p50/p99 render latency"
+WORKLOAD = "trefoil_x3_instanced_960x540_64spp_depth10"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--method", choices=["megakernel", "wavefront"], default="megakernel")
+    return p.parse_args()
+
+
+def config(method: str, n_gpus: int) -> dict:
+    return {"workload": WORKLOAD, "resolution": [WIDTH, HEIGHT], "samples_per_axis": SAMPLES_PER_AXIS,
+            "spp": SAMPLES_PER_AXIS ** 2, "max_depth": MAX_DEPTH, "roulette_start": ROULETTE_START, "seed": SEED,
+            "paths_per_step": PATHS_PER_STEP, "method": method,
+            "parallelism": "replicas" if n_gpus > 1 else "single",
+            "l2": "flushed between steps (256 MiB write)"}
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self) -> dict | None:
+        rows = []
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append({"sm": float(parts[1]), "max": float(parts[2]), "power": float(parts[3]),
+                             "hw_slowdown": parts[5], "hw_thermal": parts[6], "sw_thermal": parts[7],
+                             "sw_power_cap": parts[8]})
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw_slowdown", "hw_slowdown"), ("hw_thermal", "hw_thermal_slowdown"),
+                              ("sw_thermal", "sw_thermal_slowdown"), ("sw_power_cap", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["max"] for r in rows),
+                "power_w_max": max(r["power"] for r in rows), "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def measured_peaks() -> dict:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return {}
+
+
+def profiled_traffic() -> tuple[float | None, str | None]:
+    """DRAM bytes per launch of the megakernel from the committed ncu summary."""
+    path = ROOT / "profiles" / "megakernel_trefoil_960x540.txt"
+    if not path.exists():
+        return None, None
+    for line in path.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0]), path.name
+    return None, None
+
+
+def cpu_baseline_sample(scene_path: Path, target_seconds: float = 12.0) -> dict:
+    """The reference renderer on all host cores over a band of full-spp rows."""
+    from oracle import reference as ref
+
+    scene = ref.RefScene(scene_path)
+    threads = ref.threads()
+
+    def run(rows: int) -> float:
+        y0 = HEIGHT // 2 - rows // 2
+        xs, ys = np.meshgrid(np.arange(WIDTH), np.arange(y0, y0 + rows))
+        pixels = np.stack([xs.ravel(), ys.ravel()], axis=1)
+        start = time.perf_counter()
+        scene.render_pixels(WIDTH, HEIGHT, SAMPLES_PER_AXIS, pixels, seed=SEED, max_depth=MAX_DEPTH,
+                            roulette_start=ROULETTE_START, nthreads=threads)
+        return time.perf_counter() - start
+
+    probe_rows = 2
+    probe = run(probe_rows)
+    rows = int(np.clip(probe_rows * target_seconds / max(probe, 1e-3), probe_rows, HEIGHT))
+    seconds = run(rows)
+    paths = rows * WIDTH * SAMPLES_PER_AXIS ** 2
+    return {"value": paths / seconds / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "reference",
+            "sample": f"{rows} full rows x {WIDTH} px x {SAMPLES_PER_AXIS ** 2} spp through the middle of the frame "
+                      f"({paths} paths, {seconds:.1f} s), reference renderImage pixel loop on {threads} threads"}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from albedo_b200 import scenes
+
+    with tempfile.TemporaryDirectory() as tmp:
+        scene_path = scenes.trefoil_scene(Path(tmp))
+        for _ in range(args.warmup):
+            cpu_baseline_sample(scene_path, target_seconds=2.0)
+        values = []
+        samples = []
+        for _ in range(args.steps):
+            s = cpu_baseline_sample(scene_path, target_seconds=6.0)
+            values.append(s["value"])
+            samples.append(s)
+        value = statistics.median(values)
+        base = samples[-1]
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": PATHS_PER_STEP / value / 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded scene files)", "config": config("reference CPU renderer", 1),
+                "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": base["cores"], "kind": "reference",
+                                 "sample": "each step: " + base["sample"]},
+                "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import albedo_b200 as ab
+    from albedo_b200 import scenes
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
+    tmp = tempfile.TemporaryDirectory()
+    scene_path = scenes.trefoil_scene(Path(tmp.name))
+    scene = ab.Scene.load(scene_path)
+    job = ab.RenderJob(WIDTH, HEIGHT, samples_per_axis=SAMPLES_PER_AXIS, seed=SEED, max_depth=MAX_DEPTH,
+                       roulette_start=ROULETTE_START, method=method)
+    accum = torch.zeros((WIDTH * HEIGHT, 4), dtype=torch.float64, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    for _ in range(args.warmup):
+        ab.render_device(scene, job, accum.data_ptr())
+    torch.cuda.synchronize()
+    scene.check()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            starts[i].record()
+            ab.render_device(scene, job, accum.data_ptr())
+            ends[i].record()
+        torch.cuda.synchronize()
+    barrier()
+    scene.check()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
+    total_s = float(total_ms.item()) / 1e3
+    value = world * PATHS_PER_STEP * args.steps / total_s / 1e6
+
+    # End to end through the host-buffer entry point, pinned accumulators.
+    host_accum = torch.zeros((WIDTH * HEIGHT, 4), dtype=torch.float64).pin_memory()
+    ab.render_image_ptr(scene, job, host_accum.data_ptr())
+    e2e_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(i & 0xFF)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        ab.render_image_ptr(scene, job, host_accum.data_ptr())
+        e.record()
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+    barrier()
+    e2e_total = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
+    e2e_value = world * PATHS_PER_STEP * args.steps / (float(e2e_total.item()) / 1e3) / 1e6
+    frame_bytes = WIDTH * HEIGHT * 32
+
+    if rank == 0:
+        counts = ab.work_counts(scene, job)
+        alg_bytes = ab.algorithmic_bytes(counts)
+        launch_s = statistics.mean(step_ms) / 1e3
+        peaks = measured_peaks()
+        peak = peaks.get("hbm_gbs")
+        peak_source = "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if peak else "fallback 6650 GB/s"
+        peak = peak or 6650.0
+        achieved = alg_bytes / launch_s / 1e9
+        traffic, traffic_source = profiled_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files in the reference's formats)",
+            "config": config(args.method, world),
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+            "mrays_per_s": world * counts["rays"] * args.steps / total_s / 1e6,
+            "gpu_launches": args.steps,
+            "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": frame_bytes,
+                    "d2h_bytes_per_step": frame_bytes},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "megakernel<32, path>", "algorithmic_bytes_per_launch": alg_bytes,
+                         "work_per_launch": counts, "peak_source": peak_source,
+                         "traffic_source": traffic_source},
+            "clocks": clocks.summary(),
+        }
+        if world == 1:
+            line["cpu_baseline"] = cpu_baseline_sample(scene_path)
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -171,6 +171,10 @@ int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, 
  * optionally also returning per-pixel sums of squared samples (3 doubles each). */
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
                               int64_t pixel_count, albedo_accumulator* accumulators, double* sum_squares);
+/* Renders the job once (path estimator, into scratch accumulators) while counting
+ * traversal work: out_counts[0..4] = child boxes tested, triangles tested,
+ * spheres tested, instances entered, ray queries traced. Synchronous. */
+int albedo_render_work_counts(const albedo_scene* scene, const albedo_render_job* job, int64_t* out_counts);
 /* Reads and clears the scene's kernel error flag (synchronizes the device). */
 int albedo_scene_check(const albedo_scene* scene);
 
