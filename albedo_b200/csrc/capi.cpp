@@ -232,6 +232,7 @@ struct albedo_scene {
         dev.materials = static_cast<const DevMaterial*>(add(upload(image.materials)));
         dev.lights = static_cast<const DevLight*>(add(upload(image.lights)));
         dev.object_light = static_cast<const std::int32_t*>(add(upload(image.object_light)));
+        dev.instance_to_object64 = static_cast<const double*>(add(upload(image.instance_to_object64)));
         dev.tlas_root = image.tlas_root;
         dev.light_count = static_cast<std::uint32_t>(image.lights.size());
         dev.sky_light = image.sky_light;

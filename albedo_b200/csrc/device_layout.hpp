@@ -146,6 +146,7 @@ struct DevScene {
     const DevMaterial* materials;
     const DevLight* lights;
     const std::int32_t* object_light;  // object id -> area light index or -1
+    const double* instance_to_object64; // per instance, the exact FP64 world-to-object 3x4 rows (hit refinement)
     std::uint32_t tlas_root;           // node index of the TLAS root (kEmptyChild if no objects)
     std::uint32_t light_count;
     std::int32_t sky_light;            // light index of the sky, or -1

@@ -276,6 +276,13 @@ DeviceImage flattenScene(const HostScene& scene)
         d.root = mesh_root[inst.mesh];
         d.mesh = inst.mesh;
         image.instances.push_back(d);
+        const Affine& back{inst.to_object.forward()};
+        for (int row{0}; row < 3; ++row) {
+            image.instance_to_object64.push_back(back.linear[row][0]);
+            image.instance_to_object64.push_back(back.linear[row][1]);
+            image.instance_to_object64.push_back(back.linear[row][2]);
+            image.instance_to_object64.push_back(row == 0 ? back.offset.x : (row == 1 ? back.offset.y : back.offset.z));
+        }
     }
     for (const MaterialDesc& m : scene.materials) {
         DevMaterial d{};

@@ -18,6 +18,7 @@ struct DeviceImage {
     std::vector<DevMaterial> materials;
     std::vector<DevLight> lights;
     std::vector<std::int32_t> object_light;
+    std::vector<double> instance_to_object64;
     // Leaf position of each object id, and the triangle-table base of each mesh.
     std::vector<std::uint32_t> object_position;
     std::vector<std::uint32_t> mesh_triangle_base;

@@ -76,133 +76,195 @@ ALB_DEV float3 sampleDirectLight(const DevScene& s, const TraceContext& c, const
     return f * ls.radiance * (cos_theta * weight / light_pdf);
 }
 
-ALB_DEV float3 pathRadiance(const DevScene& s, const TraceContext& c, float3 o, float3 d, Pcg32& g, int max_depth,
-                           int roulette_start)
+// The state of one path between bounces: PathEstimator::radiance's loop
+// variables (estimator/path_estimator.cpp:155-160) plus the skip rule of the ray.
+struct PathState {
+    float3 o;
+    float3 d;
+    float3 throughput;
+    float3 result;
+    float3 arrival_origin;
+    float arrival_pdf;
+    int depth;
+    bool arrival_specular;
+    SkipRule skip;
+};
+
+ALB_DEV void beginPath(PathState& p, float3 o, float3 d)
 {
-    float3 throughput = gray(1.0f);
-    float3 result = gray(0.0f);
-    float3 arrival_origin = o;
-    float arrival_pdf = 0.0f;
-    bool arrival_specular = true;
-    SkipRule skip = SkipRule::none();
-    const float choice = s.light_count > 0u ? 1.0f / static_cast<float>(s.light_count) : INFINITY;
-    for (int depth = 0;; ++depth) {
-        TraceHit hit;
-        if (!closestHit(s, c, o, d, skip, hit)) {
-            if (s.sky_light >= 0) {
-                float3 e = skyRadiance(s.lights[s.sky_light], d);
-                if (!isBlack(e) && !arrival_specular) {
-                    e = e * powerHeuristic(arrival_pdf, choice * uniformSpherePdf());
-                }
-                result = result + throughput * e;
-            }
-            return result;
-        }
-        Surface sf;
-        resolveHit(s, o, d, hit, sf);
-        const int light_index = s.object_light[sf.object_id];
-        if (light_index >= 0 && sf.front) {
-            const DevLight light = s.lights[light_index];
-            float3 e = ld3(light.e);
-            if (!isBlack(e) && !arrival_specular) {
-                e = e * powerHeuristic(arrival_pdf, choice * lightPdf(light, arrival_origin, d));
-            }
-            result = result + throughput * e;
-        }
-        if (depth >= max_depth) {
-            return result;
-        }
-        const Scattering sc = scatteringAt(s, sf);
-        const float3 wo = -d;
-        result = result + throughput * sampleDirectLight(s, c, sf, sc, wo, g);
-        const float u_choice = g.next1D();
-        const float ux = g.next1D();
-        const float uy = g.next1D();
-        ScatterSample smp;
-        if (!sc.sample(wo, u_choice, ux, uy, smp)) {
-            return result;
-        }
-        throughput = throughput * smp.weight;
-        if (isBlack(throughput)) {
-            return result;
-        }
-        if (depth >= roulette_start) {
-            const float survival = fminf(0.95f, fmaxf(throughput.x, fmaxf(throughput.y, throughput.z)));
-            if (g.next1D() >= survival) {
-                return result;
-            }
-            throughput = throughput / survival;
-        }
-        arrival_origin = sf.p;
-        arrival_pdf = smp.pdf;
-        arrival_specular = smp.specular;
-        rayLeaving(sf, smp.dir, o, skip);
-        d = smp.dir;
-    }
+    p.o = o;
+    p.d = d;
+    p.throughput = gray(1.0f);
+    p.result = gray(0.0f);
+    p.arrival_origin = o;
+    p.arrival_pdf = 0.0f;
+    p.depth = 0;
+    p.arrival_specular = true;
+    p.skip = SkipRule::none();
 }
 
-ALB_DEV float3 scatterOnlyRadiance(const DevScene& s, const TraceContext& c, float3 o, float3 d, Pcg32& g,
-                                   int max_scatter)
+// Emission seen at a surface along the path's ray, MIS-weighted against light
+// sampling at the previous vertex (weightedEmission).
+ALB_DEV float3 weightedEmission(const DevScene& s, const PathState& p, const Surface& sf)
 {
-    float3 throughput = gray(1.0f);
-    float3 result = gray(0.0f);
-    SkipRule skip = SkipRule::none();
-    for (int count = 0;; ++count) {
-        TraceHit hit;
-        if (!closestHit(s, c, o, d, skip, hit)) {
-            if (s.sky_light >= 0) {
-                result = result + throughput * skyRadiance(s.lights[s.sky_light], d);
-            }
-            return result;
-        }
-        Surface sf;
-        resolveHit(s, o, d, hit, sf);
-        const int light_index = s.object_light[sf.object_id];
-        if (light_index >= 0 && sf.front) {
-            result = result + throughput * ld3(s.lights[light_index].e);
-        }
-        if (count >= max_scatter) {
-            return result;
-        }
-        const float u_choice = g.next1D();
-        const float ux = g.next1D();
-        const float uy = g.next1D();
-        ScatterSample smp;
-        if (!scatteringAt(s, sf).sample(-d, u_choice, ux, uy, smp)) {
-            return result;
-        }
-        throughput = throughput * smp.weight;
-        if (isBlack(throughput)) {
-            return result;
-        }
-        rayLeaving(sf, smp.dir, o, skip);
-        d = smp.dir;
+    const int light_index = s.object_light[sf.object_id];
+    if (light_index < 0 || !sf.front) {
+        return gray(0.0f);
     }
+    const DevLight light = s.lights[light_index];
+    float3 e = ld3(light.e);
+    if (!isBlack(e) && !p.arrival_specular) {
+        e = e * powerHeuristic(p.arrival_pdf, (1.0f / static_cast<float>(s.light_count)) *
+                                                  lightPdf(light, p.arrival_origin, p.d));
+    }
+    return e;
 }
 
-ALB_DEV float3 normalsRadiance(const DevScene& s, const TraceContext& c, float3 o, float3 d)
+// The sky seen by an escaping path, MIS-weighted likewise (weightedSky).
+ALB_DEV float3 weightedSky(const DevScene& s, const PathState& p)
+{
+    if (s.sky_light < 0) {
+        return gray(0.0f);
+    }
+    float3 e = skyRadiance(s.lights[s.sky_light], p.d);
+    if (!isBlack(e) && !p.arrival_specular) {
+        e = e * powerHeuristic(p.arrival_pdf, (1.0f / static_cast<float>(s.light_count)) * uniformSpherePdf());
+    }
+    return e;
+}
+
+// The part of a bounce after the surface is known: next-event estimation, BSDF
+// sampling and roulette. Returns false when the path ends.
+ALB_DEV bool scatterAtSurface(const DevScene& s, const TraceContext& c, PathState& p, const Surface& sf, Pcg32& g,
+                              int roulette_start)
+{
+    const Scattering sc = scatteringAt(s, sf);
+    const float3 wo = -p.d;
+    p.result = p.result + p.throughput * sampleDirectLight(s, c, sf, sc, wo, g);
+    const float u_choice = g.next1D();
+    const float ux = g.next1D();
+    const float uy = g.next1D();
+    ScatterSample smp;
+    if (!sc.sample(wo, u_choice, ux, uy, smp)) {
+        return false;
+    }
+    p.throughput = p.throughput * smp.weight;
+    if (isBlack(p.throughput)) {
+        return false;
+    }
+    if (p.depth >= roulette_start) {
+        const float survival = fminf(0.95f, fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z)));
+        if (g.next1D() >= survival) {
+            return false;
+        }
+        p.throughput = p.throughput / survival;
+    }
+    p.arrival_origin = sf.p;
+    p.arrival_pdf = smp.pdf;
+    p.arrival_specular = smp.specular;
+    rayLeaving(sf, smp.dir, p.o, p.skip);
+    p.d = smp.dir;
+    ++p.depth;
+    return true;
+}
+
+// One iteration of PathEstimator::radiance's loop. Returns false when the path
+// has ended; p.result then holds its radiance.
+ALB_DEV bool pathBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, int max_depth,
+                        int roulette_start)
 {
     TraceHit hit;
-    if (closestHit(s, c, o, d, SkipRule::none(), hit)) {
-        Surface sf;
-        resolveHit(s, o, d, hit, sf);
-        return mk(0.5f * (sf.ns.x + 1.0f), 0.5f * (sf.ns.y + 1.0f), 0.5f * (sf.ns.z + 1.0f));
+    if (!closestHit(s, c, p.o, p.d, p.skip, hit)) {
+        p.result = p.result + p.throughput * weightedSky(s, p);
+        return false;
     }
-    const float h = 0.5f * (normalized(d).y + 1.0f);
-    return gray(1.0f) * (1.0f - h) + mk(0.5f, 0.7f, 1.0f) * h;
+    Surface sf;
+    resolveHit(s, p.o, p.d, hit, sf);
+    p.result = p.result + p.throughput * weightedEmission(s, p, sf);
+    if (p.depth >= max_depth) {
+        return false;
+    }
+    return scatterAtSurface(s, c, p, sf, g, roulette_start);
+}
+
+// One iteration of ScatterOnlyEstimator::radiance's loop
+// (estimator/scatter_only_estimator.cpp:14-48).
+ALB_DEV bool scatterOnlyBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, int max_scatter)
+{
+    TraceHit hit;
+    if (!closestHit(s, c, p.o, p.d, p.skip, hit)) {
+        if (s.sky_light >= 0) {
+            p.result = p.result + p.throughput * skyRadiance(s.lights[s.sky_light], p.d);
+        }
+        return false;
+    }
+    Surface sf;
+    resolveHit(s, p.o, p.d, hit, sf);
+    const int light_index = s.object_light[sf.object_id];
+    if (light_index >= 0 && sf.front) {
+        p.result = p.result + p.throughput * ld3(s.lights[light_index].e);
+    }
+    if (p.depth >= max_scatter) {
+        return false;
+    }
+    const float u_choice = g.next1D();
+    const float ux = g.next1D();
+    const float uy = g.next1D();
+    ScatterSample smp;
+    if (!scatteringAt(s, sf).sample(-p.d, u_choice, ux, uy, smp)) {
+        return false;
+    }
+    p.throughput = p.throughput * smp.weight;
+    if (isBlack(p.throughput)) {
+        return false;
+    }
+    rayLeaving(sf, smp.dir, p.o, p.skip);
+    p.d = smp.dir;
+    ++p.depth;
+    return true;
+}
+
+// NormalsEstimator::radiance (estimator/normals_estimator.cpp:32-38): one query.
+ALB_DEV bool normalsBounce(const DevScene& s, const TraceContext& c, PathState& p)
+{
+    TraceHit hit;
+    if (closestHit(s, c, p.o, p.d, SkipRule::none(), hit)) {
+        Surface sf;
+        resolveHit(s, p.o, p.d, hit, sf);
+        p.result = mk(0.5f * (sf.ns.x + 1.0f), 0.5f * (sf.ns.y + 1.0f), 0.5f * (sf.ns.z + 1.0f));
+    } else {
+        const float h = 0.5f * (normalized(p.d).y + 1.0f);
+        p.result = gray(1.0f) * (1.0f - h) + mk(0.5f, 0.7f, 1.0f) * h;
+    }
+    return false;
 }
 
 template <int EST>
-ALB_DEV float3 estimateRadiance(const DevScene& s, const TraceContext& c, float3 o, float3 d, Pcg32& g,
-                                const RenderArgs& a)
+ALB_DEV bool estimatorBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, const RenderArgs& a)
 {
     if constexpr (EST == kEstimatorPath) {
-        return pathRadiance(s, c, o, d, g, a.max_depth, a.roulette_start);
+        return pathBounce(s, c, p, g, a.max_depth, a.roulette_start);
     } else if constexpr (EST == kEstimatorScatterOnly) {
-        return scatterOnlyRadiance(s, c, o, d, g, a.max_depth);
+        return scatterOnlyBounce(s, c, p, g, a.max_depth);
     } else {
-        return normalsRadiance(s, c, o, d);
+        return normalsBounce(s, c, p);
     }
+}
+
+// Draws sample `index` of a pixel's n x n grid (row-major cells, x jitter then y,
+// render/render_image.cpp:32-40) and starts its camera path.
+ALB_DEV void startSample(const DevCamera& cam, PathState& p, Pcg32& g, int x, int y, int index, int n, float inv_n,
+                         float width, float height)
+{
+    const int sy = index / n;
+    const int sx = index - sy * n;
+    const float jx = g.next1D();
+    const float jy = g.next1D();
+    const float fx = (static_cast<float>(x) + (static_cast<float>(sx) + jx) * inv_n) / width;
+    const float fy = (static_cast<float>(y) + (static_cast<float>(sy) + jy) * inv_n) / height;
+    float3 o, d;
+    cameraRay(cam, fx, fy, o, d);
+    beginPath(p, o, d);
 }
 
 } // namespace albedo_b200

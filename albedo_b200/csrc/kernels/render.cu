@@ -14,9 +14,14 @@ namespace {
 constexpr int kBlock = 128;
 constexpr int kTileW = 16;
 constexpr int kTileH = 8;
+// Resident blocks per SM the megakernel's register budget is sized for.
+#ifndef ALBEDO_MEGA_BLOCKS_PER_SM
+#define ALBEDO_MEGA_BLOCKS_PER_SM 4
+#endif
+constexpr int kMegaBlocksPerSm = ALBEDO_MEGA_BLOCKS_PER_SM;
 
 template <int STACK, int EST, bool COUNT = false>
-__global__ void __launch_bounds__(kBlock) megakernel(const DevScene scene, const DevCamera camera,
+__global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const DevScene scene, const DevCamera camera,
                                                      const RenderArgs args, PixelAccum* accum,
                                                      unsigned int* error_flag,
                                                      unsigned long long* totals = nullptr)
@@ -49,22 +54,29 @@ __global__ void __launch_bounds__(kBlock) megakernel(const DevScene scene, const
     const float height = static_cast<float>(args.height);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     double qr = 0.0, qg = 0.0, qb = 0.0;
-    for (int sy = 0; sy < n; ++sy) {
-        for (int sx = 0; sx < n; ++sx) {
-            const float jx = g.next1D();
-            const float jy = g.next1D();
-            const float fx = (static_cast<float>(x) + (static_cast<float>(sx) + jx) * inv_n) / width;
-            const float fy = (static_cast<float>(y) + (static_cast<float>(sy) + jy) * inv_n) / height;
-            float3 o, d;
-            cameraRay(camera, fx, fy, o, d);
-            const float3 L = estimateRadiance<EST>(scene, ctx, o, d, g, args);
-            sr += L.x;
-            sg += L.y;
-            sb += L.z;
-            qr += static_cast<double>(L.x) * L.x;
-            qg += static_cast<double>(L.y) * L.y;
-            qb += static_cast<double>(L.z) * L.z;
+    // One bounce per iteration: a lane whose path ends starts the pixel's next
+    // sample at once (drawing its jitter next from the same stream, as the
+    // reference does), so a warp waits for the longest pixel, not the longest
+    // path of every sample.
+    const int total = n * n;
+    int sample = 0;
+    PathState path;
+    startSample(camera, path, g, x, y, 0, n, inv_n, width, height);
+    for (;;) {
+        if (estimatorBounce<EST>(scene, ctx, path, g, args)) {
+            continue;
         }
+        const float3 L = path.result;
+        sr += L.x;
+        sg += L.y;
+        sb += L.z;
+        qr += static_cast<double>(L.x) * L.x;
+        qg += static_cast<double>(L.y) * L.y;
+        qb += static_cast<double>(L.z) * L.z;
+        if (++sample == total) {
+            break;
+        }
+        startSample(camera, path, g, x, y, sample, n, inv_n, width, height);
     }
     PixelAccum& a = accum[slot];
     a.r += sr;

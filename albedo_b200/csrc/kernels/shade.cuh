@@ -80,7 +80,7 @@ ALB_DEV double refinedDistance(const DevScene& s, float3 origin, float3 dir, con
     }
     double px = ox, py = oy, pz = oz, qx = dx, qy = dy, qz = dz;
     if (obj.kind == kObjInstance) {
-        const float* m = s.instances[obj.index].to_object;
+        const double* m = s.instance_to_object64 + 12 * obj.index;
         px = m[0] * ox + m[1] * oy + m[2] * oz + m[3];
         py = m[4] * ox + m[5] * oy + m[6] * oz + m[7];
         pz = m[8] * ox + m[9] * oy + m[10] * oz + m[11];
@@ -236,7 +236,7 @@ ALB_DEV float grad(unsigned hash, float x, float y, float z)
 }
 
 // perlinNoise (texture/perlin_noise.cpp:114-138).
-ALB_DEV float perlinNoise(float3 p)
+static __device__ __noinline__ float perlinNoise(float3 p)
 {
     if (!isfinite(p.x) || !isfinite(p.y) || !isfinite(p.z)) {
         return 0.0f;
@@ -388,7 +388,7 @@ ALB_DEV Cpx csqrt(Cpx z)
 }
 
 // reflectance() of scattering/fresnel.cpp:17-25 for eta + i k.
-ALB_DEV float conductorReflectance(float cos_i, float eta, float k)
+static __device__ __noinline__ float conductorReflectance(float cos_i, float eta, float k)
 {
     const Cpx e{eta, k};
     const float sin2 = 1.0f - cos_i * cos_i;

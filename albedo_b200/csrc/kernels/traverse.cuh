@@ -269,11 +269,28 @@ ALB_DEV std::uint32_t leafRef(std::uint32_t first, std::uint32_t count)
 // any hit (ANY = true). On return `tmax` is the nearest hit distance. The stack
 // overflow bound (TLAS depth + BLAS depth + 2) is checked on the host before
 // launch, so pushes never exceed `stack_size`.
+// One out-of-line copy serves closest-hit and any-hit queries alike (`any`
+// stops at the first hit), which keeps the kernels that call it small enough
+// for the instruction cache.
+static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
+                                            const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
+                                            int stack_size, unsigned int* error_flag, TraversalCounts* counts,
+                                            bool any);
+
 template <bool ANY>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
                         TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts = nullptr)
 {
+    return traceSceneImpl(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts, ANY);
+}
+
+static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
+                                            const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
+                                            int stack_size, unsigned int* error_flag, TraversalCounts* counts,
+                                            bool any)
+{
+    const bool ANY = any;
     if (counts != nullptr) {
         counts->rays += 1;
     }

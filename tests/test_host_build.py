@@ -1,0 +1,72 @@
+"""The host scene build reproduces the reference exactly (CPU only).
+
+The FP64 restatement of the query path (oracle/trace_oracle.cpp) runs over this
+repository's host tables: its BVHs (built by albedo_b200/csrc/host/bvh_build.cpp),
+transforms, triangles and smooth normals. Its answers must equal the reference's
+Scene::intersect bit for bit on every ray, which holds only if the hierarchy,
+the instance transforms and the geometry are the reference's own.
+"""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import albedo_b200 as ab
+from oracle import reference as ref
+from oracle import restatement
+
+pytestmark = pytest.mark.skipif(not (ref.available() and restatement.available()), reason="oracle not built")
+
+ASSETS = Path("/root/reference/assets")
+
+
+def random_rays(count, seed, low, high):
+    rng = np.random.default_rng(seed)
+    origin = rng.uniform(low, high, size=(count, 3))
+    direction = rng.normal(size=(count, 3))
+    direction /= np.linalg.norm(direction, axis=1, keepdims=True)
+    return np.concatenate([origin, direction], axis=1).astype(np.float32).astype(np.float64)
+
+
+def scene_paths(room_path, trefoil_path):
+    paths = [room_path, trefoil_path]
+    if (ASSETS / "meshes.scene").exists():
+        paths.append(ASSETS / "meshes.scene")
+    return paths
+
+
+@pytest.mark.parametrize("index", [0, 1, 2])
+def test_restatement_equals_reference_bit_for_bit(index, room_path, trefoil_path):
+    paths = scene_paths(room_path, trefoil_path)
+    if index >= len(paths):
+        pytest.skip("reference assets absent")
+    path = paths[index]
+    scene = ab.Scene.read(path)
+    rays = random_rays(20_000, 21 + index, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    ours = restatement.intersect(scene, rays)
+    theirs = ref.RefScene(path).intersect(rays)
+    np.testing.assert_array_equal(ours["hit"], theirs["hit"])
+    hit = ours["hit"] == 1
+    assert hit.mean() > 0.5
+    np.testing.assert_array_equal(ours["object"][hit], theirs["object"][hit])
+    np.testing.assert_array_equal(ours["t"][hit], theirs["t"][hit])
+    np.testing.assert_array_equal(ours["point"][hit], theirs["point"][hit])
+    np.testing.assert_array_equal(ours["normal"][hit], theirs["normal"][hit])
+    np.testing.assert_array_equal(ours["shading_normal"][hit], theirs["shading_normal"][hit])
+    np.testing.assert_array_equal(ours["front"][hit], theirs["front"][hit])
+
+
+def test_restatement_reports_triangles_inside_instances(trefoil_path):
+    scene = ab.Scene.read(trefoil_path)
+    rays = random_rays(20_000, 5, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    ours = restatement.intersect(scene, rays)
+    hit = ours["hit"] == 1
+    info = scene.info()
+    assert info["objects"] == 9
+    # Objects 0 (floor) and 5..7 (knots) are instances; 1..4 and 8 are spheres.
+    instanced = np.isin(ours["object"], [0, 5, 6, 7]) & hit
+    assert instanced.sum() > 1000
+    assert np.all(ours["triangle"][instanced] >= 0)
+    assert np.all(ours["triangle"][hit & ~instanced] == -1)
+    assert (ours["counts"][hit][:, 0] > 0).all()
