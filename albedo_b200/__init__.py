@@ -308,6 +308,29 @@ def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: i
     _raise(library().albedo_render(scene.handle, byref(c), c_void_p(accumulators_ptr), c_void_p(stream)))
 
 
+def render_batch(items, stream: int = 0) -> None:
+    """Renders [(scene, job, device_accumulators_ptr), ...] in one wavefront run."""
+    from ._lib import BatchItemC
+
+    array = (BatchItemC * len(items))()
+    for i, (scene, job, ptr) in enumerate(items):
+        array[i].scene = scene.handle.value
+        array[i].job = job.to_c()
+        array[i].accumulators = ptr
+    _raise(library().albedo_render_batch(array, len(items), c_void_p(stream)))
+
+
+def wavefront_configure(slots: int = 1 << 20, blocks_per_sm: int = 8, iterations_per_graph: int = 4) -> None:
+    """Shape of the wavefront engine: path slots, queue-kernel blocks per SM, iterations per graph."""
+    _raise(library().albedo_wavefront_configure(slots, blocks_per_sm, iterations_per_graph))
+
+
+def wavefront_last_iterations() -> int:
+    out = ctypes.c_int64()
+    _raise(library().albedo_wavefront_last_iterations(byref(out)))
+    return out.value
+
+
 def work_counts(scene: Scene, job: RenderJob) -> dict:
     """Traversal work of one render of `job` (path estimator), counted on the device."""
     out = (ctypes.c_int64 * 5)()

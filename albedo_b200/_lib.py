@@ -19,6 +19,10 @@ class RenderJobC(ctypes.Structure):
                 ("reserved", c_int32)]
 
 
+class BatchItemC(ctypes.Structure):
+    _fields_ = [("scene", c_void_p), ("job", RenderJobC), ("accumulators", c_void_p)]
+
+
 class BasicMaterialC(ctypes.Structure):
     _fields_ = [("kind", c_int32), ("texture", c_int32), ("a", c_double * 3), ("b", c_double * 3),
                 ("frequency_or_scale", c_double), ("veins", c_double), ("ior", c_double), ("roughness", c_double)]
@@ -64,6 +68,9 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
     "albedo_scene_check": (c_int32, [c_void_p]),
     "albedo_render_work_counts": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(c_int64)]),
+    "albedo_render_batch": (c_int32, [c_void_p, c_int32, c_void_p]),
+    "albedo_wavefront_configure": (c_int32, [c_int32, c_int32, c_int32]),
+    "albedo_wavefront_last_iterations": (c_int32, [POINTER(c_int64)]),
     "albedo_trace_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, _I, _F, _I, _I, _F, _F, _F, _I]),
     "albedo_occluded_host": (c_int32, [c_void_p, _F, _F, c_int64, _I]),
     "albedo_probe_pixel_stream": (c_int32, [c_uint64, c_int32, c_int32, c_int32, c_int32, _U, _F]),

@@ -6,6 +6,10 @@
 #include "host/flatten.hpp"
 #include "host/scene_file.hpp"
 #include "kernels/launch.hpp"
+#include "wavefront_engine.hpp"
+
+#include <algorithm>
+#include <mutex>
 
 #include <cuda_runtime_api.h>
 
@@ -288,6 +292,12 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     if (!scene.host.has_camera) {
         throw std::invalid_argument{"the scene has no camera"};
     }
+    if (job.method != ALBEDO_MEGAKERNEL && job.method != ALBEDO_WAVEFRONT) {
+        throw std::invalid_argument{"unknown render method"};
+    }
+    if (job.method == ALBEDO_WAVEFRONT && job.estimator != ALBEDO_PATH) {
+        throw Unsupported{"the wavefront renderer implements the path estimator only"};
+    }
     RenderArgs args{};
     args.width = job.width;
     args.height = job.height;
@@ -297,6 +307,86 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     args.max_depth = job.max_depth;
     args.roulette_start = job.roulette_start;
     return args;
+}
+
+// The process's wavefront engine on the current device, created on first use.
+constexpr int kDefaultSlots{1 << 20};
+std::mutex g_engine_mutex;
+std::unique_ptr<WavefrontEngine> g_engine;
+int g_engine_slots{kDefaultSlots};
+int g_engine_blocks_per_sm{8};
+int g_engine_iterations_per_graph{4};
+unsigned long long g_last_iterations{0};
+
+void configureEngine(int slots, int blocks_per_sm, int iterations_per_graph)
+{
+    if (slots <= 0 || blocks_per_sm <= 0 || iterations_per_graph <= 0) {
+        throw std::invalid_argument{"wavefront configuration values must be positive"};
+    }
+    const std::lock_guard lock{g_engine_mutex};
+    if (g_engine && g_engine->slotCount() != slots) {
+        g_engine.reset();
+    }
+    g_engine_slots = slots;
+    g_engine_blocks_per_sm = blocks_per_sm;
+    g_engine_iterations_per_graph = iterations_per_graph;
+}
+
+unsigned long long lastEngineIterations()
+{
+    const std::lock_guard lock{g_engine_mutex};
+    return g_last_iterations;
+}
+
+WfJob wavefrontJob(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum)
+{
+    albedo_render_job wf{job};
+    wf.method = ALBEDO_WAVEFRONT;
+    static_cast<void>(renderArgsFor(scene, wf));
+    WfJob j{};
+    j.scene = scene.dev;
+    j.camera = deviceCamera(scene.host, job.width, job.height);
+    j.accum = accum;
+    j.width = job.width;
+    j.height = job.height;
+    j.samples_per_axis = job.samples_per_axis;
+    j.max_depth = job.max_depth;
+    j.roulette_start = job.roulette_start;
+    j.seed = job.seed;
+    return j;
+}
+
+void runWavefront(const std::vector<WfJob>& jobs, int stack, unsigned int* error_flag, cudaStream_t stream)
+{
+    const std::lock_guard lock{g_engine_mutex};
+    try {
+        if (!g_engine) {
+            g_engine = std::make_unique<WavefrontEngine>(g_engine_slots);
+        }
+        g_engine->setLaunch(g_engine_blocks_per_sm, g_engine_iterations_per_graph);
+        g_engine->render(jobs, stack, error_flag, stream);
+        g_last_iterations = g_engine->lastIterations();
+    } catch (const std::bad_alloc&) {
+        throw;
+    } catch (const std::invalid_argument&) {
+        throw;
+    } catch (const std::exception& e) {
+        throw DeviceError{e.what()};
+    }
+}
+
+void renderOnDevice(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum, cudaStream_t stream)
+{
+    const RenderArgs args{renderArgsFor(scene, job)};
+    if (job.method == ALBEDO_WAVEFRONT) {
+        runWavefront({wavefrontJob(scene, job, accum)}, scene.stack_capacity, scene.error_flag.as<unsigned int>(),
+                     stream);
+        return;
+    }
+    const DevCamera camera{deviceCamera(scene.host, job.width, job.height)};
+    check(launchMegakernel(scene.dev, camera, args, accum, scene.error_flag.as<unsigned int>(), scene.stack_capacity,
+                           stream),
+          "render launch");
 }
 
 } // namespace
@@ -526,29 +616,49 @@ int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albed
                   void* stream)
 {
     return guarded([&] {
-        const RenderArgs args{renderArgsFor(*scene, *job)};
-        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
-        check(launchMegakernel(scene->dev, camera, args, reinterpret_cast<PixelAccum*>(accumulators),
-                               scene->error_flag.as<unsigned int>(), scene->stack_capacity,
-                               static_cast<cudaStream_t>(stream)),
-              "render launch");
+        renderOnDevice(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators), static_cast<cudaStream_t>(stream));
     });
 }
 
 int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators)
 {
     return guarded([&] {
-        const RenderArgs args{renderArgsFor(*scene, *job)};
+        static_cast<void>(renderArgsFor(*scene, *job));
         const std::size_t pixels{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height)};
         DeviceBuffer device{uploadRaw(accumulators, pixels)};
-        const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
-        check(launchMegakernel(scene->dev, camera, args, device.as<PixelAccum>(), scene->error_flag.as<unsigned int>(),
-                               scene->stack_capacity, nullptr),
-              "render launch");
+        renderOnDevice(*scene, *job, device.as<PixelAccum>(), nullptr);
         check(cudaDeviceSynchronize(), "render");
         download(accumulators, device, pixels);
         scene->collectKernelError();
     });
+}
+
+int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* stream)
+{
+    return guarded([&] {
+        if (count <= 0) {
+            throw std::invalid_argument{"a batch needs at least one job"};
+        }
+        std::vector<WfJob> jobs;
+        jobs.reserve(static_cast<std::size_t>(count));
+        int stack{32};
+        for (int32_t i{0}; i < count; ++i) {
+            const albedo_batch_item& item{items[i]};
+            jobs.push_back(wavefrontJob(*item.scene, item.job, reinterpret_cast<PixelAccum*>(item.accumulators)));
+            stack = std::max(stack, item.scene->stack_capacity);
+        }
+        runWavefront(jobs, stack, items[0].scene->error_flag.as<unsigned int>(), static_cast<cudaStream_t>(stream));
+    });
+}
+
+int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph)
+{
+    return guarded([&] { configureEngine(slot_count, blocks_per_sm, iterations_per_graph); });
+}
+
+int albedo_wavefront_last_iterations(int64_t* out)
+{
+    return guarded([&] { *out = static_cast<int64_t>(lastEngineIterations()); });
 }
 
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,

@@ -36,44 +36,69 @@ ALB_DEV bool occluded(const DevScene& s, const TraceContext& c, float3 o, float3
     return traceScene<true>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag, c.counts);
 }
 
-// Next-event estimation from one uniformly chosen light, MIS-weighted, scaled
-// by nothing (the caller multiplies by the throughput).
-ALB_DEV float3 sampleDirectLight(const DevScene& s, const TraceContext& c, const Surface& sf, const Scattering& sc,
-                                 float3 wo, Pcg32& g)
+// Next-event estimation from one uniformly chosen light, MIS-weighted, before
+// the shadow test: what sampleDirectLight computes up to Scene::occluded. The
+// contribution is not yet scaled by the path throughput.
+struct NeeCandidate {
+    bool valid;         // a non-zero contribution exists
+    bool needs_test;    // a shadow ray must confirm it (the range is not empty)
+    float3 contribution;
+    float3 origin;
+    float3 dir;
+    float range_max;
+    SkipRule skip;
+};
+
+ALB_DEV NeeCandidate directLightCandidate(const DevScene& s, const Surface& sf, const Scattering& sc, float3 wo,
+                                          Pcg32& g)
 {
+    NeeCandidate nc;
+    nc.valid = false;
+    nc.needs_test = false;
     const float u_light = g.next1D();
     const float ux = g.next1D();
     const float uy = g.next1D();
     if (s.light_count == 0u) {
-        return gray(0.0f);
+        return nc;
     }
     const int n = static_cast<int>(s.light_count);
     const int index = min(static_cast<int>(u_light * static_cast<float>(n)), n - 1);
     const DevLight light = s.lights[index];
     LightSample ls;
     if (!sampleLight(light, sf.p, ux, uy, ls) || isBlack(ls.radiance)) {
-        return gray(0.0f);
+        return nc;
     }
     const float3 f = sc.evaluate(wo, ls.dir);
     if (isBlack(f)) {
-        return gray(0.0f);
+        return nc;
     }
     const float range_max = shadowRangeMax(ls.distance);
     if (range_max > 0.0f) {
-        float3 so;
-        SkipRule skip;
-        rayLeaving(sf, ls.dir, so, skip);
+        nc.needs_test = true;
+        rayLeaving(sf, ls.dir, nc.origin, nc.skip);
         if (light.kind == kLightArea) {
-            skip.light_object_pos = light.object;
+            nc.skip.light_object_pos = light.object;
         }
-        if (occluded(s, c, so, ls.dir, range_max, skip)) {
-            return gray(0.0f);
-        }
+        nc.dir = ls.dir;
+        nc.range_max = range_max;
     }
     const float light_pdf = (1.0f / static_cast<float>(n)) * ls.pdf;
     const float weight = ls.delta ? 1.0f : powerHeuristic(light_pdf, sc.pdf(wo, ls.dir));
     const float cos_theta = fabsf(dot(ls.dir, sf.ns));
-    return f * ls.radiance * (cos_theta * weight / light_pdf);
+    nc.contribution = f * ls.radiance * (cos_theta * weight / light_pdf);
+    nc.valid = true;
+    return nc;
+}
+
+// sampleDirectLight: the candidate, confirmed by a shadow query.
+ALB_DEV float3 sampleDirectLight(const DevScene& s, const TraceContext& c, const Surface& sf, const Scattering& sc,
+                                 float3 wo, Pcg32& g)
+{
+    const NeeCandidate nc = directLightCandidate(s, sf, sc, wo, g);
+    if (!nc.valid || (nc.needs_test && occluded(s, c, nc.origin, nc.dir, nc.range_max, nc.skip))) {
+        return gray(0.0f);
+    }
+    return nc.contribution;
 }
 
 // The state of one path between bounces: PathEstimator::radiance's loop

@@ -687,6 +687,38 @@ ALB_DEV Scattering scatteringAt(const DevScene& s, const Surface& sf)
     return sc;
 }
 
+// Material classes the wavefront renderer shades in separate kernels.
+enum MaterialClass : int { kClassDiffuse = 0, kClassConductor = 1, kClassDielectric = 2, kClassMix = 3 };
+
+ALB_DEV int materialClass(const DevScene& s, std::uint32_t obj_pos)
+{
+    const DevMaterial& m = s.materials[s.objects[obj_pos].material];
+    return m.mix != 0u ? kClassMix : static_cast<int>(m.first.kind);
+}
+
+// scatteringAt for a material known to be of class CLASS, so that only that
+// lobe's code is compiled into the kernel shading it.
+template <int CLASS>
+ALB_DEV Scattering scatteringAtClass(const DevScene& s, const Surface& sf)
+{
+    if constexpr (CLASS == kClassMix) {
+        return scatteringAt(s, sf);
+    } else {
+        const DevBasic& b = s.materials[sf.material].first;
+        Scattering sc;
+        sc.basis = Onb::fromNormal(sf.ns);
+        sc.geometric = sf.n;
+        if constexpr (CLASS == kClassDiffuse) {
+            sc.lobe = {kLobeLambert, textureColor(s, b, sf), gray(0.0f), 0.0f, 1.0f};
+        } else if constexpr (CLASS == kClassConductor) {
+            sc.lobe = {kLobeConductor, ld3(b.a), ld3(b.b), b.s0, 1.0f};
+        } else {
+            sc.lobe = {kLobeDielectric, gray(0.0f), gray(0.0f), b.s0, sf.front ? b.s1 : 1.0f / b.s1};
+        }
+        return sc;
+    }
+}
+
 // ------------------------------------------------------------------ lights
 
 struct LightSample {

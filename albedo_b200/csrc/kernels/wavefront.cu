@@ -1,0 +1,421 @@
+// The wavefront renderer: path slots advanced one bounce per iteration by
+// stage kernels over compacted queues.
+//
+//   regenerate   finished paths are added to their pixel (PixelBuffer::addSample);
+//                the slot starts its pixel's next stratified sample, or claims the
+//                batch's next pixel (render/render_image.cpp:27-44)
+//   extend       closest hit of every queued ray; misses add the MIS-weighted sky
+//   shade x 4    one kernel per material class (diffuse / conductor / dielectric /
+//                mix): emission, next-event estimation (a shadow-ray candidate),
+//                BSDF sampling and roulette (estimator/path_estimator.cpp:153-185)
+//   shadow       any-hit test of the candidates; unoccluded ones are added
+//   advance      swaps the double-buffered extend / regenerate queues
+//
+// Every push is warp-aggregated: one ballot, one atomicAdd per warp, and each
+// lane writes at the prefix count of the lanes below it. Random numbers are drawn
+// in the same order as the megakernel (jitter, then per bounce 3 NEE, 3 BSDF,
+// 1 roulette), so each pixel's stream matches the reference's.
+#include "estimator.cuh"
+#include "wavefront.cuh"
+
+namespace albedo_b200 {
+
+namespace {
+
+ALB_DEV void pushSlot(int* queue, int* counter, int slot, bool pred)
+{
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, pred);
+    if (mask == 0u) {
+        return;
+    }
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) {
+        base = atomicAdd(counter, __popc(mask));
+    }
+    base = __shfl_sync(active, base, leader);
+    if (pred) {
+        queue[base + __popc(mask & ((1u << lane) - 1u))] = slot;
+    }
+}
+
+// Hands out work items with one atomicAdd per warp.
+ALB_DEV unsigned long long claimItem(unsigned long long* next, bool want)
+{
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, want);
+    if (mask == 0u) {
+        return ~0ull;
+    }
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) {
+        base = atomicAdd(next, static_cast<unsigned long long>(__popc(mask)));
+    }
+    base = __shfl_sync(active, base, leader);
+    return want ? base + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u))) : ~0ull;
+}
+
+ALB_DEV int findJob(const WfJob* jobs, int job_count, long long item)
+{
+    int lo = 0;
+    int hi = job_count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (jobs[mid].item_begin <= item) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+ALB_DEV void storeRay(const WfSlots& sl, int s, const PathState& p)
+{
+    sl.ray_o[s] = make_float4(p.o.x, p.o.y, p.o.z, p.arrival_pdf);
+    sl.ray_d[s] = make_float4(p.d.x, p.d.y, p.d.z, p.arrival_specular ? 1.0f : 0.0f);
+    sl.throughput[s] = make_float4(p.throughput.x, p.throughput.y, p.throughput.z, 0.0f);
+    sl.result[s] = make_float4(p.result.x, p.result.y, p.result.z, 0.0f);
+    sl.arrival[s] = make_float4(p.arrival_origin.x, p.arrival_origin.y, p.arrival_origin.z, 0.0f);
+    sl.skip[s] = make_uint4(p.skip.object_pos, p.skip.tri_pos, static_cast<unsigned>(p.skip.sphere_mode), 0u);
+}
+
+ALB_DEV void loadPath(const WfSlots& sl, int s, int depth, PathState& p)
+{
+    const float4 o = sl.ray_o[s];
+    const float4 d = sl.ray_d[s];
+    const float4 t = sl.throughput[s];
+    const float4 r = sl.result[s];
+    const float4 a = sl.arrival[s];
+    const uint4 k = sl.skip[s];
+    p.o = mk(o.x, o.y, o.z);
+    p.arrival_pdf = o.w;
+    p.d = mk(d.x, d.y, d.z);
+    p.arrival_specular = d.w != 0.0f;
+    p.throughput = mk(t.x, t.y, t.z);
+    p.result = mk(r.x, r.y, r.z);
+    p.arrival_origin = mk(a.x, a.y, a.z);
+    p.skip = {k.x, k.y, static_cast<int>(k.z), kNoPrim};
+    p.depth = depth;
+}
+
+__global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ jobs, int job_count,
+                                                   unsigned long long total_items, WfBuffers b)
+{
+    WfControl* ctl = b.control;
+    const int parity = ctl->parity;
+    const int in = kQRegen0 + parity;
+    const int out = kQExtend0 + parity;
+    const int count = ctl->count[in];
+    const WfSlots& sl = b.slots;
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const int s = b.queue[in][i];
+        int4 w = sl.where[s];
+        bool start = false;
+        Pcg32 g;
+        if (w.x >= 0) {
+            const WfJob& job = jobs[w.x];
+            const float4 r = sl.result[s];
+            PixelAccum& acc = job.accum[w.y];
+            acc.r += r.x;
+            acc.g += r.y;
+            acc.b += r.z;
+            acc.count += 1;
+            w.z += 1;
+            if (w.z < job.samples_per_axis * job.samples_per_axis) {
+                start = true;
+                const ulonglong2 st = sl.rng[s];
+                g = {st.x, st.y};
+            } else {
+                atomicAdd(&ctl->completed, 1ull);
+                w.x = -1;
+            }
+        }
+        const unsigned long long item = claimItem(&ctl->next_item, w.x < 0);
+        if (w.x < 0 && item < total_items) {
+            const int j = findJob(jobs, job_count, static_cast<long long>(item));
+            const WfJob& job = jobs[j];
+            const int pixel = static_cast<int>(static_cast<long long>(item) - job.item_begin);
+            w = make_int4(j, pixel, 0, 0);
+            g = pixelGenerator(job.seed, static_cast<std::uint32_t>(pixel % job.width),
+                               static_cast<std::uint32_t>(pixel / job.width), static_cast<std::uint32_t>(job.width));
+            start = true;
+        }
+        if (start) {
+            const WfJob& job = jobs[w.x];
+            const int n = job.samples_per_axis;
+            PathState p;
+            startSample(job.camera, p, g, w.y % job.width, w.y / job.width, w.z, n, 1.0f / static_cast<float>(n),
+                        static_cast<float>(job.width), static_cast<float>(job.height));
+            storeRay(sl, s, p);
+            sl.rng[s] = make_ulonglong2(g.state, g.inc);
+            w.w = 0;
+        }
+        sl.where[s] = w;
+        pushSlot(b.queue[out], &ctl->count[out], s, start);
+    }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
+                                                    unsigned int* error_flag)
+{
+    extern __shared__ uint2 stack[];
+    WfControl* ctl = b.control;
+    const int parity = ctl->parity;
+    const int in = kQExtend0 + parity;
+    const int ended = kQRegen0 + (parity ^ 1);
+    const int count = ctl->count[in];
+    const WfSlots& sl = b.slots;
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const int s = b.queue[in][i];
+        const int job_index = sl.where[s].x;
+        const DevScene& scene = jobs[job_index].scene;
+        const float4 o = sl.ray_o[s];
+        const float4 d = sl.ray_d[s];
+        const uint4 k = sl.skip[s];
+        const SkipRule skip{k.x, k.y, static_cast<int>(k.z), kNoPrim};
+        TraceHit hit;
+        float tmax = INFINITY;
+        const bool found = traceScene<false>(scene, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, tmax, skip, hit,
+                                             stack + threadIdx.x, static_cast<int>(blockDim.x), STACK, error_flag);
+        int cls = -1;
+        if (found) {
+            sl.hit[s] = make_float4(hit.t, __uint_as_float(hit.obj_pos), __uint_as_float(hit.tri_pos), hit.b0);
+            sl.hit_b[s] = make_float2(hit.b1, hit.b2);
+            cls = materialClass(scene, hit.obj_pos);
+        } else {
+            PathState p;
+            p.d = mk(d.x, d.y, d.z);
+            p.arrival_pdf = o.w;
+            p.arrival_specular = d.w != 0.0f;
+            const float4 t = sl.throughput[s];
+            const float3 e = weightedSky(scene, p);
+            float4 r = sl.result[s];
+            r.x += t.x * e.x;
+            r.y += t.y * e.y;
+            r.z += t.z * e.z;
+            sl.result[s] = r;
+        }
+        pushSlot(b.queue[ended], &ctl->count[ended], s, !found);
+        pushSlot(b.queue[kQDiffuse], &ctl->count[kQDiffuse], s, cls == kClassDiffuse);
+        pushSlot(b.queue[kQConductor], &ctl->count[kQConductor], s, cls == kClassConductor);
+        pushSlot(b.queue[kQDielectric], &ctl->count[kQDielectric], s, cls == kClassDielectric);
+        pushSlot(b.queue[kQMix], &ctl->count[kQMix], s, cls == kClassMix);
+    }
+}
+
+template <int CLASS>
+__global__ void __launch_bounds__(128) shadeKernel(const WfJob* __restrict__ jobs, WfBuffers b)
+{
+    WfControl* ctl = b.control;
+    const int parity = ctl->parity;
+    const int in = kQDiffuse + CLASS;
+    const int next = kQExtend0 + (parity ^ 1);
+    const int ended = kQRegen0 + (parity ^ 1);
+    const int count = ctl->count[in];
+    const WfSlots& sl = b.slots;
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const int s = b.queue[in][i];
+        int4 w = sl.where[s];
+        const WfJob& job = jobs[w.x];
+        const DevScene& scene = job.scene;
+        PathState p;
+        loadPath(sl, s, w.w, p);
+        const float4 h = sl.hit[s];
+        const float2 hb = sl.hit_b[s];
+        const TraceHit hit{h.x, __float_as_uint(h.y), __float_as_uint(h.z), h.w, hb.x, hb.y};
+        const ulonglong2 st = sl.rng[s];
+        Pcg32 g{st.x, st.y};
+        Surface sf;
+        resolveHit(scene, p.o, p.d, hit, sf);
+        p.result = p.result + p.throughput * weightedEmission(scene, p, sf);
+        bool alive = false;
+        bool shadow = false;
+        if (p.depth < job.max_depth) {
+            const Scattering sc = scatteringAtClass<CLASS>(scene, sf);
+            const float3 wo = -p.d;
+            const NeeCandidate nc = directLightCandidate(scene, sf, sc, wo, g);
+            if (nc.valid) {
+                const float3 c = p.throughput * nc.contribution;
+                if (nc.needs_test) {
+                    shadow = true;
+                    sl.shadow_o[s] = make_float4(nc.origin.x, nc.origin.y, nc.origin.z, nc.range_max);
+                    sl.shadow_d[s] = make_float4(nc.dir.x, nc.dir.y, nc.dir.z, __uint_as_float(nc.skip.light_object_pos));
+                    sl.shadow_skip[s] = make_uint4(nc.skip.object_pos, nc.skip.tri_pos,
+                                                   static_cast<unsigned>(nc.skip.sphere_mode), 0u);
+                    sl.shadow_c[s] = make_float4(c.x, c.y, c.z, 0.0f);
+                } else {
+                    p.result = p.result + c;
+                }
+            }
+            const float u_choice = g.next1D();
+            const float ux = g.next1D();
+            const float uy = g.next1D();
+            ScatterSample smp;
+            if (sc.sample(wo, u_choice, ux, uy, smp)) {
+                p.throughput = p.throughput * smp.weight;
+                if (!isBlack(p.throughput)) {
+                    alive = true;
+                    if (p.depth >= job.roulette_start) {
+                        const float survival =
+                            fminf(0.95f, fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z)));
+                        if (g.next1D() >= survival) {
+                            alive = false;
+                        } else {
+                            p.throughput = p.throughput / survival;
+                        }
+                    }
+                    if (alive) {
+                        p.arrival_origin = sf.p;
+                        p.arrival_pdf = smp.pdf;
+                        p.arrival_specular = smp.specular;
+                        rayLeaving(sf, smp.dir, p.o, p.skip);
+                        p.d = smp.dir;
+                        w.w = p.depth + 1;
+                    }
+                }
+            }
+        }
+        storeRay(sl, s, p);
+        sl.rng[s] = make_ulonglong2(g.state, g.inc);
+        sl.where[s] = w;
+        pushSlot(b.queue[kQShadow], &ctl->count[kQShadow], s, shadow);
+        pushSlot(b.queue[next], &ctl->count[next], s, alive);
+        pushSlot(b.queue[ended], &ctl->count[ended], s, !alive);
+    }
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
+                                                    unsigned int* error_flag)
+{
+    extern __shared__ uint2 stack[];
+    WfControl* ctl = b.control;
+    const int count = ctl->count[kQShadow];
+    const WfSlots& sl = b.slots;
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const int s = b.queue[kQShadow][i];
+        const DevScene& scene = jobs[sl.where[s].x].scene;
+        const float4 o = sl.shadow_o[s];
+        const float4 d = sl.shadow_d[s];
+        const uint4 k = sl.shadow_skip[s];
+        const SkipRule skip{k.x, k.y, static_cast<int>(k.z), __float_as_uint(d.w)};
+        TraceHit hit;
+        float tmax = o.w;
+        if (!traceScene<true>(scene, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, tmax, skip, hit,
+                              stack + threadIdx.x, static_cast<int>(blockDim.x), STACK, error_flag)) {
+            const float4 c = sl.shadow_c[s];
+            float4 r = sl.result[s];
+            r.x += c.x;
+            r.y += c.y;
+            r.z += c.z;
+            sl.result[s] = r;
+        }
+    }
+}
+
+__global__ void advanceKernel(WfControl* ctl)
+{
+    const int parity = ctl->parity;
+    ctl->count[kQExtend0 + parity] = 0;
+    ctl->count[kQRegen0 + parity] = 0;
+    ctl->count[kQDiffuse] = 0;
+    ctl->count[kQConductor] = 0;
+    ctl->count[kQDielectric] = 0;
+    ctl->count[kQMix] = 0;
+    ctl->count[kQShadow] = 0;
+    ctl->parity = parity ^ 1;
+    ctl->iterations += 1;
+}
+
+__global__ void resetKernel(WfBuffers b)
+{
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i < b.slot_count) {
+        b.slots.where[i] = make_int4(-1, 0, 0, 0);
+        b.queue[kQRegen0][i] = i;
+    }
+    if (i == 0) {
+        WfControl* ctl = b.control;
+        for (int q = 0; q < kQueueCount; ++q) {
+            ctl->count[q] = 0;
+        }
+        ctl->count[kQRegen0] = b.slot_count;
+        ctl->parity = 0;
+        ctl->next_item = 0;
+        ctl->completed = 0;
+        ctl->iterations = 0;
+    }
+}
+
+template <typename Kernel>
+cudaError_t allowStack(Kernel kernel, int stack, bool& configured)
+{
+    if (configured) {
+        return cudaSuccess;
+    }
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               stack * 128 * static_cast<int>(sizeof(uint2)));
+    configured = e == cudaSuccess;
+    return e;
+}
+
+} // namespace
+
+cudaError_t wfPrepare(int stack)
+{
+    static bool configured[4] = {false, false, false, false};
+    cudaError_t e;
+    if (stack == 32) {
+        if ((e = allowStack(extendKernel<32>, 32, configured[0])) != cudaSuccess) {
+            return e;
+        }
+        return allowStack(shadowKernel<32>, 32, configured[1]);
+    }
+    if ((e = allowStack(extendKernel<64>, 64, configured[2])) != cudaSuccess) {
+        return e;
+    }
+    return allowStack(shadowKernel<64>, 64, configured[3]);
+}
+
+cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream)
+{
+    (void)total_items;
+    resetKernel<<<(b.slot_count + 255) / 256, 256, 0, stream>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long total_items, const WfBuffers& b,
+                        const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream)
+{
+    const int g = launch.blocks;
+    const std::size_t smem = static_cast<std::size_t>(launch.stack) * 128 * sizeof(uint2);
+    regenKernel<<<g, 128, 0, stream>>>(jobs, job_count, total_items, b);
+    if (launch.stack == 32) {
+        extendKernel<32><<<g, 128, smem, stream>>>(jobs, b, error_flag);
+    } else {
+        extendKernel<64><<<g, 128, smem, stream>>>(jobs, b, error_flag);
+    }
+    shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
+    shadeKernel<kClassConductor><<<g, 128, 0, stream>>>(jobs, b);
+    shadeKernel<kClassDielectric><<<g, 128, 0, stream>>>(jobs, b);
+    shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
+    if (launch.stack == 32) {
+        shadowKernel<32><<<g, 128, smem, stream>>>(jobs, b, error_flag);
+    } else {
+        shadowKernel<64><<<g, 128, smem, stream>>>(jobs, b, error_flag);
+    }
+    advanceKernel<<<1, 1, 0, stream>>>(b.control);
+    return cudaGetLastError();
+}
+
+} // namespace albedo_b200

@@ -1,0 +1,91 @@
+// Wavefront renderer layout: jobs, path slots and queues shared by the kernels
+// in wavefront.cu and the host engine that drives them.
+#pragma once
+
+#include "launch.hpp"
+
+#include <cstdint>
+
+namespace albedo_b200 {
+
+// One render job of a batch: its scene, camera, accumulators and parameters, and
+// where its pixels sit in the batch's work-item range.
+struct WfJob {
+    DevScene scene;
+    DevCamera camera;
+    PixelAccum* accum;
+    int width;
+    int height;
+    int samples_per_axis;
+    int max_depth;
+    int roulette_start;
+    int pad;
+    unsigned long long seed;
+    long long item_begin;   // first work item (pixel) of this job
+    long long item_end;     // one past its last
+};
+
+// Path slots, one record per field group so a gather of one slot reads whole
+// 16-byte records. A slot owns one pixel for all of that pixel's samples, so its
+// PCG32 stream advances exactly as the reference's per-pixel generator does.
+struct WfSlots {
+    float4* ray_o;      // origin xyz, arrival pdf
+    float4* ray_d;      // direction xyz, arrival-specular flag (0 or 1)
+    float4* throughput; // xyz, unused
+    float4* result;     // radiance gathered so far xyz, unused
+    float4* arrival;    // previous scattering point xyz, unused
+    uint4* skip;        // object position, triangle position, sphere mode, unused
+    ulonglong2* rng;    // PCG32 state, increment
+    int4* where;        // job (-1: idle), pixel index in the job, sample index, depth
+    float4* hit;        // t, object position bits, triangle position bits, b0
+    float2* hit_b;      // b1, b2
+    float4* shadow_o;   // shadow ray origin xyz, range end
+    float4* shadow_d;   // shadow ray direction xyz, area-light object position bits
+    uint4* shadow_skip; // object position, triangle position, sphere mode, unused
+    float4* shadow_c;   // contribution if unoccluded xyz, unused
+};
+
+enum WfQueueId : int {
+    kQExtend0 = 0,
+    kQExtend1 = 1,
+    kQRegen0 = 2,
+    kQRegen1 = 3,
+    kQDiffuse = 4,
+    kQConductor = 5,
+    kQDielectric = 6,
+    kQMix = 7,
+    kQShadow = 8,
+    kQueueCount = 9
+};
+
+struct WfControl {
+    int count[kQueueCount];
+    int parity;                   // current extend/regen buffers: kQExtend0 + parity, kQRegen0 + parity
+    unsigned long long next_item; // next pixel work item to hand out
+    unsigned long long completed; // pixels whose last sample has been accumulated
+    unsigned long long iterations;
+};
+
+struct WfBuffers {
+    WfSlots slots;
+    int* queue[kQueueCount]; // each `slot_count` entries
+    WfControl* control;
+    int slot_count;
+};
+
+struct WfLaunch {
+    int blocks;       // grid of the queue kernels (a multiple of the SM count)
+    int threads;      // threads per block
+    int stack;        // traversal stack entries per thread
+};
+
+// Opts the traversal kernels into `stack` entries of dynamic shared memory; call
+// before capturing iterations into a graph.
+cudaError_t wfPrepare(int stack);
+// Puts every slot in the regeneration queue with no job, and clears counters.
+cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream);
+// Enqueues one iteration (regenerate, extend, shade x 4, shadow, advance).
+cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long total_items, const WfBuffers& b,
+                        const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream);
+
+} // namespace albedo_b200

@@ -171,6 +171,25 @@ int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, 
  * optionally also returning per-pixel sums of squared samples (3 doubles each). */
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
                               int64_t pixel_count, albedo_accumulator* accumulators, double* sum_squares);
+/* One job of a batch: a committed scene, its job, and a device array of its
+ * width*height accumulators. */
+typedef struct albedo_batch_item {
+    const albedo_scene* scene;
+    albedo_render_job job;
+    albedo_accumulator* accumulators;
+} albedo_batch_item;
+
+/* Renders many jobs (any scenes, sizes and sample counts; path estimator) in one
+ * wavefront run that shares the path slots among them, so small jobs fill the
+ * GPU together. Each job's image is the one renderImage would give it alone.
+ * Returns when every job is done. No counterpart in the reference, which renders
+ * one job per call; this batches renderImage (render_image.hpp:36-49). */
+int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* stream);
+/* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
+ * iterations per captured CUDA graph (the autotuner's knobs). */
+int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph);
+/* Iterations the last wavefront run took. */
+int albedo_wavefront_last_iterations(int64_t* out);
 /* Renders the job once (path estimator, into scratch accumulators) while counting
  * traversal work: out_counts[0..4] = child boxes tested, triangles tested,
  * spheres tested, instances entered, ray queries traced. Synchronous. */
