@@ -70,10 +70,15 @@ WavefrontEngine::WavefrontEngine(int slot_count)
     int device{0};
     cudaCheck(cudaGetDevice(&device), "cudaGetDevice");
     cudaCheck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SM count");
+    cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "engine stream");
+    cudaCheck(cudaEventCreateWithFlags(&ordering_, cudaEventDisableTiming), "engine event");
 }
 
 WavefrontEngine::~WavefrontEngine()
 {
+    cudaStreamSynchronize(stream_);
+    cudaEventDestroy(ordering_);
+    cudaStreamDestroy(stream_);
     cudaFree(slab_);
     cudaFree(device_jobs_);
     cudaFreeHost(staging_jobs_);
@@ -89,11 +94,25 @@ void WavefrontEngine::setLaunch(int blocks_per_sm, int iterations_per_graph)
     iterations_per_graph_ = iterations_per_graph;
 }
 
-void WavefrontEngine::render(const std::vector<WfJob>& input, int stack, unsigned int* error_flag, cudaStream_t stream)
+void WavefrontEngine::render(const std::vector<WfJob>& input, int stack, unsigned int* error_flag,
+                             cudaStream_t caller)
 {
     if (input.empty()) {
         return;
     }
+    // Work runs on the engine's own stream (graphs cannot be captured on the
+    // legacy default stream), ordered after the caller's stream and before
+    // anything the caller enqueues next.
+    cudaCheck(cudaEventRecord(ordering_, caller), "ordering event");
+    cudaCheck(cudaStreamWaitEvent(stream_, ordering_, 0), "ordering wait");
+    renderOnOwnStream(input, stack, error_flag);
+    cudaCheck(cudaEventRecord(ordering_, stream_), "ordering event");
+    cudaCheck(cudaStreamWaitEvent(caller, ordering_, 0), "ordering wait");
+}
+
+void WavefrontEngine::renderOnOwnStream(const std::vector<WfJob>& input, int stack, unsigned int* error_flag)
+{
+    const cudaStream_t stream{stream_};
     const auto count{static_cast<int>(input.size())};
     if (count > job_capacity_) {
         cudaFree(device_jobs_);

@@ -32,6 +32,10 @@ public:
     void setLaunch(int blocks_per_sm, int iterations_per_graph);
 
 private:
+    void renderOnOwnStream(const std::vector<WfJob>& jobs, int stack, unsigned int* error_flag);
+
+    cudaStream_t stream_{nullptr};
+    cudaEvent_t ordering_{nullptr};
     WfBuffers buffers_{};
     void* slab_{nullptr};
     WfJob* device_jobs_{nullptr};
