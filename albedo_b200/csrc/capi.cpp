@@ -651,6 +651,31 @@ int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* str
     });
 }
 
+int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
+                          void* stream)
+{
+    return guarded([&] {
+        const long long pixels{static_cast<long long>(job->width) * static_cast<long long>(job->height)};
+        if (job->width > 0 && job->height > 0 && pixels > noAllocMaxPixels()) {
+            throw std::invalid_argument{std::format(
+                "albedo_render_noalloc renders images of at most {} pixels (one path slot per pixel in its static "
+                "scratch); {}x{} has {}",
+                noAllocMaxPixels(), job->width, job->height, pixels)};
+        }
+        const WfJob wf{wavefrontJob(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators))};
+        int device{0};
+        int sms{0};
+        check(cudaGetDevice(&device), "cudaGetDevice");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+        const cudaError_t e{renderNoAlloc(wf, scene->stack_capacity, 4 * sms, scene->error_flag.as<unsigned int>(),
+                                          static_cast<cudaStream_t>(stream))};
+        if (e == cudaErrorLaunchTimeout) {
+            throw DeviceError{"albedo_render_noalloc made no progress within its iteration bound"};
+        }
+        check(e, "albedo_render_noalloc");
+    });
+}
+
 int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph)
 {
     return guarded([&] { configureEngine(slot_count, blocks_per_sm, iterations_per_graph); });

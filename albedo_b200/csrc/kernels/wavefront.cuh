@@ -84,6 +84,10 @@ struct WfLaunch {
 cudaError_t wfPrepare(int stack);
 // Puts every slot in the regeneration queue with no job, and clears counters.
 cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream);
+// The allocation-free variant (noalloc.cu): one job, one path slot per pixel, all
+// scratch in a static device array; at most noAllocMaxPixels() pixels.
+int noAllocMaxPixels();
+cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int* error_flag, cudaStream_t stream);
 // Enqueues one iteration (regenerate, extend, shade x 4, shadow, advance).
 cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long total_items, const WfBuffers& b,
                         const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream);

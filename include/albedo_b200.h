@@ -185,6 +185,24 @@ typedef struct albedo_batch_item {
  * Returns when every job is done. No counterpart in the reference, which renders
  * one job per call; this batches renderImage (render_image.hpp:36-49). */
 int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* stream);
+/* Renders one job (path estimator) without allocating any device memory: no
+ * cudaMalloc, cudaFree or allocating library call. It has no counterpart in the
+ * reference, whose renderImage allocates nothing on a GPU because it has none.
+ * It is for callers that cannot allocate: a program whose device memory another
+ * allocator owns up front (a framework's caching pool that has reserved the
+ * GPU), or a loop with a latency budget, where an allocation can stall on the
+ * driver or synchronize the device. The wavefront's path slots, queues and
+ * control block live in a static device array of about 17 MB that every GPU
+ * loading the library holds until exit. It holds one path slot per pixel, so
+ * images are limited to 65,536 pixels; larger ones are rejected with
+ * ALBEDO_INVALID_ARGUMENT. The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture. All calls share the array and it keeps the last call's contents:
+ * each call clears what must start at zero, and calls that overlap on the GPU
+ * race, so do not overlap them. `accumulators` is a device array of width *
+ * height entries; the call returns after the render is complete on `stream`. */
+int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
+                          void* stream);
 /* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
  * iterations per captured CUDA graph (the autotuner's knobs). */
 int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph);
