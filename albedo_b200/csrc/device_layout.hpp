@@ -26,16 +26,25 @@ constexpr std::uint32_t kLeafFirstMask{0x0FFFFFFFu};
 constexpr std::uint32_t kEmptyChild{0xFFFFFFFFu};
 constexpr std::uint32_t kMaxLeafFirst{kLeafFirstMask};
 
+// A 4-wide node: two levels of the reference's binary BVH collapsed into one.
+// Child i's box is (lo_x[i], hi_x[i], lo_y[i], ...); absent children are
+// kEmptyChild. `order[o]` lists, for the ray octant o (bit a set when the
+// direction's component a is negative), the children in the order the
+// reference's depth-first, near-first traversal reaches them: 2 bits per child,
+// nearest first, low bits first.
 struct alignas(16) DevNode {
-    float c0_lo_x, c0_hi_x, c0_lo_y, c0_hi_y;
-    float c1_lo_x, c1_hi_x, c1_lo_y, c1_hi_y;
-    float c0_lo_z, c0_hi_z, c1_lo_z, c1_hi_z;
-    std::uint32_t child0;
-    std::uint32_t child1;
-    std::uint32_t axis; // split axis of this node: near child is child1 when dir[axis] < 0
+    float lo_x[4];
+    float hi_x[4];
+    float lo_y[4];
+    float hi_y[4];
+    float lo_z[4];
+    float hi_z[4];
+    std::uint32_t child[4];
+    std::uint8_t order[8];
+    std::uint32_t count; // children present (1..4); they are child[0..count-1]
     std::uint32_t pad;
 };
-static_assert(sizeof(DevNode) == 64);
+static_assert(sizeof(DevNode) == 128);
 
 // v0.w holds the triangle's index within its mesh (or, for scene triangles, its
 // index in the scene triangle table) as raw bits.

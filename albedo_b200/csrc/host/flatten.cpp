@@ -3,6 +3,8 @@
 // contiguous run; everything else becomes flat FP32 tables.
 #include "flatten.hpp"
 
+#include <algorithm>
+#include <array>
 #include <bit>
 #include <cmath>
 #include <format>
@@ -40,72 +42,135 @@ std::uint32_t leafRef(std::uint64_t first, std::uint32_t count)
 
 void setChildBox(DevNode& node, int child, const Box3& box)
 {
-    if (child == 0) {
-        node.c0_lo_x = roundDown(box.min.x);
-        node.c0_hi_x = roundUp(box.max.x);
-        node.c0_lo_y = roundDown(box.min.y);
-        node.c0_hi_y = roundUp(box.max.y);
-        node.c0_lo_z = roundDown(box.min.z);
-        node.c0_hi_z = roundUp(box.max.z);
-    } else {
-        node.c1_lo_x = roundDown(box.min.x);
-        node.c1_hi_x = roundUp(box.max.x);
-        node.c1_lo_y = roundDown(box.min.y);
-        node.c1_hi_y = roundUp(box.max.y);
-        node.c1_lo_z = roundDown(box.min.z);
-        node.c1_hi_z = roundUp(box.max.z);
-    }
+    node.lo_x[child] = roundDown(box.min.x);
+    node.hi_x[child] = roundUp(box.max.x);
+    node.lo_y[child] = roundDown(box.min.y);
+    node.hi_y[child] = roundUp(box.max.y);
+    node.lo_z[child] = roundDown(box.min.z);
+    node.hi_z[child] = roundUp(box.max.z);
 }
 
-// Emits the interior nodes of `bvh` (depth-first, first child at i + 1) as
-// child-box nodes; leaves index primitives from `prim_base` in leaf order.
-// Returns the device index of the root. A root that is itself a leaf gets a
-// node whose second child is empty.
-std::uint32_t emitBvh(const BuiltBvh& bvh, std::uint64_t prim_base, std::vector<DevNode>& out)
+struct Emitted {
+    std::uint32_t root{kEmptyChild};
+    // Most traversal-stack entries a query over this tree can hold at once.
+    std::uint32_t stack_need{0};
+};
+
+// Emits `bvh` (binary, depth-first, first child at i + 1) as 4-wide nodes, each
+// collapsing an interior node and its interior children. Leaves index
+// primitives from `prim_base` in leaf order. For every ray octant the node lists
+// its children in the order the reference's traversal (accel/bvh.hpp:239-278,
+// near child by the sign of the split axis) reaches them, so the order in which
+// leaves are visited is the reference's. A root that is a leaf gets a node with
+// that one child.
+Emitted emitBvh(const BuiltBvh& bvh, std::uint64_t prim_base, std::vector<DevNode>& out)
 {
-    const std::size_t n{bvh.nodes.size()};
-    std::vector<std::uint32_t> device_index(n, kEmptyChild);
-    const auto base{static_cast<std::uint32_t>(out.size())};
-    std::uint32_t next{base};
-    for (std::size_t i{0}; i < n; ++i) {
-        if (bvh.nodes[i].count == 0) {
-            device_index[i] = next++;
+    Emitted emitted;
+    if (bvh.nodes.empty()) {
+        return emitted;
+    }
+    const auto isLeaf = [&](std::size_t i) { return bvh.nodes[i].count != 0; };
+    const auto secondOf = [&](std::size_t i) { return static_cast<std::size_t>(bvh.nodes[i].offset); };
+    // Binary nodes that head a 4-wide node, and the 4-wide index of each.
+    std::vector<std::uint32_t> device_index(bvh.nodes.size(), kEmptyChild);
+    std::vector<std::size_t> heads{0};
+    device_index[0] = static_cast<std::uint32_t>(out.size());
+    out.emplace_back();
+    std::vector<std::uint32_t> need(bvh.nodes.size(), 0);
+    // Heads are discovered in order; their children are filled afterwards.
+    for (std::size_t h{0}; h < heads.size(); ++h) {
+        const std::size_t i{heads[h]};
+        std::vector<std::size_t> slots;
+        if (isLeaf(i)) {
+            slots.push_back(i);
+        } else {
+            for (const std::size_t x : {i + 1, secondOf(i)}) {
+                if (isLeaf(x)) {
+                    slots.push_back(x);
+                } else {
+                    slots.push_back(x + 1);
+                    slots.push_back(secondOf(x));
+                }
+            }
+        }
+        for (const std::size_t s : slots) {
+            if (!isLeaf(s) && device_index[s] == kEmptyChild) {
+                device_index[s] = static_cast<std::uint32_t>(out.size());
+                out.emplace_back();
+                heads.push_back(s);
+            }
         }
     }
-    const auto childRef = [&](std::size_t i) {
-        const BuildNode& node{bvh.nodes[i]};
-        return node.count != 0 ? leafRef(prim_base + node.offset, node.count) : device_index[i];
-    };
-    if (n == 0) {
-        return kEmptyChild;
-    }
-    if (bvh.nodes[0].count != 0) {
-        DevNode root{};
-        setChildBox(root, 0, bvh.nodes[0].bounds);
-        setChildBox(root, 1, Box3{{0, 0, 0}, {0, 0, 0}});
-        root.child0 = childRef(0);
-        root.child1 = kEmptyChild;
-        root.axis = 0;
-        out.push_back(root);
-        return base;
-    }
-    out.resize(next);
-    for (std::size_t i{0}; i < n; ++i) {
-        const BuildNode& node{bvh.nodes[i]};
-        if (node.count != 0) {
+    // Fill nodes bottom-up (heads in reverse discovery order) so stack needs of
+    // children are known when their parent is filled.
+    for (std::size_t h{heads.size()}; h-- > 0;) {
+        const std::size_t i{heads[h]};
+        DevNode& dev{out[device_index[i]]};
+        dev = DevNode{};
+        for (int c{0}; c < 4; ++c) {
+            dev.child[c] = kEmptyChild;
+        }
+        if (isLeaf(i)) {
+            setChildBox(dev, 0, bvh.nodes[i].bounds);
+            dev.child[0] = leafRef(prim_base + bvh.nodes[i].offset, bvh.nodes[i].count);
+            dev.count = 1;
             continue;
         }
-        DevNode& dev{out[device_index[i]]};
-        const std::size_t first{i + 1};
-        const std::size_t second{static_cast<std::size_t>(node.offset)};
-        setChildBox(dev, 0, bvh.nodes[first].bounds);
-        setChildBox(dev, 1, bvh.nodes[second].bounds);
-        dev.child0 = childRef(first);
-        dev.child1 = childRef(second);
-        dev.axis = node.axis;
-        dev.pad = 0;
+        // Groups: the first and second child of i, each a leaf or two children.
+        struct Group {
+            std::size_t node;
+            int first_slot;
+            int size;
+        };
+        std::array<Group, 2> groups{};
+        int slot{0};
+        const std::array<std::size_t, 2> halves{i + 1, secondOf(i)};
+        for (int g{0}; g < 2; ++g) {
+            const std::size_t x{halves[g]};
+            groups[g] = {x, slot, isLeaf(x) ? 1 : 2};
+            const std::array<std::size_t, 2> kids{x + 1, isLeaf(x) ? 0 : secondOf(x)};
+            for (int k{0}; k < groups[g].size; ++k) {
+                const std::size_t s{isLeaf(x) ? x : kids[k]};
+                setChildBox(dev, slot, bvh.nodes[s].bounds);
+                dev.child[slot] = isLeaf(s) ? leafRef(prim_base + bvh.nodes[s].offset, bvh.nodes[s].count)
+                                            : device_index[s];
+                ++slot;
+            }
+        }
+        dev.count = static_cast<std::uint32_t>(slot);
+        for (unsigned octant{0}; octant < 8; ++octant) {
+            const bool swap{((octant >> bvh.nodes[i].axis) & 1U) != 0};
+            std::uint8_t packed{0};
+            int position{0};
+            for (int g{0}; g < 2; ++g) {
+                const Group& group{groups[swap ? 1 - g : g]};
+                if (group.size == 1) {
+                    packed |= static_cast<std::uint8_t>(group.first_slot << (2 * position++));
+                } else {
+                    const bool inner_swap{((octant >> bvh.nodes[group.node].axis) & 1U) != 0};
+                    packed |= static_cast<std::uint8_t>((group.first_slot + (inner_swap ? 1 : 0)) << (2 * position++));
+                    packed |= static_cast<std::uint8_t>((group.first_slot + (inner_swap ? 0 : 1)) << (2 * position++));
+                }
+            }
+            dev.order[octant] = packed;
+        }
+        // Stack need: pushes here (count - 1) plus the deepest interior child's need.
+        std::uint32_t child_need{0};
+        for (int g{0}; g < 2; ++g) {
+            const std::size_t x{halves[g]};
+            const std::array<std::size_t, 2> kids{x + 1, isLeaf(x) ? 0 : secondOf(x)};
+            for (int k{0}; k < groups[g].size; ++k) {
+                const std::size_t s{isLeaf(x) ? x : kids[k]};
+                if (!isLeaf(s)) {
+                    child_need = std::max(child_need, need[s]);
+                }
+            }
+        }
+        need[i] = dev.count - 1 + child_need;
     }
-    return base;
+    emitted.root = device_index[0];
+    emitted.stack_need = need[0];
+    return emitted;
 }
 
 float f32(double x) { return static_cast<float>(x); }
@@ -218,7 +283,7 @@ DeviceImage flattenScene(const HostScene& scene)
         image.attrs.push_back(deviceAttr(scene.triangles[i], nullptr));
     }
     std::vector<std::uint32_t> mesh_root(scene.meshes.size(), kEmptyChild);
-    std::uint32_t max_blas_depth{0};
+    std::uint32_t max_blas_need{0};
     for (std::size_t m{0}; m < scene.meshes.size(); ++m) {
         const MeshDesc& mesh{scene.meshes[m]};
         const std::uint64_t base{image.triangles.size()};
@@ -227,15 +292,19 @@ DeviceImage flattenScene(const HostScene& scene)
             image.triangles.push_back(deviceTriangle(mesh.triangles[t], t));
             image.attrs.push_back(deviceAttr(mesh.triangles[t], mesh.corner_normals.empty() ? nullptr : &mesh.corner_normals[t]));
         }
-        mesh_root[m] = emitBvh(mesh.bvh, base, image.nodes);
-        max_blas_depth = std::max(max_blas_depth, mesh.bvh.max_depth);
+        const Emitted blas{emitBvh(mesh.bvh, base, image.nodes)};
+        mesh_root[m] = blas.root;
+        max_blas_need = std::max(max_blas_need, blas.stack_need);
     }
     if (image.triangles.size() > kMaxLeafFirst) {
         throw std::invalid_argument{std::format("scene has more than {} triangles", kMaxLeafFirst)};
     }
 
-    image.tlas_root = emitBvh(scene.tlas, 0, image.nodes);
-    image.stack_need = scene.tlas.max_depth + max_blas_depth + 3;
+    const Emitted tlas{emitBvh(scene.tlas, 0, image.nodes)};
+    image.tlas_root = tlas.root;
+    // TLAS pushes, then a resume entry and an exit marker when entering an
+    // instance, then the deepest BLAS's pushes.
+    image.stack_need = tlas.stack_need + 2 + max_blas_need;
 
     image.object_position.assign(scene.objects.size(), 0);
     for (std::size_t pos{0}; pos < scene.tlas.order.size(); ++pos) {

@@ -34,6 +34,35 @@ struct RenderArgs {
 // the scene's hierarchy is deeper than every compiled variant supports.
 int stackCapacityFor(std::uint32_t stack_need);
 
+// Traversal-stack capacities the kernels are compiled for (8 bytes per entry per
+// thread of shared memory; 48 entries keep four 128-thread blocks per SM).
+template <int S>
+struct StackSize {
+    static constexpr int value = S;
+};
+
+// Calls f(StackSize<S>{}) for the compiled capacity S that `capacity` names.
+template <typename F>
+auto withStack(int capacity, F&& f)
+{
+    if (capacity <= 32) {
+        return f(StackSize<32>{});
+    }
+    if (capacity <= 48) {
+        return f(StackSize<48>{});
+    }
+    return f(StackSize<64>{});
+}
+
+// Lets `kernel` use `entries` stack entries of dynamic shared memory per thread
+// in 128-thread blocks (above the 48 KB default when needed).
+template <typename Kernel>
+cudaError_t allowStackMemory(Kernel kernel, int entries)
+{
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                entries * 128 * static_cast<int>(sizeof(uint2)));
+}
+
 // The plain megakernel: one thread per pixel, serial over that pixel's n x n
 // stratified samples so each pixel's PCG32 stream is consumed as the
 // reference consumes it. Adds into `accum` (one PixelAccum per pixel, or per

@@ -160,61 +160,27 @@ __global__ void __launch_bounds__(kBlock) occludedKernel(const DevScene scene, c
 
 constexpr std::size_t stackBytes(int stack) { return static_cast<std::size_t>(stack) * kBlock * sizeof(uint2); }
 
-// Opts a kernel into the dynamic shared memory its stack needs (above the 48 KB
-// default for 64-entry stacks); done once per kernel.
-template <typename Kernel>
-cudaError_t launchWithStack(Kernel kernel, int stack, int blocks, cudaStream_t stream, bool& configured)
+int megaBlocks(const RenderArgs& args)
 {
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   static_cast<int>(stackBytes(stack)));
-        if (e != cudaSuccess) {
-            return e;
-        }
-        configured = true;
+    if (args.pixels != nullptr) {
+        return (args.pixel_count + kBlock - 1) / kBlock;
     }
-    (void)blocks;
-    (void)stream;
-    return cudaSuccess;
+    return ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
 }
 
-template <int STACK>
-cudaError_t launchMegaStack(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
-                            unsigned int* error_flag, cudaStream_t stream)
+// Launches `kernel` over `blocks` blocks with a STACK-entry shared-memory stack.
+template <int STACK, typename Kernel, typename... Args>
+cudaError_t launchStacked(Kernel kernel, int blocks, cudaStream_t stream, Args... args)
 {
-    int blocks;
-    if (args.pixels != nullptr) {
-        blocks = (args.pixel_count + kBlock - 1) / kBlock;
-    } else {
-        blocks = ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
-    }
     if (blocks == 0) {
         return cudaSuccess;
     }
-    static bool configured[3] = {false, false, false};
-    const std::size_t smem = stackBytes(STACK);
-    cudaError_t e = cudaSuccess;
-    switch (args.estimator) {
-    case kEstimatorScatterOnly:
-        e = launchWithStack(megakernel<STACK, kEstimatorScatterOnly>, STACK, blocks, stream, configured[1]);
-        if (e == cudaSuccess) {
-            megakernel<STACK, kEstimatorScatterOnly><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
-        }
-        break;
-    case kEstimatorNormals:
-        e = launchWithStack(megakernel<STACK, kEstimatorNormals>, STACK, blocks, stream, configured[2]);
-        if (e == cudaSuccess) {
-            megakernel<STACK, kEstimatorNormals><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
-        }
-        break;
-    default:
-        e = launchWithStack(megakernel<STACK, kEstimatorPath>, STACK, blocks, stream, configured[0]);
-        if (e == cudaSuccess) {
-            megakernel<STACK, kEstimatorPath><<<blocks, kBlock, smem, stream>>>(scene, camera, args, accum, error_flag);
-        }
-        break;
+    const cudaError_t e = allowStackMemory(kernel, STACK);
+    if (e != cudaSuccess) {
+        return e;
     }
-    return e != cudaSuccess ? e : cudaGetLastError();
+    kernel<<<blocks, kBlock, stackBytes(STACK), stream>>>(args...);
+    return cudaGetLastError();
 }
 
 } // namespace
@@ -223,37 +189,20 @@ cudaError_t launchMegakernelCounting(const DevScene& scene, const DevCamera& cam
                                      PixelAccum* accum, unsigned int* error_flag, int stack_capacity,
                                      unsigned long long* totals, cudaStream_t stream)
 {
-    int blocks;
-    if (args.pixels != nullptr) {
-        blocks = (args.pixel_count + kBlock - 1) / kBlock;
-    } else {
-        blocks = ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
-    }
-    if (blocks == 0) {
-        return cudaSuccess;
-    }
-    static bool configured[2] = {false, false};
-    cudaError_t e;
-    if (stack_capacity == 32) {
-        e = launchWithStack(megakernel<32, kEstimatorPath, true>, 32, blocks, stream, configured[0]);
-        if (e == cudaSuccess) {
-            megakernel<32, kEstimatorPath, true>
-                <<<blocks, kBlock, stackBytes(32), stream>>>(scene, camera, args, accum, error_flag, totals);
-        }
-    } else {
-        e = launchWithStack(megakernel<64, kEstimatorPath, true>, 64, blocks, stream, configured[1]);
-        if (e == cudaSuccess) {
-            megakernel<64, kEstimatorPath, true>
-                <<<blocks, kBlock, stackBytes(64), stream>>>(scene, camera, args, accum, error_flag, totals);
-        }
-    }
-    return e != cudaSuccess ? e : cudaGetLastError();
+    return withStack(stack_capacity, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        return launchStacked<S>(megakernel<S, kEstimatorPath, true>, megaBlocks(args), stream, scene, camera, args,
+                                accum, error_flag, totals);
+    });
 }
 
 int stackCapacityFor(std::uint32_t stack_need)
 {
     if (stack_need <= 32u) {
         return 32;
+    }
+    if (stack_need <= 48u) {
+        return 48;
     }
     if (stack_need <= 64u) {
         return 64;
@@ -264,56 +213,41 @@ int stackCapacityFor(std::uint32_t stack_need)
 cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
                              unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
 {
-    if (stack_capacity == 32) {
-        return launchMegaStack<32>(scene, camera, args, accum, error_flag, stream);
-    }
-    return launchMegaStack<64>(scene, camera, args, accum, error_flag, stream);
+    return withStack(stack_capacity, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        unsigned long long* no_totals = nullptr;
+        switch (args.estimator) {
+        case kEstimatorScatterOnly:
+            return launchStacked<S>(megakernel<S, kEstimatorScatterOnly>, megaBlocks(args), stream, scene, camera,
+                                    args, accum, error_flag, no_totals);
+        case kEstimatorNormals:
+            return launchStacked<S>(megakernel<S, kEstimatorNormals>, megaBlocks(args), stream, scene, camera, args,
+                                    accum, error_flag, no_totals);
+        default:
+            return launchStacked<S>(megakernel<S, kEstimatorPath>, megaBlocks(args), stream, scene, camera, args,
+                                    accum, error_flag, no_totals);
+        }
+    });
 }
 
 cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
                         const TraceOutputs& out, unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
 {
-    const int blocks = (count + kBlock - 1) / kBlock;
-    if (blocks == 0) {
-        return cudaSuccess;
-    }
-    static bool configured[2] = {false, false};
-    cudaError_t e;
-    if (stack_capacity == 32) {
-        e = launchWithStack(traceKernel<32>, 32, blocks, stream, configured[0]);
-        if (e == cudaSuccess) {
-            traceKernel<32><<<blocks, kBlock, stackBytes(32), stream>>>(scene, rays, count, t_min, t_max, out, error_flag);
-        }
-    } else {
-        e = launchWithStack(traceKernel<64>, 64, blocks, stream, configured[1]);
-        if (e == cudaSuccess) {
-            traceKernel<64><<<blocks, kBlock, stackBytes(64), stream>>>(scene, rays, count, t_min, t_max, out, error_flag);
-        }
-    }
-    return e != cudaSuccess ? e : cudaGetLastError();
+    return withStack(stack_capacity, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        return launchStacked<S>(traceKernel<S>, (count + kBlock - 1) / kBlock, stream, scene, rays, count, t_min,
+                                t_max, out, error_flag);
+    });
 }
 
 cudaError_t launchOccluded(const DevScene& scene, const float* rays, const float* t_max, int count, int* occluded_out,
                            unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
 {
-    const int blocks = (count + kBlock - 1) / kBlock;
-    if (blocks == 0) {
-        return cudaSuccess;
-    }
-    static bool configured[2] = {false, false};
-    cudaError_t e;
-    if (stack_capacity == 32) {
-        e = launchWithStack(occludedKernel<32>, 32, blocks, stream, configured[0]);
-        if (e == cudaSuccess) {
-            occludedKernel<32><<<blocks, kBlock, stackBytes(32), stream>>>(scene, rays, t_max, count, occluded_out, error_flag);
-        }
-    } else {
-        e = launchWithStack(occludedKernel<64>, 64, blocks, stream, configured[1]);
-        if (e == cudaSuccess) {
-            occludedKernel<64><<<blocks, kBlock, stackBytes(64), stream>>>(scene, rays, t_max, count, occluded_out, error_flag);
-        }
-    }
-    return e != cudaSuccess ? e : cudaGetLastError();
+    return withStack(stack_capacity, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        return launchStacked<S>(occludedKernel<S>, (count + kBlock - 1) / kBlock, stream, scene, rays, t_max, count,
+                                occluded_out, error_flag);
+    });
 }
 
 } // namespace albedo_b200

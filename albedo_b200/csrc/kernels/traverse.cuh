@@ -305,33 +305,57 @@ static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 ori
     std::uint32_t ref = s.tlas_root;
     for (;;) {
         if ((ref & kLeafBit) == 0u) {
+            // A 4-wide node: test every child box, then continue with the hit child
+            // the reference reaches first and push the others, last first.
             const float4* np = reinterpret_cast<const float4*>(s.nodes + ref);
-            const float4 n0 = __ldg(np);
-            const float4 n1 = __ldg(np + 1);
-            const float4 n2 = __ldg(np + 2);
-            const uint4 n3 = __ldg(reinterpret_cast<const uint4*>(np + 3));
+            const float4 lx = __ldg(np);
+            const float4 hx = __ldg(np + 1);
+            const float4 ly = __ldg(np + 2);
+            const float4 hy = __ldg(np + 3);
+            const float4 lz = __ldg(np + 4);
+            const float4 hz = __ldg(np + 5);
+            const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
+            const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
+            const int present = static_cast<int>(meta.z);
             if (counts != nullptr) {
-                counts->boxes += (n3.x != kEmptyChild ? 1u : 0u) + (n3.y != kEmptyChild ? 1u : 0u);
+                counts->boxes += static_cast<unsigned>(present);
             }
-            float e0, e1;
-            const bool h0 = n3.x != kEmptyChild && slabTest(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, r, tmin, tmax, e0);
-            const bool h1 = n3.y != kEmptyChild && slabTest(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, r, tmin, tmax, e1);
-            if (h0 && h1) {
-                if (sp >= stack_size) {
+            float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
+            unsigned mask = slabTest(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, tmin, tmax, e0) ? 1u : 0u;
+            if (present > 1 && slabTest(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, tmin, tmax, e1)) {
+                mask |= 2u;
+            }
+            if (present > 2 && slabTest(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, tmin, tmax, e2)) {
+                mask |= 4u;
+            }
+            if (present > 3 && slabTest(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, tmin, tmax, e3)) {
+                mask |= 8u;
+            }
+            if (mask != 0u) {
+                int remaining = __popc(mask);
+                if (sp + remaining - 1 > stack_size) {
                     atomicOr(error_flag, 1u);
                     return found;
                 }
-                const bool second_first = ((r.neg >> n3.z) & 1u) != 0u;
-                const std::uint32_t near_ref = second_first ? n3.y : n3.x;
-                const std::uint32_t far_ref = second_first ? n3.x : n3.y;
-                const float far_entry = second_first ? e0 : e1;
-                stack[sp * stride] = make_uint2(far_ref, __float_as_uint(far_entry));
-                ++sp;
-                ref = near_ref;
-                continue;
-            }
-            if (h0 || h1) {
-                ref = h0 ? n3.x : n3.y;
+                const unsigned packed = (r.neg < 4u ? (meta.x >> (8u * r.neg)) : (meta.y >> (8u * (r.neg - 4u)))) & 0xFFu;
+#pragma unroll
+                for (int position = 3; position >= 0; --position) {
+                    if (position >= present) {
+                        continue;
+                    }
+                    const unsigned c = (packed >> (2 * position)) & 3u;
+                    if (((mask >> c) & 1u) == 0u) {
+                        continue;
+                    }
+                    const std::uint32_t child = c == 0u ? ch.x : (c == 1u ? ch.y : (c == 2u ? ch.z : ch.w));
+                    if (--remaining == 0) {
+                        ref = child;
+                    } else {
+                        const float entry = c == 0u ? e0 : (c == 1u ? e1 : (c == 2u ? e2 : e3));
+                        stack[sp * stride] = make_uint2(child, __float_as_uint(entry));
+                        ++sp;
+                    }
+                }
                 continue;
             }
         } else {

@@ -357,34 +357,15 @@ __global__ void resetKernel(WfBuffers b)
     }
 }
 
-template <typename Kernel>
-cudaError_t allowStack(Kernel kernel, int stack, bool& configured)
-{
-    if (configured) {
-        return cudaSuccess;
-    }
-    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               stack * 128 * static_cast<int>(sizeof(uint2)));
-    configured = e == cudaSuccess;
-    return e;
-}
-
 } // namespace
 
 cudaError_t wfPrepare(int stack)
 {
-    static bool configured[4] = {false, false, false, false};
-    cudaError_t e;
-    if (stack == 32) {
-        if ((e = allowStack(extendKernel<32>, 32, configured[0])) != cudaSuccess) {
-            return e;
-        }
-        return allowStack(shadowKernel<32>, 32, configured[1]);
-    }
-    if ((e = allowStack(extendKernel<64>, 64, configured[2])) != cudaSuccess) {
-        return e;
-    }
-    return allowStack(shadowKernel<64>, 64, configured[3]);
+    return withStack(stack, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        const cudaError_t e = allowStackMemory(extendKernel<S>, S);
+        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S>, S);
+    });
 }
 
 cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream)
@@ -398,22 +379,22 @@ cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long tot
                         const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream)
 {
     const int g = launch.blocks;
-    const std::size_t smem = static_cast<std::size_t>(launch.stack) * 128 * sizeof(uint2);
+    const auto smemFor = [](int entries) { return static_cast<std::size_t>(entries) * 128 * sizeof(uint2); };
     regenKernel<<<g, 128, 0, stream>>>(jobs, job_count, total_items, b);
-    if (launch.stack == 32) {
-        extendKernel<32><<<g, 128, smem, stream>>>(jobs, b, error_flag);
-    } else {
-        extendKernel<64><<<g, 128, smem, stream>>>(jobs, b, error_flag);
-    }
+    withStack(launch.stack, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        extendKernel<S><<<g, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        return 0;
+    });
     shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
     shadeKernel<kClassConductor><<<g, 128, 0, stream>>>(jobs, b);
     shadeKernel<kClassDielectric><<<g, 128, 0, stream>>>(jobs, b);
     shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
-    if (launch.stack == 32) {
-        shadowKernel<32><<<g, 128, smem, stream>>>(jobs, b, error_flag);
-    } else {
-        shadowKernel<64><<<g, 128, smem, stream>>>(jobs, b, error_flag);
-    }
+    withStack(launch.stack, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        shadowKernel<S><<<g, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        return 0;
+    });
     advanceKernel<<<1, 1, 0, stream>>>(b.control);
     return cudaGetLastError();
 }

@@ -60,7 +60,70 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--method", choices=["megakernel", "wavefront"], default="megakernel")
+    p.add_argument("--workload", choices=["trefoil", "batched"], default="trefoil",
+                   help="trefoil: the instanced-mesh frame (default); batched: 64 seeded jobs of uneven size")
     return p.parse_args()
+
+
+def run_batched(args) -> None:
+    """64 seeded jobs of uneven size (displaced icospheres of 1k-500k triangles,
+    0-8 spheres, mixed materials, 128x72..1024x576, 4-64 spp), one scene each:
+    the plain megakernel serving them one at a time (a synchronize after each)
+    against one batched wavefront run of all of them. Each step renders every job
+    once; value is the batched form's Mpaths/s."""
+    import torch
+
+    import albedo_b200 as ab
+    from albedo_b200 import scenes
+
+    tmp = tempfile.TemporaryDirectory()
+    jobs = scenes.batch_jobs(Path(tmp.name), count=64)
+    loaded = {j.scene: ab.Scene.load(j.scene) for j in jobs}
+    paths = sum(j.width * j.height * j.samples_per_axis ** 2 for j in jobs)
+    accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for j in jobs]
+
+    def rjob(j, method):
+        return ab.RenderJob(j.width, j.height, samples_per_axis=j.samples_per_axis, seed=j.seed, max_depth=8,
+                            method=method)
+
+    def one_at_a_time():
+        for j, a in zip(jobs, accs):
+            ab.render_device(loaded[j.scene], rjob(j, ab.MEGAKERNEL), a.data_ptr())
+            torch.cuda.synchronize()
+
+    def batched():
+        ab.render_batch([(loaded[j.scene], rjob(j, ab.WAVEFRONT), a.data_ptr()) for j, a in zip(jobs, accs)])
+        torch.cuda.synchronize()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ms = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            start = time.perf_counter()
+            fn()
+            ms.append((time.perf_counter() - start) * 1e3)
+        return ms
+
+    with ClockSampler(0) as clocks:
+        batch_ms = timed(batched)
+        mega_ms = timed(one_at_a_time)
+    for s in loaded.values():
+        s.check()
+    value = paths * args.steps / (sum(batch_ms) / 1e3) / 1e6
+    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(batch_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
+            "config": {"workload": "batched_64_jobs_mixed", "jobs": len(jobs), "paths_per_step": paths,
+                       "max_depth": 8, "method": "wavefront batch (one run for all jobs)",
+                       "jobs_detail": [[j.width, j.height, j.samples_per_axis ** 2] for j in jobs]},
+            "megakernel_one_at_a_time": {"value": paths * args.steps / (sum(mega_ms) / 1e3) / 1e6,
+                                         "unit": "Mpaths/s", "ms_per_step": statistics.mean(mega_ms)},
+            "wavefront_iterations": ab.wavefront_last_iterations(),
+            "timing": "wall clock around each step, device synchronized on both sides",
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
 
 
 def config(method: str, n_gpus: int) -> dict:
@@ -210,6 +273,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
         return
 
     import torch
