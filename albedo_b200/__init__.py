@@ -320,6 +320,44 @@ def render_batch(items, stream: int = 0) -> None:
     _raise(library().albedo_render_batch(array, len(items), c_void_p(stream)))
 
 
+class Server:
+    """Continuous-batching render server (albedo_server_* in the C ABI)."""
+
+    def __init__(self, memory_budget_bytes: int = 150 << 30, slots: int = 1 << 20):
+        handle = c_void_p()
+        _raise(library().albedo_server_create(memory_budget_bytes, slots, byref(handle)))
+        self._handle = handle
+
+    def submit(self, scene: Scene, job: RenderJob, accumulators_ptr: int) -> int:
+        c = job.to_c()
+        ticket = ctypes.c_int64()
+        _raise(library().albedo_server_submit(self._handle, scene.handle, byref(c), c_void_p(accumulators_ptr),
+                                              byref(ticket)))
+        return ticket.value
+
+    def step(self, capacity: int = 4096) -> list[int]:
+        out = (ctypes.c_int64 * capacity)()
+        count = c_int32()
+        _raise(library().albedo_server_step(self._handle, out, capacity, byref(count)))
+        return [out[i] for i in range(count.value)]
+
+    def pending(self) -> tuple[int, int]:
+        waiting, running = c_int32(), c_int32()
+        _raise(library().albedo_server_pending(self._handle, byref(waiting), byref(running)))
+        return waiting.value, running.value
+
+    def close(self) -> None:
+        if self._handle is not None and self._handle.value:
+            library().albedo_server_destroy(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def wavefront_configure(slots: int = 1 << 20, blocks_per_sm: int = 8, iterations_per_graph: int = 4) -> None:
     """Shape of the wavefront engine: path slots, queue-kernel blocks per SM, iterations per graph."""
     _raise(library().albedo_wavefront_configure(slots, blocks_per_sm, iterations_per_graph))

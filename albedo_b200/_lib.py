@@ -71,6 +71,11 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render_batch": (c_int32, [c_void_p, c_int32, c_void_p]),
     "albedo_render_noalloc": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
     "albedo_wavefront_configure": (c_int32, [c_int32, c_int32, c_int32]),
+    "albedo_server_create": (c_int32, [c_int64, c_int32, POINTER(c_void_p)]),
+    "albedo_server_submit": (c_int32, [c_void_p, c_void_p, POINTER(RenderJobC), c_void_p, POINTER(c_int64)]),
+    "albedo_server_step": (c_int32, [c_void_p, POINTER(c_int64), c_int32, POINTER(c_int32)]),
+    "albedo_server_pending": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
+    "albedo_server_destroy": (None, [c_void_p]),
     "albedo_wavefront_last_iterations": (c_int32, [POINTER(c_int64)]),
     "albedo_trace_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, _I, _F, _I, _I, _F, _F, _F, _I]),
     "albedo_occluded_host": (c_int32, [c_void_p, _F, _F, c_int64, _I]),

@@ -9,7 +9,10 @@
 #include "wavefront_engine.hpp"
 
 #include <algorithm>
+#include <deque>
+#include <map>
 #include <mutex>
+#include <set>
 
 #include <cuda_runtime_api.h>
 
@@ -311,6 +314,7 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
 
 // The process's wavefront engine on the current device, created on first use.
 constexpr int kDefaultSlots{1 << 20};
+constexpr int kBatchJobCapacity{4096};
 std::mutex g_engine_mutex;
 std::unique_ptr<WavefrontEngine> g_engine;
 int g_engine_slots{kDefaultSlots};
@@ -361,7 +365,7 @@ void runWavefront(const std::vector<WfJob>& jobs, int stack, unsigned int* error
     const std::lock_guard lock{g_engine_mutex};
     try {
         if (!g_engine) {
-            g_engine = std::make_unique<WavefrontEngine>(g_engine_slots);
+            g_engine = std::make_unique<WavefrontEngine>(g_engine_slots, kBatchJobCapacity);
         }
         g_engine->setLaunch(g_engine_blocks_per_sm, g_engine_iterations_per_graph);
         g_engine->render(jobs, stack, error_flag, stream);
@@ -374,6 +378,69 @@ void runWavefront(const std::vector<WfJob>& jobs, int stack, unsigned int* error
         throw DeviceError{e.what()};
     }
 }
+
+} // namespace
+
+// A request server: continuous batching over one wavefront engine, with
+// admission against a device-memory budget.
+struct albedo_server {
+    struct Request {
+        std::int64_t ticket{};
+        const albedo_scene* scene{};
+        WfJob job{};
+        std::int64_t bytes{};
+    };
+
+    std::unique_ptr<WavefrontEngine> engine;
+    std::int64_t budget{0};
+    std::int64_t used{0};
+    int stack{32};
+    std::int64_t next_ticket{1};
+    std::deque<Request> waiting;
+    std::map<int, Request> running; // engine job index -> request
+    std::set<const albedo_scene*> resident;
+    std::deque<std::int64_t> finished; // tickets not yet handed to the caller
+
+    std::int64_t sceneBytes(const albedo_scene* scene) const
+    {
+        return resident.contains(scene) ? 0 : static_cast<std::int64_t>(scene->deviceBytes());
+    }
+
+    // Admits waiting requests in arrival order while they fit the budget.
+    void admit()
+    {
+        while (!waiting.empty()) {
+            Request& head{waiting.front()};
+            const std::int64_t need{head.bytes + sceneBytes(head.scene)};
+            if (used + need > budget) {
+                return;
+            }
+            const int head_stack{head.scene->stack_capacity};
+            const bool table_full{submitted_in_batch >= engine->jobCapacity()};
+            if (engine->isOpen() && (head_stack > stack || table_full)) {
+                if (!running.empty()) {
+                    return; // wait for the batch to drain, then reopen
+                }
+                engine->close();
+            }
+            if (!engine->isOpen()) {
+                stack = std::max(stack, head_stack);
+                engine->open(stack, head.scene->error_flag.as<unsigned int>());
+                submitted_in_batch = 0;
+            }
+            used += need;
+            resident.insert(head.scene);
+            const int index{engine->submit(head.job)};
+            ++submitted_in_batch;
+            running.emplace(index, head);
+            waiting.pop_front();
+        }
+    }
+
+    int submitted_in_batch{0};
+};
+
+namespace {
 
 void renderOnDevice(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum, cudaStream_t stream)
 {
@@ -680,6 +747,106 @@ int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_
 {
     return guarded([&] { configureEngine(slot_count, blocks_per_sm, iterations_per_graph); });
 }
+
+int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo_server** out)
+{
+    *out = nullptr;
+    return guarded([&] {
+        if (memory_budget_bytes <= 0 || slot_count <= 0) {
+            throw std::invalid_argument{"the server needs a positive memory budget and slot count"};
+        }
+        auto server{std::make_unique<albedo_server>()};
+        try {
+            server->engine = std::make_unique<WavefrontEngine>(slot_count, kBatchJobCapacity);
+        } catch (const std::bad_alloc&) {
+            throw;
+        } catch (const std::exception& e) {
+            throw DeviceError{e.what()};
+        }
+        server->budget = memory_budget_bytes;
+        server->used = static_cast<std::int64_t>(server->engine->deviceBytes());
+        if (server->used > server->budget) {
+            throw std::invalid_argument{std::format("the server's path slots alone ({} bytes) exceed the budget",
+                                                    server->used)};
+        }
+        *out = server.release();
+    });
+}
+
+int albedo_server_submit(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
+                         albedo_accumulator* accumulators, int64_t* out_ticket)
+{
+    return guarded([&] {
+        albedo_server::Request request;
+        request.ticket = server->next_ticket++;
+        request.scene = scene;
+        request.job = wavefrontJob(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators));
+        request.bytes = static_cast<std::int64_t>(job->width) * job->height * static_cast<std::int64_t>(sizeof(PixelAccum));
+        const std::int64_t fixed{static_cast<std::int64_t>(server->engine->deviceBytes())};
+        if (fixed + request.bytes + static_cast<std::int64_t>(scene->deviceBytes()) > server->budget) {
+            throw std::invalid_argument{"the request alone exceeds the server's memory budget"};
+        }
+        server->waiting.push_back(request);
+        try {
+            server->admit();
+        } catch (const std::invalid_argument&) {
+            throw;
+        } catch (const std::bad_alloc&) {
+            throw;
+        } catch (const std::exception& e) {
+            throw DeviceError{e.what()};
+        }
+        *out_ticket = request.ticket;
+    });
+}
+
+int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacity, int32_t* out_finished)
+{
+    return guarded([&] {
+        *out_finished = 0;
+        const auto report = [&] {
+            while (!server->finished.empty() && *out_finished < capacity) {
+                finished[(*out_finished)++] = server->finished.front();
+                server->finished.pop_front();
+            }
+        };
+        try {
+            server->admit();
+            if (!server->engine->isOpen() || server->running.empty()) {
+                report();
+                return;
+            }
+            server->engine->step();
+            for (const int index : server->engine->poll()) {
+                const auto found{server->running.find(index)};
+                if (found == server->running.end()) {
+                    continue;
+                }
+                server->finished.push_back(found->second.ticket);
+                server->used -= found->second.bytes;
+                server->running.erase(found);
+            }
+            server->admit();
+            report();
+        } catch (const std::invalid_argument&) {
+            throw;
+        } catch (const std::bad_alloc&) {
+            throw;
+        } catch (const std::exception& e) {
+            throw DeviceError{e.what()};
+        }
+    });
+}
+
+int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int32_t* out_running)
+{
+    return guarded([&] {
+        *out_waiting = static_cast<int32_t>(server->waiting.size());
+        *out_running = static_cast<int32_t>(server->running.size());
+    });
+}
+
+void albedo_server_destroy(albedo_server* server) { delete server; }
 
 int albedo_wavefront_last_iterations(int64_t* out)
 {

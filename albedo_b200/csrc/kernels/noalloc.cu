@@ -33,7 +33,8 @@ constexpr std::size_t kU2 = alignUp(sizeof(ulonglong2) * kNoAllocMaxSlots);
 constexpr std::size_t kQueue = alignUp(sizeof(int) * kNoAllocMaxSlots);
 constexpr std::size_t kControl = alignUp(sizeof(WfControl));
 constexpr std::size_t kJob = alignUp(sizeof(WfJob));
-constexpr std::size_t kScratchBytes = 12 * kF4 + kF2 + kU2 + kQueueCount * kQueue + kControl + kJob;
+constexpr std::size_t kJobDone = alignUp(sizeof(unsigned long long));
+constexpr std::size_t kScratchBytes = 12 * kF4 + kF2 + kU2 + kQueueCount * kQueue + kControl + kJob + kJobDone;
 
 // The scratch. In host code this name is a host-side stand-in, not a device
 // address; the host passes the address cudaGetSymbolAddress returns.
@@ -95,6 +96,7 @@ WfBuffers carve(void* base, int slots, WfJob** job)
     }
     b.control = static_cast<WfControl*>(take(kControl));
     *job = static_cast<WfJob*>(take(kJob));
+    b.job_done = static_cast<unsigned long long*>(take(kJobDone));
     b.slot_count = slots;
     return b;
 }
@@ -129,7 +131,7 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
         return e;
     }
     const auto total = static_cast<unsigned long long>(pixels);
-    if ((e = wfReset(buffers, total, stream)) != cudaSuccess) {
+    if ((e = wfReset(buffers, total, 1, stream)) != cudaSuccess) {
         return e;
     }
     const WfLaunch launch{blocks, 128, stack};
@@ -141,7 +143,7 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
     WfControl snapshot{};
     for (unsigned long long done = 0; done <= bound; done += kIterationsPerCheck) {
         for (int i = 0; i < kIterationsPerCheck; ++i) {
-            if ((e = wfIteration(device_job, 1, total, buffers, launch, error_flag, stream)) != cudaSuccess) {
+            if ((e = wfIteration(device_job, buffers, launch, error_flag, stream)) != cudaSuccess) {
                 return e;
             }
         }

@@ -103,11 +103,12 @@ ALB_DEV void loadPath(const WfSlots& sl, int s, int depth, PathState& p)
     p.depth = depth;
 }
 
-__global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ jobs, int job_count,
-                                                   unsigned long long total_items, WfBuffers b)
+__global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ jobs, WfBuffers b)
 {
     WfControl* ctl = b.control;
     const int parity = ctl->parity;
+    const unsigned long long total_items = ctl->total_items;
+    const int job_count = ctl->job_count;
     const int in = kQRegen0 + parity;
     const int out = kQExtend0 + parity;
     const int count = ctl->count[in];
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
                 g = {st.x, st.y};
             } else {
                 atomicAdd(&ctl->completed, 1ull);
+                atomicAdd(&b.job_done[w.x], 1ull);
                 w.x = -1;
             }
         }
@@ -158,6 +160,7 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
         }
         sl.where[s] = w;
         pushSlot(b.queue[out], &ctl->count[out], s, start);
+        pushSlot(b.queue[kQParked], &ctl->count[kQParked], s, !start);
     }
 }
 
@@ -337,12 +340,15 @@ __global__ void advanceKernel(WfControl* ctl)
     ctl->iterations += 1;
 }
 
-__global__ void resetKernel(WfBuffers b)
+__global__ void resetKernel(WfBuffers b, unsigned long long total_items, int job_count)
 {
     const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     if (i < b.slot_count) {
         b.slots.where[i] = make_int4(-1, 0, 0, 0);
         b.queue[kQRegen0][i] = i;
+    }
+    if (i < job_count) {
+        b.job_done[i] = 0;
     }
     if (i == 0) {
         WfControl* ctl = b.control;
@@ -354,7 +360,42 @@ __global__ void resetKernel(WfBuffers b)
         ctl->next_item = 0;
         ctl->completed = 0;
         ctl->iterations = 0;
+        ctl->total_items = total_items;
+        ctl->job_count = job_count;
     }
+}
+
+// Appending jobs, step 1: parked slots rejoin the current regeneration queue and
+// the new jobs' completion counters start at zero.
+__global__ void appendCopyKernel(WfBuffers b, int first, int count)
+{
+    const WfControl* ctl = b.control;
+    const int parity = ctl->parity;
+    const int parked = ctl->count[kQParked];
+    const int base = ctl->count[kQRegen0 + parity];
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i < parked) {
+        b.queue[kQRegen0 + parity][base + i] = b.queue[kQParked][i];
+    }
+    if (i < count) {
+        b.job_done[first + i] = 0;
+    }
+}
+
+// Appending jobs, step 2 (one thread, after step 1): queue counts and the batch's
+// size. Claims past the old end only happened once every old item was claimed, so
+// handing out resumes at the old end.
+__global__ void appendFinishKernel(WfBuffers b, int first, int count, unsigned long long new_total_items)
+{
+    WfControl* ctl = b.control;
+    const int parity = ctl->parity;
+    ctl->count[kQRegen0 + parity] += ctl->count[kQParked];
+    ctl->count[kQParked] = 0;
+    if (ctl->next_item > ctl->total_items) {
+        ctl->next_item = ctl->total_items;
+    }
+    ctl->total_items = new_total_items;
+    ctl->job_count = first + count;
 }
 
 } // namespace
@@ -368,19 +409,28 @@ cudaError_t wfPrepare(int stack)
     });
 }
 
-cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream)
+cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, int job_count, cudaStream_t stream)
 {
-    (void)total_items;
-    resetKernel<<<(b.slot_count + 255) / 256, 256, 0, stream>>>(b);
+    const int n = b.slot_count > job_count ? b.slot_count : job_count;
+    resetKernel<<<(n + 255) / 256, 256, 0, stream>>>(b, total_items, job_count);
     return cudaGetLastError();
 }
 
-cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long total_items, const WfBuffers& b,
-                        const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream)
+cudaError_t wfAppend(const WfBuffers& b, int first, int count, unsigned long long new_total_items,
+                     cudaStream_t stream)
+{
+    const int n = b.slot_count > count ? b.slot_count : count;
+    appendCopyKernel<<<(n + 255) / 256, 256, 0, stream>>>(b, first, count);
+    appendFinishKernel<<<1, 1, 0, stream>>>(b, first, count, new_total_items);
+    return cudaGetLastError();
+}
+
+cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
+                        cudaStream_t stream)
 {
     const int g = launch.blocks;
     const auto smemFor = [](int entries) { return static_cast<std::size_t>(entries) * 128 * sizeof(uint2); };
-    regenKernel<<<g, 128, 0, stream>>>(jobs, job_count, total_items, b);
+    regenKernel<<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
         extendKernel<S><<<g, 128, smemFor(S), stream>>>(jobs, b, error_flag);

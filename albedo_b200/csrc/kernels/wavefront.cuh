@@ -55,7 +55,8 @@ enum WfQueueId : int {
     kQDielectric = 6,
     kQMix = 7,
     kQShadow = 8,
-    kQueueCount = 9
+    kQParked = 9, // slots that found no pixel; an append puts them back to work
+    kQueueCount = 10
 };
 
 struct WfControl {
@@ -64,12 +65,18 @@ struct WfControl {
     unsigned long long next_item; // next pixel work item to hand out
     unsigned long long completed; // pixels whose last sample has been accumulated
     unsigned long long iterations;
+    // The batch so far: work items (pixels) and jobs in the job table. A server
+    // appends jobs between iterations, growing both.
+    unsigned long long total_items;
+    int job_count;
+    int pad;
 };
 
 struct WfBuffers {
     WfSlots slots;
     int* queue[kQueueCount]; // each `slot_count` entries
     WfControl* control;
+    unsigned long long* job_done; // per job: pixels whose last sample has been accumulated
     int slot_count;
 };
 
@@ -82,14 +89,21 @@ struct WfLaunch {
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call
 // before capturing iterations into a graph.
 cudaError_t wfPrepare(int stack);
-// Puts every slot in the regeneration queue with no job, and clears counters.
-cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, cudaStream_t stream);
+// Puts every slot in the regeneration queue with no job, clears the counters and
+// the first `job_count` per-job counters, and sets the batch's size.
+cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, int job_count, cudaStream_t stream);
 // The allocation-free variant (noalloc.cu): one job, one path slot per pixel, all
 // scratch in a static device array; at most noAllocMaxPixels() pixels.
 int noAllocMaxPixels();
 cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int* error_flag, cudaStream_t stream);
-// Enqueues one iteration (regenerate, extend, shade x 4, shadow, advance).
-cudaError_t wfIteration(const WfJob* jobs, int job_count, unsigned long long total_items, const WfBuffers& b,
-                        const WfLaunch& launch, unsigned int* error_flag, cudaStream_t stream);
+// Enqueues one iteration (regenerate, extend, shade x 4, shadow, advance). The
+// batch's size is read from the control block, so iterations captured in a graph
+// keep serving jobs appended later.
+cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
+                        cudaStream_t stream);
+// Appends jobs [first, first + count) of the (already uploaded) job table to a
+// running batch: zeroes their completion counters and grows the batch's size.
+cudaError_t wfAppend(const WfBuffers& b, int first, int count, unsigned long long new_total_items,
+                     cudaStream_t stream);
 
 } // namespace albedo_b200

@@ -1,13 +1,13 @@
-// Wavefront engine: slot and queue allocation, job upload, graph capture and
-// pipelined completion polling.
+// Wavefront engine: slot, queue and job-table allocation, graph capture, job
+// submission between graph launches, and pipelined completion polling.
 #include "wavefront_engine.hpp"
 
 #include <algorithm>
 #include <cstring>
 #include <format>
-#include <string>
 #include <new>
 #include <stdexcept>
+#include <string>
 
 namespace albedo_b200 {
 
@@ -27,18 +27,21 @@ std::size_t align256(std::size_t n) { return (n + 255) & ~std::size_t{255}; }
 
 } // namespace
 
-WavefrontEngine::WavefrontEngine(int slot_count)
+WavefrontEngine::WavefrontEngine(int slot_count, int job_capacity)
 {
-    if (slot_count <= 0) {
-        throw std::invalid_argument{"the wavefront engine needs at least one slot"};
+    if (slot_count <= 0 || job_capacity <= 0) {
+        throw std::invalid_argument{"the wavefront engine needs at least one slot and one job"};
     }
     const auto n{static_cast<std::size_t>(slot_count)};
     const std::size_t f4{align256(n * sizeof(float4))};
     const std::size_t f2{align256(n * sizeof(float2))};
     const std::size_t u2{align256(n * sizeof(ulonglong2))};
     const std::size_t q{align256(n * sizeof(int))};
-    const std::size_t total{12 * f4 + f2 + u2 + kQueueCount * q + align256(sizeof(WfControl))};
+    const auto jobs{static_cast<std::size_t>(job_capacity)};
+    const std::size_t total{12 * f4 + f2 + u2 + kQueueCount * q + align256(sizeof(WfControl)) +
+                            align256(jobs * sizeof(unsigned long long)) + align256(jobs * sizeof(WfJob))};
     cudaCheck(cudaMalloc(&slab_, total), "wavefront slots");
+    device_bytes_ = total;
     auto* p{static_cast<char*>(slab_)};
     const auto take = [&](std::size_t bytes) {
         void* r{p};
@@ -64,24 +67,36 @@ WavefrontEngine::WavefrontEngine(int slot_count)
         buffers_.queue[i] = static_cast<int*>(take(q));
     }
     buffers_.control = static_cast<WfControl*>(take(align256(sizeof(WfControl))));
+    buffers_.job_done = static_cast<unsigned long long*>(take(align256(jobs * sizeof(unsigned long long))));
+    device_jobs_ = static_cast<WfJob*>(take(align256(jobs * sizeof(WfJob))));
     buffers_.slot_count = slot_count;
+    job_capacity_ = job_capacity;
     cudaCheck(cudaMallocHost(&host_control_, 2 * sizeof(WfControl)), "pinned control");
+    cudaCheck(cudaMallocHost(&host_done_, 2 * jobs * sizeof(unsigned long long)), "pinned counters");
+    cudaCheck(cudaMallocHost(&staging_jobs_, jobs * sizeof(WfJob)), "pinned jobs");
     std::memset(host_control_, 0, 2 * sizeof(WfControl));
     int device{0};
     cudaCheck(cudaGetDevice(&device), "cudaGetDevice");
     cudaCheck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SM count");
     cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "engine stream");
     cudaCheck(cudaEventCreateWithFlags(&ordering_, cudaEventDisableTiming), "engine event");
+    cudaCheck(cudaEventCreateWithFlags(&step_done_[0], cudaEventDisableTiming), "engine event");
+    cudaCheck(cudaEventCreateWithFlags(&step_done_[1], cudaEventDisableTiming), "engine event");
 }
 
 WavefrontEngine::~WavefrontEngine()
 {
     cudaStreamSynchronize(stream_);
+    if (graph_ != nullptr) {
+        cudaGraphExecDestroy(graph_);
+    }
+    cudaEventDestroy(step_done_[0]);
+    cudaEventDestroy(step_done_[1]);
     cudaEventDestroy(ordering_);
     cudaStreamDestroy(stream_);
     cudaFree(slab_);
-    cudaFree(device_jobs_);
     cudaFreeHost(staging_jobs_);
+    cudaFreeHost(host_done_);
     cudaFreeHost(host_control_);
 }
 
@@ -94,114 +109,171 @@ void WavefrontEngine::setLaunch(int blocks_per_sm, int iterations_per_graph)
     iterations_per_graph_ = iterations_per_graph;
 }
 
-void WavefrontEngine::render(const std::vector<WfJob>& input, int stack, unsigned int* error_flag,
-                             cudaStream_t caller)
+void WavefrontEngine::open(int stack, unsigned int* error_flag)
 {
-    if (input.empty()) {
-        return;
+    if (open_) {
+        throw std::logic_error{"the wavefront batch is already open"};
     }
-    // Work runs on the engine's own stream (graphs cannot be captured on the
-    // legacy default stream), ordered after the caller's stream and before
-    // anything the caller enqueues next.
-    cudaCheck(cudaEventRecord(ordering_, caller), "ordering event");
-    cudaCheck(cudaStreamWaitEvent(stream_, ordering_, 0), "ordering wait");
-    renderOnOwnStream(input, stack, error_flag);
-    cudaCheck(cudaEventRecord(ordering_, stream_), "ordering event");
-    cudaCheck(cudaStreamWaitEvent(caller, ordering_, 0), "ordering wait");
-}
-
-void WavefrontEngine::renderOnOwnStream(const std::vector<WfJob>& input, int stack, unsigned int* error_flag)
-{
-    const cudaStream_t stream{stream_};
-    const auto count{static_cast<int>(input.size())};
-    if (count > job_capacity_) {
-        cudaFree(device_jobs_);
-        cudaFreeHost(staging_jobs_);
-        device_jobs_ = nullptr;
-        staging_jobs_ = nullptr;
-        job_capacity_ = 0;
-        cudaCheck(cudaMalloc(&device_jobs_, static_cast<std::size_t>(count) * sizeof(WfJob)), "job table");
-        cudaCheck(cudaMallocHost(&staging_jobs_, static_cast<std::size_t>(count) * sizeof(WfJob)), "job staging");
-        job_capacity_ = count;
-    }
-    // The stream may still read the staging copy of a previous render.
-    cudaCheck(cudaStreamSynchronize(stream), "stream");
-    unsigned long long total{0};
-    for (int j{0}; j < count; ++j) {
-        staging_jobs_[j] = input[static_cast<std::size_t>(j)];
-        staging_jobs_[j].item_begin = static_cast<long long>(total);
-        total += static_cast<unsigned long long>(input[static_cast<std::size_t>(j)].width) *
-                 static_cast<unsigned long long>(input[static_cast<std::size_t>(j)].height);
-        staging_jobs_[j].item_end = static_cast<long long>(total);
-    }
-    cudaCheck(cudaMemcpyAsync(device_jobs_, staging_jobs_, static_cast<std::size_t>(count) * sizeof(WfJob),
-                              cudaMemcpyHostToDevice, stream),
-              "job upload");
-    cudaCheck(wfReset(buffers_, total, stream), "wavefront reset");
-
-    const WfLaunch launch{sm_count_ * blocks_per_sm_, 128, stack};
+    cudaCheck(cudaStreamSynchronize(stream_), "engine stream");
+    job_count_ = 0;
+    total_items_ = 0;
+    job_pixels_.clear();
+    in_flight_.clear();
+    steps_launched_ = 0;
+    steps_polled_ = 0;
+    stall_limit_ = 16;
+    last_completed_ = 0;
+    last_progress_iteration_ = 0;
+    cudaCheck(wfReset(buffers_, 0, 0, stream_), "wavefront reset");
     cudaCheck(wfPrepare(stack), "wavefront kernel attributes");
+    const WfLaunch launch{sm_count_ * blocks_per_sm_, 128, stack};
     cudaGraph_t graph{nullptr};
-    cudaGraphExec_t exec{nullptr};
-    cudaCheck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture begin");
+    cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};
     for (int i{0}; i < iterations_per_graph_ && captured == cudaSuccess; ++i) {
-        captured = wfIteration(device_jobs_, count, total, buffers_, launch, error_flag, stream);
+        captured = wfIteration(device_jobs_, buffers_, launch, error_flag, stream_);
     }
-    const cudaError_t ended{cudaStreamEndCapture(stream, &graph)};
+    const cudaError_t ended{cudaStreamEndCapture(stream_, &graph)};
     cudaCheck(captured, "wavefront iteration");
     cudaCheck(ended, "capture end");
-    cudaCheck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    const cudaError_t instantiated{cudaGraphInstantiate(&graph_, graph, 0)};
     cudaGraphDestroy(graph);
+    cudaCheck(instantiated, "graph instantiate");
+    open_ = true;
+}
 
-    // Poll one graph behind: launch graph k + 1 before looking at graph k's snapshot.
-    cudaEvent_t done[2];
-    cudaCheck(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming), "event");
-    cudaCheck(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming), "event");
-    // A slot finishes its pixel within n^2 (max_depth + 2) iterations, so a batch
-    // that completes no pixel for longer than that is stuck (a defect, reported
-    // instead of looping forever).
-    unsigned long long stall_limit{16};
-    for (const WfJob& j : input) {
-        const auto n2{static_cast<unsigned long long>(j.samples_per_axis) * static_cast<unsigned long long>(j.samples_per_axis)};
-        stall_limit = std::max(stall_limit, n2 * static_cast<unsigned long long>(j.max_depth + 2) + 16);
+int WavefrontEngine::submit(const WfJob& input)
+{
+    if (!open_) {
+        throw std::logic_error{"submit needs an open wavefront batch"};
     }
-    unsigned long long last_completed{0};
-    unsigned long long last_progress_iteration{0};
-    int launched{0};
-    bool finished{false};
-    std::string failure;
-    while (!finished) {
-        const int slot{launched & 1};
-        cudaCheck(cudaGraphLaunch(exec, stream), "graph launch");
-        cudaCheck(cudaMemcpyAsync(&host_control_[slot], buffers_.control, sizeof(WfControl), cudaMemcpyDeviceToHost,
-                                  stream),
-                  "control snapshot");
-        cudaCheck(cudaEventRecord(done[slot], stream), "event record");
-        ++launched;
-        if (launched >= 2) {
-            const int previous{(launched - 2) & 1};
-            cudaCheck(cudaEventSynchronize(done[previous]), "event sync");
-            const WfControl& snapshot{host_control_[previous]};
-            finished = snapshot.completed >= total;
-            if (snapshot.completed != last_completed) {
-                last_completed = snapshot.completed;
-                last_progress_iteration = snapshot.iterations;
-            } else if (snapshot.iterations - last_progress_iteration > stall_limit) {
-                failure = std::format("wavefront batch made no progress for {} iterations ({} of {} pixels done)",
-                                      snapshot.iterations - last_progress_iteration, snapshot.completed, total);
-                finished = true;
-            }
+    if (job_count_ >= job_capacity_) {
+        throw std::length_error{std::format("the job table holds {} jobs", job_capacity_)};
+    }
+    const int index{job_count_};
+    // The staging entry of a job index is written once per batch, so no copy in
+    // flight can still be reading it.
+    WfJob& staged{staging_jobs_[index]};
+    staged = input;
+    const long long pixels{static_cast<long long>(input.width) * input.height};
+    staged.item_begin = static_cast<long long>(total_items_);
+    staged.item_end = staged.item_begin + pixels;
+    cudaCheck(cudaMemcpyAsync(&device_jobs_[index], &staged, sizeof(WfJob), cudaMemcpyHostToDevice, stream_),
+              "job upload");
+    total_items_ += static_cast<unsigned long long>(pixels);
+    cudaCheck(wfAppend(buffers_, index, 1, total_items_, stream_), "job append");
+    ++job_count_;
+    job_pixels_.push_back(pixels);
+    in_flight_.push_back(index);
+    const auto n2{static_cast<unsigned long long>(input.samples_per_axis) * input.samples_per_axis};
+    stall_limit_ = std::max(stall_limit_, n2 * static_cast<unsigned long long>(input.max_depth + 2) + 16);
+    return index;
+}
+
+void WavefrontEngine::step()
+{
+    if (!open_) {
+        throw std::logic_error{"step needs an open wavefront batch"};
+    }
+    const int slot{steps_launched_ & 1};
+    cudaCheck(cudaGraphLaunch(graph_, stream_), "graph launch");
+    cudaCheck(cudaMemcpyAsync(&host_control_[slot], buffers_.control, sizeof(WfControl), cudaMemcpyDeviceToHost,
+                              stream_),
+              "control snapshot");
+    if (job_count_ > 0) {
+        cudaCheck(cudaMemcpyAsync(host_done_ + static_cast<std::size_t>(slot) * job_capacity_, buffers_.job_done,
+                                  static_cast<std::size_t>(job_count_) * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "counter snapshot");
+    }
+    cudaCheck(cudaEventRecord(step_done_[slot], stream_), "event record");
+    ++steps_launched_;
+}
+
+std::vector<int> WavefrontEngine::poll()
+{
+    std::vector<int> finished;
+    // Look at the step before the last, so the device always has a graph queued.
+    const int target{steps_launched_ - (steps_launched_ >= 2 ? 2 : 1)};
+    if (target < steps_polled_ || steps_launched_ == 0) {
+        return finished;
+    }
+    const int slot{target & 1};
+    cudaCheck(cudaEventSynchronize(step_done_[slot]), "event sync");
+    steps_polled_ = target + 1;
+    const WfControl& snapshot{host_control_[slot]};
+    const unsigned long long* done{host_done_ + static_cast<std::size_t>(slot) * job_capacity_};
+    last_iterations_ = snapshot.iterations;
+    std::vector<int> still;
+    for (const int j : in_flight_) {
+        // A job submitted after this snapshot was taken is not in it yet.
+        if (j < snapshot.job_count && static_cast<long long>(done[j]) >= job_pixels_[static_cast<std::size_t>(j)]) {
+            finished.push_back(j);
+        } else {
+            still.push_back(j);
         }
     }
-    cudaCheck(cudaEventSynchronize(done[(launched - 1) & 1]), "event sync");
-    last_iterations_ = host_control_[(launched - 1) & 1].iterations;
-    cudaEventDestroy(done[0]);
-    cudaEventDestroy(done[1]);
-    cudaGraphExecDestroy(exec);
-    if (!failure.empty()) {
-        throw std::runtime_error{failure};
+    in_flight_.swap(still);
+    if (snapshot.completed != last_completed_) {
+        last_completed_ = snapshot.completed;
+        last_progress_iteration_ = snapshot.iterations;
+    } else if (!in_flight_.empty() && snapshot.iterations - last_progress_iteration_ > stall_limit_) {
+        throw std::runtime_error{std::format("wavefront batch made no progress for {} iterations ({} of {} pixels done)",
+                                             snapshot.iterations - last_progress_iteration_, snapshot.completed,
+                                             total_items_)};
     }
+    return finished;
+}
+
+bool WavefrontEngine::saturated() const
+{
+    if (steps_polled_ == 0) {
+        return false;
+    }
+    const WfControl& snapshot{host_control_[(steps_polled_ - 1) & 1]};
+    return snapshot.next_item >= snapshot.total_items;
+}
+
+void WavefrontEngine::close()
+{
+    if (!open_) {
+        return;
+    }
+    cudaStreamSynchronize(stream_);
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    open_ = false;
+}
+
+void WavefrontEngine::render(const std::vector<WfJob>& jobs, int stack, unsigned int* error_flag, cudaStream_t caller)
+{
+    if (jobs.empty()) {
+        return;
+    }
+    if (static_cast<int>(jobs.size()) > job_capacity_) {
+        throw std::invalid_argument{std::format("a batch holds at most {} jobs", job_capacity_)};
+    }
+    cudaCheck(cudaEventRecord(ordering_, caller), "ordering event");
+    cudaCheck(cudaStreamWaitEvent(stream_, ordering_, 0), "ordering wait");
+    open(stack, error_flag);
+    try {
+        for (const WfJob& job : jobs) {
+            submit(job);
+        }
+        while (!in_flight_.empty()) {
+            step();
+            static_cast<void>(poll());
+        }
+    } catch (...) {
+        close();
+        throw;
+    }
+    // Drain the graph still queued after the last poll.
+    cudaCheck(cudaStreamSynchronize(stream_), "engine stream");
+    last_iterations_ = host_control_[(steps_launched_ - 1) & 1].iterations;
+    close();
+    cudaCheck(cudaEventRecord(ordering_, stream_), "ordering event");
+    cudaCheck(cudaStreamWaitEvent(caller, ordering_, 0), "ordering wait");
 }
 
 } // namespace albedo_b200

@@ -60,9 +60,110 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--method", choices=["megakernel", "wavefront"], default="megakernel")
-    p.add_argument("--workload", choices=["trefoil", "batched"], default="trefoil",
-                   help="trefoil: the instanced-mesh frame (default); batched: 64 seeded jobs of uneven size")
+    p.add_argument("--workload", choices=["trefoil", "batched", "served"], default="trefoil",
+                   help="trefoil: the instanced-mesh frame (default); batched: 64 seeded jobs of uneven size; "
+                        "served: Poisson request streams over 16 resident scenes")
+    p.add_argument("--rates", default="10,50,100,200,500", help="served: arrival rates (requests/s) to sweep")
+    p.add_argument("--requests", type=int, default=96, help="served: requests per rate")
     return p.parse_args()
+
+
+def run_served(args) -> None:
+    """Poisson request streams (seeded) drawn from the batched-job distribution
+    over 16 resident scenes, served under a 150 GB device budget: the
+    continuous-batching server against the plain megakernel serving one request
+    at a time in arrival order. Latency is completion minus arrival; throughput
+    is paths over the time from the first arrival to the last completion."""
+    import torch
+
+    import albedo_b200 as ab
+    from albedo_b200 import scenes
+
+    tmp = tempfile.TemporaryDirectory()
+    pool = scenes.batch_jobs(Path(tmp.name), count=16, scenes=16)
+    loaded = [ab.Scene.load(j.scene) for j in pool]
+    # Warm-up: module load, kernel attributes and one graph capture per form.
+    warm = torch.zeros((128 * 72, 4), dtype=torch.float64, device="cuda")
+    for scene in loaded:
+        ab.render_device(scene, ab.RenderJob(128, 72, samples_per_axis=1, max_depth=8), warm.data_ptr())
+    server = ab.Server(memory_budget_bytes=150 << 30, slots=1 << 20)
+    server.submit(loaded[0], ab.RenderJob(128, 72, samples_per_axis=1, max_depth=8, method=ab.WAVEFRONT),
+                  warm.data_ptr())
+    while server.pending() != (0, 0):
+        server.step()
+    server.close()
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(2024)
+    results = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        gaps = rng.exponential(1.0 / rate, size=args.requests)
+        arrivals = np.cumsum(gaps) - gaps[0]
+        reqs = []
+        for k in range(args.requests):
+            w, h = scenes.RESOLUTIONS[int(rng.integers(0, 4))]
+            n = int(np.clip(round(np.sqrt(np.exp(rng.uniform(np.log(4), np.log(64))))), 2, 8))
+            reqs.append((int(rng.integers(0, 16)), w, h, n, k))
+        paths = sum(w * h * n * n for _, w, h, n, _ in reqs)
+        accs = [torch.zeros((w * h, 4), dtype=torch.float64, device="cuda") for _, w, h, _, _ in reqs]
+
+        def job(r, method):
+            _, w, h, n, seed = r
+            return ab.RenderJob(w, h, samples_per_axis=n, seed=seed, max_depth=8, method=method)
+
+        # Continuous batching.
+        server = ab.Server(memory_budget_bytes=150 << 30, slots=1 << 20)
+        done_at = {}
+        ticket_of = {}
+        submitted = 0
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        while len(done_at) < len(reqs):
+            now = time.perf_counter() - start
+            while submitted < len(reqs) and arrivals[submitted] <= now:
+                r = reqs[submitted]
+                ticket_of[server.submit(loaded[r[0]], job(r, ab.WAVEFRONT), accs[submitted].data_ptr())] = submitted
+                submitted += 1
+            finished = server.step()
+            now = time.perf_counter() - start
+            for t in finished:
+                done_at[ticket_of[t]] = now
+            waiting, running = server.pending()
+            if waiting == 0 and running == 0 and submitted < len(reqs):
+                time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - start)))
+        server.close()
+        lat_server = np.array([done_at[k] - arrivals[k] for k in range(len(reqs))])
+        span_server = max(done_at.values()) - arrivals[0]
+
+        # One request at a time, megakernel.
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        finish = []
+        for k, r in enumerate(reqs):
+            now = time.perf_counter() - start
+            if now < arrivals[k]:
+                time.sleep(arrivals[k] - now)
+            ab.render_device(loaded[r[0]], job(r, ab.MEGAKERNEL), accs[k].data_ptr())
+            torch.cuda.synchronize()
+            finish.append(time.perf_counter() - start)
+        lat_mega = np.array(finish) - arrivals
+        span_mega = finish[-1] - arrivals[0]
+        results.append({
+            "rate_per_s": rate, "requests": len(reqs), "paths": paths,
+            "server": {"mpaths_per_s": paths / span_server / 1e6, "p50_ms": float(np.percentile(lat_server, 50) * 1e3),
+                       "p99_ms": float(np.percentile(lat_server, 99) * 1e3)},
+            "megakernel_one_at_a_time": {"mpaths_per_s": paths / span_mega / 1e6,
+                                         "p50_ms": float(np.percentile(lat_mega, 50) * 1e3),
+                                         "p99_ms": float(np.percentile(lat_mega, 99) * 1e3)}})
+    for s in loaded:
+        s.check()
+    best = max(r["server"]["mpaths_per_s"] for r in results)
+    line = {"metric": METRIC, "value": best, "unit": "Mpaths/s", "n_gpus": 1, "steps": len(results), "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files, seeded Poisson arrivals)",
+            "config": {"workload": "served_poisson_16_scenes", "budget_bytes": 150 << 30, "slots": 1 << 20,
+                       "max_depth": 8, "timing": "wall clock from arrival to observed completion"},
+            "sweep": results}
+    print(json.dumps(line), flush=True)
 
 
 def run_batched(args) -> None:
@@ -277,6 +378,10 @@ def main():
     if args.workload == "batched":
         if rank == 0:
             run_batched(args)
+        return
+    if args.workload == "served":
+        if rank == 0:
+            run_served(args)
         return
 
     import torch

@@ -203,6 +203,26 @@ int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* str
  * height entries; the call returns after the render is complete on `stream`. */
 int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
                           void* stream);
+/* A render server: continuous batching of requests on one wavefront engine. A
+ * request is admitted, in arrival order, once the device memory it needs fits
+ * the budget: the engine's path slots and queues, each scene's tables (counted
+ * once; scenes stay resident) and each running request's accumulators. Admitted
+ * requests join the batch already on the device between graph launches, so
+ * their work overlaps the work of requests admitted before them; each result
+ * is the image the same request would get alone. No counterpart in the
+ * reference, which renders one image per process. */
+typedef struct albedo_server albedo_server;
+int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo_server** out);
+/* Queues a request (committed scene, job, device accumulators) and admits what
+ * fits. The ticket identifies it in albedo_server_step's results. */
+int albedo_server_submit(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
+                         albedo_accumulator* accumulators, int64_t* out_ticket);
+/* Advances the device by one graph of iterations and reports (up to `capacity`)
+ * tickets whose accumulators are now complete; tickets beyond `capacity` are
+ * reported by later calls. */
+int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacity, int32_t* out_finished);
+int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int32_t* out_running);
+void albedo_server_destroy(albedo_server* server);
 /* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
  * iterations per captured CUDA graph (the autotuner's knobs). */
 int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph);

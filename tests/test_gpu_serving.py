@@ -1,0 +1,108 @@
+"""The render server: continuous batching gives each request the image it gets
+alone (GPU).
+
+Requests are submitted while others are already running on the device; each
+finished result is compared with the same job rendered alone, with the wavefront
+tests' tolerance (identical sample counts, image sums within 1e-4 relative, at
+most 0.5% of pixels differing by more than 1e-3 relative). A second run uses a
+memory budget that admits one request at a time, so later requests wait.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import albedo_b200 as ab
+
+pytestmark = pytest.mark.gpu
+
+
+def counts(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a[:, 3]).view(np.int64)
+
+
+def assert_same_image(a: np.ndarray, b: np.ndarray):
+    np.testing.assert_array_equal(counts(a), counts(b))
+    ca, cb = a[:, :3], b[:, :3]
+    assert np.abs(ca.sum() - cb.sum()) / cb.sum() < 1e-4
+    rel = np.abs(ca - cb) / np.maximum(np.abs(cb), 1e-3)
+    assert np.mean(rel.max(axis=1) > 1e-3) < 0.005
+
+
+def alone(scene, job) -> np.ndarray:
+    acc = torch.zeros((job.width * job.height, 4), dtype=torch.float64, device="cuda")
+    ab.render_device(scene, job, acc.data_ptr())
+    torch.cuda.synchronize()
+    return acc.cpu().numpy()
+
+
+def requests(room, trefoil):
+    return [(room, ab.RenderJob(160, 90, samples_per_axis=4, seed=11, max_depth=8, method=ab.WAVEFRONT)),
+            (trefoil, ab.RenderJob(96, 54, samples_per_axis=2, seed=12, max_depth=10, method=ab.WAVEFRONT)),
+            (room, ab.RenderJob(64, 36, samples_per_axis=3, seed=13, max_depth=64, method=ab.WAVEFRONT)),
+            (trefoil, ab.RenderJob(128, 72, samples_per_axis=3, seed=14, max_depth=6, method=ab.WAVEFRONT))]
+
+
+def serve(server, items, stagger=True):
+    accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in items]
+    tickets = {}
+    done = set()
+    # The first request starts alone; the others arrive while it runs.
+    tickets[server.submit(items[0][0], items[0][1], accs[0].data_ptr())] = 0
+    steps = 0
+    for k, (scene, job) in enumerate(items[1:], start=1):
+        if stagger:
+            done.update(server.step())
+            steps += 1
+        tickets[server.submit(scene, job, accs[k].data_ptr())] = k
+    while len(done) < len(items):
+        done.update(server.step())
+        steps += 1
+        assert steps < 100000
+    torch.cuda.synchronize()
+    assert set(tickets) == done
+    return [a.cpu().numpy() for a in accs]
+
+
+def test_each_request_is_the_same_alone_and_in_the_mix(room_path, trefoil_path):
+    room, trefoil = ab.Scene.load(room_path), ab.Scene.load(trefoil_path)
+    items = requests(room, trefoil)
+    server = ab.Server(memory_budget_bytes=8 << 30, slots=1 << 16)
+    results = serve(server, items)
+    assert server.pending() == (0, 0)
+    for (scene, job), result in zip(items, results):
+        assert_same_image(result, alone(scene, job))
+    server.close()
+
+
+def test_requests_wait_for_memory_and_still_match(room_path, trefoil_path):
+    room, trefoil = ab.Scene.load(room_path), ab.Scene.load(trefoil_path)
+    items = requests(room, trefoil)
+    slots = 1 << 14
+    # Budget: the slot pool, both scenes and the largest request's accumulators,
+    # so at most one or two requests fit at once and the rest wait.
+    slot_bytes = slots * 232 + (1 << 20)
+    scene_bytes = room.info()["device_bytes"] + trefoil.info()["device_bytes"]
+    budget = slot_bytes + scene_bytes + 160 * 90 * 32 + 64 * 36 * 32 + (4 << 20)
+    server = ab.Server(memory_budget_bytes=budget, slots=slots)
+    accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in items]
+    for (scene, job), acc in zip(items, accs):
+        server.submit(scene, job, acc.data_ptr())
+    waiting, running = server.pending()
+    assert waiting >= 1 and running >= 1
+    finished = []
+    while len(finished) < len(items):
+        finished += server.step()
+    torch.cuda.synchronize()
+    for (scene, job), acc in zip(items, accs):
+        assert_same_image(acc.cpu().numpy(), alone(scene, job))
+    server.close()
+
+
+def test_a_request_larger_than_the_budget_is_refused(room_path):
+    room = ab.Scene.load(room_path)
+    server = ab.Server(memory_budget_bytes=(1 << 14) * 232 + (8 << 20), slots=1 << 14)
+    acc = torch.zeros((1024 * 576, 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError, match="exceeds the server's memory budget"):
+        server.submit(room, ab.RenderJob(1024, 576, method=ab.WAVEFRONT), acc.data_ptr())
+    server.close()
