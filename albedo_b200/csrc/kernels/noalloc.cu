@@ -134,7 +134,14 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
     if ((e = wfReset(buffers, total, 1, stream)) != cudaSuccess) {
         return e;
     }
-    const WfLaunch launch{blocks, 128, stack};
+    int per_sm = 1;
+    int device = 0;
+    int sms = 1;
+    if ((e = wfTraceBlocksPerSm(stack, &per_sm)) != cudaSuccess || (e = cudaGetDevice(&device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+        return e;
+    }
+    const WfLaunch launch{blocks, 128, stack, per_sm * sms};
     // A slot finishes its pixel within n^2 (max_depth + 2) iterations.
     const unsigned long long bound = static_cast<unsigned long long>(job.samples_per_axis) * job.samples_per_axis *
                                          static_cast<unsigned long long>(job.max_depth + 2) +

@@ -265,17 +265,284 @@ ALB_DEV std::uint32_t leafRef(std::uint32_t first, std::uint32_t count)
     return kLeafBit | ((count - 1u) << 28) | first;
 }
 
+// One ray query in flight: the ray in the space being traversed (world or the
+// current instance's object space), the world ray it came from, the live range,
+// the node reference to visit next, the stack depth and the hit so far.
+struct TraceState {
+    TravRay r;
+    float3 origin;
+    float3 dir;
+    float tmin;
+    float tmax;
+    std::uint32_t ref;
+    std::uint32_t inst_pos; // TLAS leaf position of the instance being traversed, or kNoPrim
+    int sp;
+    bool found;
+    TraceHit hit;
+};
+
+// What a traversal step leaves to do next.
+enum TraceStep : int {
+    kStepDescend = 0, // `ref` holds the next node or leaf to visit
+    kStepPop = 1,     // continue with the next stack entry
+    kStepFinished = 2 // any-hit found, or the stack would overflow (error flag set)
+};
+
+// Starts a query over (tmin, tmax); false when the scene has no objects.
+ALB_DEV bool traceBegin(const DevScene& s, TraceState& q, float3 origin, float3 dir, float tmin, float tmax)
+{
+    q.origin = origin;
+    q.dir = dir;
+    q.tmin = tmin;
+    q.tmax = tmax;
+    q.found = false;
+    q.sp = 0;
+    q.inst_pos = kNoPrim;
+    q.ref = s.tlas_root;
+    if (s.tlas_root == kEmptyChild) {
+        return false;
+    }
+    q.r.setup(origin, dir);
+    return true;
+}
+
+// A 4-wide node: tests every child box, continues with the hit child the
+// reference reaches first and pushes the other hit children, last first, so
+// leaves are reached in the reference's depth-first near-first order.
+__device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, uint2* stack, int stride, int stack_size,
+                                        unsigned int* error_flag, TraversalCounts* counts)
+{
+    const float4* np = reinterpret_cast<const float4*>(s.nodes + q.ref);
+    const float4 lx = __ldg(np);
+    const float4 hx = __ldg(np + 1);
+    const float4 ly = __ldg(np + 2);
+    const float4 hy = __ldg(np + 3);
+    const float4 lz = __ldg(np + 4);
+    const float4 hz = __ldg(np + 5);
+    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
+    const int present = static_cast<int>(meta.z);
+    if (counts != nullptr) {
+        counts->boxes += static_cast<unsigned>(present);
+    }
+    const TravRay& r = q.r;
+    float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
+    unsigned mask = slabTest(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, q.tmin, q.tmax, e0) ? 1u : 0u;
+    if (present > 1 && slabTest(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, q.tmin, q.tmax, e1)) {
+        mask |= 2u;
+    }
+    if (present > 2 && slabTest(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, q.tmin, q.tmax, e2)) {
+        mask |= 4u;
+    }
+    if (present > 3 && slabTest(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, q.tmin, q.tmax, e3)) {
+        mask |= 8u;
+    }
+    if (mask == 0u) {
+        return kStepPop;
+    }
+    int remaining = __popc(mask);
+    if (q.sp + remaining - 1 > stack_size) {
+        atomicOr(error_flag, 1u);
+        return kStepFinished;
+    }
+    const unsigned packed = (r.neg < 4u ? (meta.x >> (8u * r.neg)) : (meta.y >> (8u * (r.neg - 4u)))) & 0xFFu;
+#pragma unroll
+    for (int position = 3; position >= 0; --position) {
+        if (position >= present) {
+            continue;
+        }
+        const unsigned c = (packed >> (2 * position)) & 3u;
+        if (((mask >> c) & 1u) == 0u) {
+            continue;
+        }
+        const std::uint32_t child = c == 0u ? ch.x : (c == 1u ? ch.y : (c == 2u ? ch.z : ch.w));
+        if (--remaining == 0) {
+            q.ref = child;
+        } else {
+            const float entry = c == 0u ? e0 : (c == 1u ? e1 : (c == 2u ? e2 : e3));
+            stack[q.sp * stride] = make_uint2(child, __float_as_uint(entry));
+            ++q.sp;
+        }
+    }
+    return kStepDescend;
+}
+
+// A leaf. In the TLAS: spheres, scene triangles and instances in leaf order; an
+// instance is entered at once (the rest of the leaf and an exit marker are
+// pushed). In a BLAS: the current instance's triangles.
+__device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const SkipRule& skip, uint2* stack,
+                                        int stride, int stack_size, unsigned int* error_flag,
+                                        TraversalCounts* counts, bool any)
+{
+    const std::uint32_t first = q.ref & kLeafFirstMask;
+    const std::uint32_t count = ((q.ref >> 28) & 7u) + 1u;
+    if (q.inst_pos == kNoPrim) {
+        for (std::uint32_t k = 0; k < count; ++k) {
+            const std::uint32_t pos = first + k;
+            const DevObject obj = s.objects[pos];
+            if (pos == skip.light_object_pos) {
+                continue;
+            }
+            if (obj.kind == kObjInstance) {
+                if (q.sp + 2 > stack_size) {
+                    atomicOr(error_flag, 1u);
+                    return kStepFinished;
+                }
+                if (k + 1 < count) {
+                    stack[q.sp * stride] = make_uint2(leafRef(pos + 1, count - k - 1), __float_as_uint(-INFINITY));
+                    ++q.sp;
+                }
+                stack[q.sp * stride] = make_uint2(kExitMarker, 0u);
+                ++q.sp;
+                const DevInstance& inst = s.instances[obj.index];
+                if (counts != nullptr) {
+                    counts->instances += 1;
+                }
+                q.r.setup(affinePoint(inst.to_object, q.origin), affineVector(inst.to_object, q.dir));
+                q.inst_pos = pos;
+                q.ref = inst.root;
+                return kStepDescend;
+            }
+            float t;
+            float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
+            bool h;
+            if (obj.kind == kObjTriangle) {
+                if (pos == skip.object_pos) {
+                    continue;
+                }
+                const float4* tp = reinterpret_cast<const float4*>(s.triangles + obj.index);
+                if (counts != nullptr) {
+                    counts->triangles += 1;
+                }
+                h = q.r.usable &&
+                    intersectTriangle(q.r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q.tmin, q.tmax, t, b0, b1, b2);
+            } else {
+                int mode = kSphereTestBoth;
+                if (pos == skip.object_pos) {
+                    if (skip.sphere_mode == kSphereSkipAll) {
+                        continue;
+                    }
+                    mode = skip.sphere_mode;
+                }
+                if (counts != nullptr) {
+                    counts->spheres += 1;
+                }
+                h = intersectSphere(q.r, s.spheres[obj.index], obj.kind == kObjSphereWide, q.tmin, q.tmax, mode, t);
+            }
+            if (h) {
+                q.found = true;
+                q.tmax = t;
+                q.hit = {t, pos, obj.kind == kObjTriangle ? obj.index : kNoPrim, b0, b1, b2};
+                if (any) {
+                    return kStepFinished;
+                }
+            }
+        }
+        return kStepPop;
+    }
+    if (q.r.usable) {
+        for (std::uint32_t k = 0; k < count; ++k) {
+            const std::uint32_t pos = first + k;
+            if (pos == skip.tri_pos && q.inst_pos == skip.object_pos) {
+                continue;
+            }
+            const float4* tp = reinterpret_cast<const float4*>(s.triangles + pos);
+            float t, b0, b1, b2;
+            if (counts != nullptr) {
+                counts->triangles += 1;
+            }
+            if (intersectTriangle(q.r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q.tmin, q.tmax, t, b0, b1, b2)) {
+                q.found = true;
+                q.tmax = t;
+                q.hit = {t, q.inst_pos, pos, b0, b1, b2};
+                if (any) {
+                    return kStepFinished;
+                }
+            }
+        }
+    }
+    return kStepPop;
+}
+
+// Pops the next entry still worth visiting into `ref`; false when none is left.
+// An exit marker returns the ray to world space; an entry whose box is entered
+// beyond the current hit is dropped (accel/bvh.hpp:240-247).
+__device__ __forceinline__ bool popNext(TraceState& q, const uint2* stack, int stride)
+{
+    for (;;) {
+        if (q.sp == 0) {
+            return false;
+        }
+        --q.sp;
+        const uint2 e = stack[q.sp * stride];
+        if (e.x == kExitMarker) {
+            q.r.setup(q.origin, q.dir);
+            q.inst_pos = kNoPrim;
+            continue;
+        }
+        if (__uint_as_float(e.y) > q.tmax) {
+            continue;
+        }
+        q.ref = e.x;
+        return true;
+    }
+}
+
+// Runs one query to its end: descends through interior nodes, then handles the
+// leaf reached, so that the lanes of a warp move through each phase together.
+// Returns whether the query has more work (false: finished).
+__device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, uint2* stack,
+                                             int stride, int stack_size, unsigned int* error_flag,
+                                             TraversalCounts* counts, bool any)
+{
+    int step = kStepDescend;
+    while (step == kStepDescend && (q.ref & kLeafBit) == 0u) {
+        step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
+    }
+    if (step == kStepDescend) {
+        step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+    }
+    if (step == kStepFinished) {
+        return false;
+    }
+    return step == kStepDescend || popNext(q, stack, stride);
+}
+
 // Traverses the scene for the nearest hit in (tmin, tmax) (ANY = false), or for
 // any hit (ANY = true). On return `tmax` is the nearest hit distance. The stack
 // overflow bound (TLAS depth + BLAS depth + 2) is checked on the host before
 // launch, so pushes never exceed `stack_size`.
 // One out-of-line copy serves closest-hit and any-hit queries alike (`any`
 // stops at the first hit), which keeps the kernels that call it small enough
-// for the instruction cache.
-static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
-                                            const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
-                                            int stack_size, unsigned int* error_flag, TraversalCounts* counts,
-                                            bool any);
+// for the instruction cache. It takes one step (a node or a leaf) per loop
+// turn: inside the megakernel, the nested node/leaf loops of traceAdvance
+// measured 3.4x slower.
+static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin,
+                                                   float& tmax, const SkipRule& skip, TraceHit& hit, uint2* stack,
+                                                   int stride, int stack_size, unsigned int* error_flag,
+                                                   TraversalCounts* counts, bool any)
+{
+    if (counts != nullptr) {
+        counts->rays += 1;
+    }
+    TraceState q;
+    if (!traceBegin(s, q, origin, dir, tmin, tmax)) {
+        return false;
+    }
+    for (;;) {
+        const int step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
+                                                  : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts,
+                                                             any);
+        if (step == kStepFinished || (step == kStepPop && !popNext(q, stack, stride))) {
+            break;
+        }
+    }
+    if (q.found) {
+        tmax = q.tmax;
+        hit = q.hit;
+    }
+    return q.found;
+}
 
 template <bool ANY>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
@@ -283,195 +550,6 @@ ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin
                         TraversalCounts* counts = nullptr)
 {
     return traceSceneImpl(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts, ANY);
-}
-
-static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
-                                            const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
-                                            int stack_size, unsigned int* error_flag, TraversalCounts* counts,
-                                            bool any)
-{
-    const bool ANY = any;
-    if (counts != nullptr) {
-        counts->rays += 1;
-    }
-    if (s.tlas_root == kEmptyChild) {
-        return false;
-    }
-    TravRay r;
-    r.setup(origin, dir);
-    bool found = false;
-    int sp = 0;
-    std::uint32_t inst_pos = kNoPrim; // TLAS leaf position of the instance being traversed
-    std::uint32_t ref = s.tlas_root;
-    for (;;) {
-        if ((ref & kLeafBit) == 0u) {
-            // A 4-wide node: test every child box, then continue with the hit child
-            // the reference reaches first and push the others, last first.
-            const float4* np = reinterpret_cast<const float4*>(s.nodes + ref);
-            const float4 lx = __ldg(np);
-            const float4 hx = __ldg(np + 1);
-            const float4 ly = __ldg(np + 2);
-            const float4 hy = __ldg(np + 3);
-            const float4 lz = __ldg(np + 4);
-            const float4 hz = __ldg(np + 5);
-            const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
-            const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
-            const int present = static_cast<int>(meta.z);
-            if (counts != nullptr) {
-                counts->boxes += static_cast<unsigned>(present);
-            }
-            float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
-            unsigned mask = slabTest(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, tmin, tmax, e0) ? 1u : 0u;
-            if (present > 1 && slabTest(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, tmin, tmax, e1)) {
-                mask |= 2u;
-            }
-            if (present > 2 && slabTest(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, tmin, tmax, e2)) {
-                mask |= 4u;
-            }
-            if (present > 3 && slabTest(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, tmin, tmax, e3)) {
-                mask |= 8u;
-            }
-            if (mask != 0u) {
-                int remaining = __popc(mask);
-                if (sp + remaining - 1 > stack_size) {
-                    atomicOr(error_flag, 1u);
-                    return found;
-                }
-                const unsigned packed = (r.neg < 4u ? (meta.x >> (8u * r.neg)) : (meta.y >> (8u * (r.neg - 4u)))) & 0xFFu;
-#pragma unroll
-                for (int position = 3; position >= 0; --position) {
-                    if (position >= present) {
-                        continue;
-                    }
-                    const unsigned c = (packed >> (2 * position)) & 3u;
-                    if (((mask >> c) & 1u) == 0u) {
-                        continue;
-                    }
-                    const std::uint32_t child = c == 0u ? ch.x : (c == 1u ? ch.y : (c == 2u ? ch.z : ch.w));
-                    if (--remaining == 0) {
-                        ref = child;
-                    } else {
-                        const float entry = c == 0u ? e0 : (c == 1u ? e1 : (c == 2u ? e2 : e3));
-                        stack[sp * stride] = make_uint2(child, __float_as_uint(entry));
-                        ++sp;
-                    }
-                }
-                continue;
-            }
-        } else {
-            const std::uint32_t first = ref & kLeafFirstMask;
-            const std::uint32_t count = ((ref >> 28) & 7u) + 1u;
-            if (inst_pos == kNoPrim) {
-                // TLAS leaf: spheres, scene triangles and instances, in leaf order.
-                bool entered = false;
-                for (std::uint32_t k = 0; k < count; ++k) {
-                    const std::uint32_t pos = first + k;
-                    const DevObject obj = s.objects[pos];
-                    if (pos == skip.light_object_pos) {
-                        continue;
-                    }
-                    if (obj.kind == kObjInstance) {
-                        if (sp + 2 > stack_size) {
-                            atomicOr(error_flag, 1u);
-                            return found;
-                        }
-                        if (k + 1 < count) {
-                            stack[sp * stride] = make_uint2(leafRef(pos + 1, count - k - 1), __float_as_uint(-INFINITY));
-                            ++sp;
-                        }
-                        stack[sp * stride] = make_uint2(kExitMarker, 0u);
-                        ++sp;
-                        const DevInstance& inst = s.instances[obj.index];
-                        if (counts != nullptr) {
-                            counts->instances += 1;
-                        }
-                        r.setup(affinePoint(inst.to_object, origin), affineVector(inst.to_object, dir));
-                        inst_pos = pos;
-                        ref = inst.root;
-                        entered = true;
-                        break;
-                    }
-                    float t;
-                    float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
-                    bool h;
-                    if (obj.kind == kObjTriangle) {
-                        if (pos == skip.object_pos) {
-                            continue;
-                        }
-                        const float4* tp = reinterpret_cast<const float4*>(s.triangles + obj.index);
-                        if (counts != nullptr) {
-                            counts->triangles += 1;
-                        }
-                        h = r.usable && intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2);
-                    } else {
-                        int mode = kSphereTestBoth;
-                        if (pos == skip.object_pos) {
-                            if (skip.sphere_mode == kSphereSkipAll) {
-                                continue;
-                            }
-                            mode = skip.sphere_mode;
-                        }
-                        if (counts != nullptr) {
-                            counts->spheres += 1;
-                        }
-                        h = intersectSphere(r, s.spheres[obj.index], obj.kind == kObjSphereWide, tmin, tmax, mode, t);
-                    }
-                    if (h) {
-                        found = true;
-                        tmax = t;
-                        hit = {t, pos, obj.kind == kObjTriangle ? obj.index : kNoPrim, b0, b1, b2};
-                        if (ANY) {
-                            return true;
-                        }
-                    }
-                }
-                if (entered) {
-                    continue;
-                }
-            } else {
-                // BLAS leaf: triangles of the current instance's mesh.
-                if (r.usable) {
-                    for (std::uint32_t k = 0; k < count; ++k) {
-                        const std::uint32_t pos = first + k;
-                        if (pos == skip.tri_pos && inst_pos == skip.object_pos) {
-                            continue;
-                        }
-                        const float4* tp = reinterpret_cast<const float4*>(s.triangles + pos);
-                        float t, b0, b1, b2;
-                        if (counts != nullptr) {
-                            counts->triangles += 1;
-                        }
-                        if (intersectTriangle(r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tmin, tmax, t, b0, b1, b2)) {
-                            found = true;
-                            tmax = t;
-                            hit = {t, inst_pos, pos, b0, b1, b2};
-                            if (ANY) {
-                                return true;
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        // Pop the next entry still worth visiting.
-        for (;;) {
-            if (sp == 0) {
-                return found;
-            }
-            --sp;
-            const uint2 e = stack[sp * stride];
-            if (e.x == kExitMarker) {
-                r.setup(origin, dir);
-                inst_pos = kNoPrim;
-                continue;
-            }
-            if (__uint_as_float(e.y) > tmax) {
-                continue;
-            }
-            ref = e.x;
-            break;
-        }
-    }
 }
 
 } // namespace albedo_b200

@@ -59,6 +59,55 @@ ALB_DEV unsigned long long claimItem(unsigned long long* next, bool want)
     return want ? base + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u))) : ~0ull;
 }
 
+// Deals queue entries [0, count) to the lanes of a warp that need a ray, in
+// lane order; the warp claims kFetchBatch entries at a time with one atomicAdd.
+// All 32 lanes call take() together.
+constexpr int kFetchBatch = 32;
+
+// Resident blocks per SM the traversal kernels' register budget is sized for.
+#ifndef ALBEDO_TRACE_BLOCKS_PER_SM
+#define ALBEDO_TRACE_BLOCKS_PER_SM 4
+#endif
+constexpr int kTraceBlocksPerSm = ALBEDO_TRACE_BLOCKS_PER_SM;
+
+struct WarpFetch {
+    int next;
+    int end;
+    bool drained;
+
+    ALB_DEV int take(int* counter, int count, bool want)
+    {
+        const int lane = static_cast<int>(threadIdx.x & 31u);
+        const unsigned below = (1u << lane) - 1u;
+        unsigned need = __ballot_sync(0xFFFFFFFFu, want);
+        int got = -1;
+        while (need != 0u && !drained) {
+            if (next >= end) {
+                int base = 0;
+                if (lane == 0) {
+                    base = atomicAdd(counter, kFetchBatch);
+                }
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= count) {
+                    drained = true;
+                    break;
+                }
+                next = base;
+                end = base + kFetchBatch < count ? base + kFetchBatch : count;
+            }
+            const int avail = end - next;
+            const int rank = __popc(need & below);
+            if (((need >> lane) & 1u) != 0u && rank < avail) {
+                got = next + rank;
+            }
+            const int wanted = __popc(need);
+            next += wanted < avail ? wanted : avail;
+            need = __ballot_sync(0xFFFFFFFFu, want && got < 0);
+        }
+        return got;
+    }
+};
+
 ALB_DEV int findJob(const WfJob* jobs, int job_count, long long item)
 {
     int lo = 0;
@@ -164,8 +213,12 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
     }
 }
 
+// Closest hit of every ray in the extend queue. The kernel is persistent: a lane
+// whose query ends files the result and takes the next queued ray, so a warp is
+// not held by its slowest ray. Each query runs the same traversal steps, in the
+// same order, as a query traced alone.
 template <int STACK>
-__global__ void __launch_bounds__(128) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
+__global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
                                                     unsigned int* error_flag)
 {
     extern __shared__ uint2 stack[];
@@ -175,42 +228,62 @@ __global__ void __launch_bounds__(128) extendKernel(const WfJob* __restrict__ jo
     const int ended = kQRegen0 + (parity ^ 1);
     const int count = ctl->count[in];
     const WfSlots& sl = b.slots;
-    const int stride = static_cast<int>(gridDim.x * blockDim.x);
-    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
-        const int s = b.queue[in][i];
-        const int job_index = sl.where[s].x;
-        const DevScene& scene = jobs[job_index].scene;
-        const float4 o = sl.ray_o[s];
-        const float4 d = sl.ray_d[s];
-        const uint4 k = sl.skip[s];
-        const SkipRule skip{k.x, k.y, static_cast<int>(k.z), kNoPrim};
-        TraceHit hit;
-        float tmax = INFINITY;
-        const bool found = traceScene<false>(scene, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, tmax, skip, hit,
-                                             stack + threadIdx.x, static_cast<int>(blockDim.x), STACK, error_flag);
-        int cls = -1;
-        if (found) {
-            sl.hit[s] = make_float4(hit.t, __uint_as_float(hit.obj_pos), __uint_as_float(hit.tri_pos), hit.b0);
-            sl.hit_b[s] = make_float2(hit.b1, hit.b2);
-            cls = materialClass(scene, hit.obj_pos);
-        } else {
-            PathState p;
-            p.d = mk(d.x, d.y, d.z);
-            p.arrival_pdf = o.w;
-            p.arrival_specular = d.w != 0.0f;
-            const float4 t = sl.throughput[s];
-            const float3 e = weightedSky(scene, p);
-            float4 r = sl.result[s];
-            r.x += t.x * e.x;
-            r.y += t.y * e.y;
-            r.z += t.z * e.z;
-            sl.result[s] = r;
+    uint2* const lane_stack = stack + threadIdx.x;
+    const int stride = static_cast<int>(blockDim.x);
+    WarpFetch fetch{0, 0, false};
+    TraceState q;
+    SkipRule skip = SkipRule::none();
+    const DevScene* scene = nullptr;
+    int s = -1;
+    bool active = false;
+    for (;;) {
+        const int i = fetch.take(&ctl->fetch_extend, count, !active);
+        bool finished = false;
+        if (i >= 0) {
+            s = b.queue[in][i];
+            scene = &jobs[sl.where[s].x].scene;
+            const float4 o = sl.ray_o[s];
+            const float4 d = sl.ray_d[s];
+            const uint4 k = sl.skip[s];
+            skip = {k.x, k.y, static_cast<int>(k.z), kNoPrim};
+            active = traceBegin(*scene, q, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, INFINITY);
+            finished = !active;
         }
-        pushSlot(b.queue[ended], &ctl->count[ended], s, !found);
-        pushSlot(b.queue[kQDiffuse], &ctl->count[kQDiffuse], s, cls == kClassDiffuse);
-        pushSlot(b.queue[kQConductor], &ctl->count[kQConductor], s, cls == kClassConductor);
-        pushSlot(b.queue[kQDielectric], &ctl->count[kQDielectric], s, cls == kClassDielectric);
-        pushSlot(b.queue[kQMix], &ctl->count[kQMix], s, cls == kClassMix);
+        if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
+            break;
+        }
+        if (active && !traceAdvance(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, false)) {
+            active = false;
+            finished = true;
+        }
+        if (finished) {
+            int cls = -1;
+            if (q.found) {
+                sl.hit[s] = make_float4(q.hit.t, __uint_as_float(q.hit.obj_pos), __uint_as_float(q.hit.tri_pos),
+                                        q.hit.b0);
+                sl.hit_b[s] = make_float2(q.hit.b1, q.hit.b2);
+                cls = materialClass(*scene, q.hit.obj_pos);
+            } else {
+                const float4 o = sl.ray_o[s];
+                const float4 d = sl.ray_d[s];
+                PathState p;
+                p.d = mk(d.x, d.y, d.z);
+                p.arrival_pdf = o.w;
+                p.arrival_specular = d.w != 0.0f;
+                const float4 t = sl.throughput[s];
+                const float3 e = weightedSky(*scene, p);
+                float4 r = sl.result[s];
+                r.x += t.x * e.x;
+                r.y += t.y * e.y;
+                r.z += t.z * e.z;
+                sl.result[s] = r;
+            }
+            pushSlot(b.queue[ended], &ctl->count[ended], s, !q.found);
+            pushSlot(b.queue[kQDiffuse], &ctl->count[kQDiffuse], s, cls == kClassDiffuse);
+            pushSlot(b.queue[kQConductor], &ctl->count[kQConductor], s, cls == kClassConductor);
+            pushSlot(b.queue[kQDielectric], &ctl->count[kQDielectric], s, cls == kClassDielectric);
+            pushSlot(b.queue[kQMix], &ctl->count[kQMix], s, cls == kClassMix);
+        }
     }
 }
 
@@ -296,26 +369,45 @@ __global__ void __launch_bounds__(128) shadeKernel(const WfJob* __restrict__ job
     }
 }
 
+// Any-hit test of every shadow candidate; unoccluded candidates are added to
+// their path. Persistent, like extendKernel.
 template <int STACK>
-__global__ void __launch_bounds__(128) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
+__global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
                                                     unsigned int* error_flag)
 {
     extern __shared__ uint2 stack[];
     WfControl* ctl = b.control;
     const int count = ctl->count[kQShadow];
     const WfSlots& sl = b.slots;
-    const int stride = static_cast<int>(gridDim.x * blockDim.x);
-    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
-        const int s = b.queue[kQShadow][i];
-        const DevScene& scene = jobs[sl.where[s].x].scene;
-        const float4 o = sl.shadow_o[s];
-        const float4 d = sl.shadow_d[s];
-        const uint4 k = sl.shadow_skip[s];
-        const SkipRule skip{k.x, k.y, static_cast<int>(k.z), __float_as_uint(d.w)};
-        TraceHit hit;
-        float tmax = o.w;
-        if (!traceScene<true>(scene, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, tmax, skip, hit,
-                              stack + threadIdx.x, static_cast<int>(blockDim.x), STACK, error_flag)) {
+    uint2* const lane_stack = stack + threadIdx.x;
+    const int stride = static_cast<int>(blockDim.x);
+    WarpFetch fetch{0, 0, false};
+    TraceState q;
+    SkipRule skip = SkipRule::none();
+    const DevScene* scene = nullptr;
+    int s = -1;
+    bool active = false;
+    for (;;) {
+        const int i = fetch.take(&ctl->fetch_shadow, count, !active);
+        bool finished = false;
+        if (i >= 0) {
+            s = b.queue[kQShadow][i];
+            scene = &jobs[sl.where[s].x].scene;
+            const float4 o = sl.shadow_o[s];
+            const float4 d = sl.shadow_d[s];
+            const uint4 k = sl.shadow_skip[s];
+            skip = {k.x, k.y, static_cast<int>(k.z), __float_as_uint(d.w)};
+            active = traceBegin(*scene, q, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), 0.0f, o.w);
+            finished = !active;
+        }
+        if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
+            break;
+        }
+        if (active && !traceAdvance(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, true)) {
+            active = false;
+            finished = true;
+        }
+        if (finished && !q.found) {
             const float4 c = sl.shadow_c[s];
             float4 r = sl.result[s];
             r.x += c.x;
@@ -336,6 +428,8 @@ __global__ void advanceKernel(WfControl* ctl)
     ctl->count[kQDielectric] = 0;
     ctl->count[kQMix] = 0;
     ctl->count[kQShadow] = 0;
+    ctl->fetch_extend = 0;
+    ctl->fetch_shadow = 0;
     ctl->parity = parity ^ 1;
     ctl->iterations += 1;
 }
@@ -362,6 +456,8 @@ __global__ void resetKernel(WfBuffers b, unsigned long long total_items, int job
         ctl->iterations = 0;
         ctl->total_items = total_items;
         ctl->job_count = job_count;
+        ctl->fetch_extend = 0;
+        ctl->fetch_shadow = 0;
     }
 }
 
@@ -409,6 +505,24 @@ cudaError_t wfPrepare(int stack)
     });
 }
 
+cudaError_t wfTraceBlocksPerSm(int stack, int* out)
+{
+    *out = 1;
+    return withStack(stack, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        const std::size_t smem = static_cast<std::size_t>(S) * 128 * sizeof(uint2);
+        int extend = 0;
+        int shadow = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend, extendKernel<S>, 128, smem);
+        if (e == cudaSuccess) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow, shadowKernel<S>, 128, smem);
+        }
+        const int blocks = extend < shadow ? extend : shadow;
+        *out = blocks > 0 ? blocks : 1;
+        return e;
+    });
+}
+
 cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, int job_count, cudaStream_t stream)
 {
     const int n = b.slot_count > job_count ? b.slot_count : job_count;
@@ -429,11 +543,12 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
                         cudaStream_t stream)
 {
     const int g = launch.blocks;
+    const int tg = launch.trace_blocks > 0 ? launch.trace_blocks : launch.blocks;
     const auto smemFor = [](int entries) { return static_cast<std::size_t>(entries) * 128 * sizeof(uint2); };
     regenKernel<<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        extendKernel<S><<<g, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        extendKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag);
         return 0;
     });
     shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
@@ -442,7 +557,7 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        shadowKernel<S><<<g, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        shadowKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag);
         return 0;
     });
     advanceKernel<<<1, 1, 0, stream>>>(b.control);

@@ -70,6 +70,10 @@ struct WfControl {
     unsigned long long total_items;
     int job_count;
     int pad;
+    // Queue entries handed out so far in this iteration by the extend and shadow
+    // kernels (which take rays in warp batches as lanes finish).
+    int fetch_extend;
+    int fetch_shadow;
 };
 
 struct WfBuffers {
@@ -84,6 +88,7 @@ struct WfLaunch {
     int blocks;       // grid of the queue kernels (a multiple of the SM count)
     int threads;      // threads per block
     int stack;        // traversal stack entries per thread
+    int trace_blocks; // grid of the persistent traversal kernels (blocks resident at once), or 0 for `blocks`
 };
 
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call
@@ -99,6 +104,9 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
 // Enqueues one iteration (regenerate, extend, shade x 4, shadow, advance). The
 // batch's size is read from the control block, so iterations captured in a graph
 // keep serving jobs appended later.
+// Blocks per SM of the persistent traversal kernels that fit at once with
+// `stack` entries per thread (after wfPrepare).
+cudaError_t wfTraceBlocksPerSm(int stack, int* out);
 cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
                         cudaStream_t stream);
 // Appends jobs [first, first + count) of the (already uploaded) job table to a

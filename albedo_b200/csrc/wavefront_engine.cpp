@@ -126,7 +126,9 @@ void WavefrontEngine::open(int stack, unsigned int* error_flag)
     last_progress_iteration_ = 0;
     cudaCheck(wfReset(buffers_, 0, 0, stream_), "wavefront reset");
     cudaCheck(wfPrepare(stack), "wavefront kernel attributes");
-    const WfLaunch launch{sm_count_ * blocks_per_sm_, 128, stack};
+    int trace_per_sm{1};
+    cudaCheck(wfTraceBlocksPerSm(stack, &trace_per_sm), "traversal residency");
+    const WfLaunch launch{sm_count_ * blocks_per_sm_, 128, stack, sm_count_ * trace_per_sm};
     cudaGraph_t graph{nullptr};
     cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};
