@@ -26,12 +26,13 @@ from pathlib import Path
 
 import numpy as np
 
-from ._lib import Accumulator, BasicMaterialC, MaterialC, RenderJobC, SceneInfoC, library
+from ._lib import Accumulator, BasicMaterialC, CameraC, MaterialC, RenderJobC, SceneInfoC, TuningC, library
 
 ACCUMULATOR_DTYPE = np.dtype([("r", "<f8"), ("g", "<f8"), ("b", "<f8"), ("count", "<i8")])
 
 PATH, SCATTER_ONLY, NORMALS = 0, 1, 2
 MEGAKERNEL, WAVEFRONT = 0, 1
+ACCUMULATE_FP64, ACCUMULATE_KAHAN_FP32 = 0, 1
 
 
 class SceneParseError(ValueError):
@@ -117,10 +118,33 @@ class RenderJob:
     max_depth: int = 64
     roulette_start: int = 3
     method: int = MEGAKERNEL
+    accumulation: int = ACCUMULATE_FP64
 
     def to_c(self) -> RenderJobC:
         return RenderJobC(self.width, self.height, self.samples_per_axis, self.estimator, self.seed, self.max_depth,
-                          self.roulette_start, self.method, 0)
+                          self.roulette_start, self.method, self.accumulation)
+
+
+@dataclass
+class Camera:
+    """CameraSettings (src/albedo/camera/perspective_camera.hpp:13-26) for one render."""
+
+    look_from: tuple
+    look_at: tuple
+    up: tuple = (0.0, 1.0, 0.0)
+    vertical_fov_degrees: float = 60.0
+
+    def to_c(self) -> CameraC:
+        c = CameraC()
+        c.look_from[:] = [float(v) for v in self.look_from]
+        c.look_at[:] = [float(v) for v in self.look_at]
+        c.up[:] = [float(v) for v in self.up]
+        c.vertical_fov_degrees = float(self.vertical_fov_degrees)
+        return c
+
+
+def _camera_ref(camera: Camera | None):
+    return None if camera is None else byref(camera.to_c())
 
 
 class PixelBuffer:
@@ -302,14 +326,19 @@ def render_image_ptr(scene: Scene, job: RenderJob, host_accumulators_ptr: int) -
     _raise(library().albedo_render_host(scene.handle, byref(c), c_void_p(host_accumulators_ptr)))
 
 
-def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: int = 0) -> None:
-    """Stream-ordered render into a device array of width*height accumulators."""
+def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: int = 0,
+                  camera: Camera | None = None) -> None:
+    """Stream-ordered render into a device array of width*height accumulators,
+    from `camera` instead of the scene's when given."""
     c = job.to_c()
-    _raise(library().albedo_render(scene.handle, byref(c), c_void_p(accumulators_ptr), c_void_p(stream)))
+    if camera is None:
+        _raise(library().albedo_render(scene.handle, byref(c), c_void_p(accumulators_ptr), c_void_p(stream)))
+    else:
+        _raise(library().albedo_render_view(scene.handle, byref(c), _camera_ref(camera), c_void_p(accumulators_ptr),
+                                            c_void_p(stream)))
 
 
-def render_batch(items, stream: int = 0) -> None:
-    """Renders [(scene, job, device_accumulators_ptr), ...] in one wavefront run."""
+def _batch_array(items):
     from ._lib import BatchItemC
 
     array = (BatchItemC * len(items))()
@@ -317,7 +346,44 @@ def render_batch(items, stream: int = 0) -> None:
         array[i].scene = scene.handle.value
         array[i].job = job.to_c()
         array[i].accumulators = ptr
-    _raise(library().albedo_render_batch(array, len(items), c_void_p(stream)))
+    return array
+
+
+def render_batch(items, stream: int = 0) -> None:
+    """Renders [(scene, job, device_accumulators_ptr), ...] in one wavefront run."""
+    _raise(library().albedo_render_batch(_batch_array(items), len(items), c_void_p(stream)))
+
+
+_TUNING_FIELDS = ["tile_width", "blocks_per_sm", "trace_blocks_per_sm", "fetch_batch", "iterations_per_graph",
+                  "slot_count", "evaluations", "best_ms", "default_ms"]
+
+
+def _tuning_dict(t: TuningC) -> dict:
+    return {k: getattr(t, k) for k in _TUNING_FIELDS}
+
+
+def autotune_megakernel(scene: Scene, job: RenderJob) -> dict:
+    """Times every megakernel shape (tile width x register budget) on `job` at a
+    quarter of its samples and keeps the fastest for `scene`."""
+    out = TuningC()
+    c = job.to_c()
+    _raise(library().albedo_autotune_megakernel(scene.handle, byref(c), byref(out)))
+    return _tuning_dict(out)
+
+
+def autotune_batch(items) -> dict:
+    """Tunes the wavefront engine's shape on [(scene, job, ptr), ...] (the
+    accumulators are not touched) and keeps it for later batches and servers."""
+    out = TuningC()
+    _raise(library().albedo_autotune_batch(_batch_array(items), len(items), byref(out)))
+    return _tuning_dict(out)
+
+
+def tuning(scene: Scene | None = None) -> dict:
+    """The shape renders use now: the scene's megakernel shape, or (no scene) the wavefront engine's."""
+    out = TuningC()
+    _raise(library().albedo_tuning_get(None if scene is None else scene.handle, byref(out)))
+    return _tuning_dict(out)
 
 
 class Server:
@@ -328,11 +394,11 @@ class Server:
         _raise(library().albedo_server_create(memory_budget_bytes, slots, byref(handle)))
         self._handle = handle
 
-    def submit(self, scene: Scene, job: RenderJob, accumulators_ptr: int) -> int:
+    def submit(self, scene: Scene, job: RenderJob, accumulators_ptr: int, camera: Camera | None = None) -> int:
         c = job.to_c()
         ticket = ctypes.c_int64()
-        _raise(library().albedo_server_submit(self._handle, scene.handle, byref(c), c_void_p(accumulators_ptr),
-                                              byref(ticket)))
+        _raise(library().albedo_server_submit_view(self._handle, scene.handle, byref(c), _camera_ref(camera),
+                                                   c_void_p(accumulators_ptr), byref(ticket)))
         return ticket.value
 
     def step(self, capacity: int = 4096) -> list[int]:
@@ -340,6 +406,12 @@ class Server:
         count = c_int32()
         _raise(library().albedo_server_step(self._handle, out, capacity, byref(count)))
         return [out[i] for i in range(count.value)]
+
+    def rays(self) -> int:
+        """Ray queries the current batch has traced as of the last polled step."""
+        out = ctypes.c_int64()
+        _raise(library().albedo_server_rays(self._handle, byref(out)))
+        return out.value
 
     def pending(self) -> tuple[int, int]:
         waiting, running = c_int32(), c_int32()
@@ -366,6 +438,13 @@ def wavefront_configure(slots: int = 1 << 20, blocks_per_sm: int = 8, iterations
 def wavefront_last_iterations() -> int:
     out = ctypes.c_int64()
     _raise(library().albedo_wavefront_last_iterations(byref(out)))
+    return out.value
+
+
+def wavefront_last_rays() -> int:
+    """Ray queries (closest hit plus shadow) the last wavefront run traced."""
+    out = ctypes.c_int64()
+    _raise(library().albedo_wavefront_last_rays(byref(out)))
     return out.value
 
 
@@ -397,7 +476,8 @@ def render_pixels(scene: Scene, job: RenderJob, pixels: np.ndarray, with_squares
 
 
 __all__ = [
-    "ACCUMULATOR_DTYPE", "BasicMaterial", "DeviceError", "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer",
-    "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError", "Unsupported", "WAVEFRONT", "read_scene",
-    "render_device", "render_image", "render_pixels", "Accumulator",
+    "ACCUMULATE_FP64", "ACCUMULATE_KAHAN_FP32", "ACCUMULATOR_DTYPE", "BasicMaterial", "Camera", "DeviceError",
+    "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
+    "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
+    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "tuning", "wavefront_last_rays",
 ]

@@ -16,7 +16,18 @@ class Accumulator(ctypes.Structure):
 class RenderJobC(ctypes.Structure):
     _fields_ = [("width", c_int32), ("height", c_int32), ("samples_per_axis", c_int32), ("estimator", c_int32),
                 ("seed", c_uint64), ("max_depth", c_int32), ("roulette_start", c_int32), ("method", c_int32),
-                ("reserved", c_int32)]
+                ("accumulation", c_int32)]
+
+
+class CameraC(ctypes.Structure):
+    _fields_ = [("look_from", c_double * 3), ("look_at", c_double * 3), ("up", c_double * 3),
+                ("vertical_fov_degrees", c_double)]
+
+
+class TuningC(ctypes.Structure):
+    _fields_ = [("tile_width", c_int32), ("blocks_per_sm", c_int32), ("trace_blocks_per_sm", c_int32),
+                ("fetch_batch", c_int32), ("iterations_per_graph", c_int32), ("slot_count", c_int32),
+                ("evaluations", c_int32), ("reserved", c_int32), ("best_ms", c_double), ("default_ms", c_double)]
 
 
 class BatchItemC(ctypes.Structure):
@@ -65,6 +76,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_scene_get_info": (c_int32, [c_void_p, POINTER(SceneInfoC)]),
     "albedo_render": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
     "albedo_render_host": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p]),
+    "albedo_render_view": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(CameraC), c_void_p, c_void_p]),
     "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
     "albedo_scene_check": (c_int32, [c_void_p]),
     "albedo_render_work_counts": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(c_int64)]),
@@ -73,10 +85,17 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_wavefront_configure": (c_int32, [c_int32, c_int32, c_int32]),
     "albedo_server_create": (c_int32, [c_int64, c_int32, POINTER(c_void_p)]),
     "albedo_server_submit": (c_int32, [c_void_p, c_void_p, POINTER(RenderJobC), c_void_p, POINTER(c_int64)]),
+    "albedo_server_submit_view": (c_int32, [c_void_p, c_void_p, POINTER(RenderJobC), POINTER(CameraC), c_void_p,
+                                            POINTER(c_int64)]),
     "albedo_server_step": (c_int32, [c_void_p, POINTER(c_int64), c_int32, POINTER(c_int32)]),
     "albedo_server_pending": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
     "albedo_server_destroy": (None, [c_void_p]),
+    "albedo_autotune_megakernel": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(TuningC)]),
+    "albedo_autotune_batch": (c_int32, [c_void_p, c_int32, POINTER(TuningC)]),
+    "albedo_tuning_get": (c_int32, [c_void_p, POINTER(TuningC)]),
     "albedo_wavefront_last_iterations": (c_int32, [POINTER(c_int64)]),
+    "albedo_wavefront_last_rays": (c_int32, [POINTER(c_int64)]),
+    "albedo_server_rays": (c_int32, [c_void_p, POINTER(c_int64)]),
     "albedo_trace_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, _I, _F, _I, _I, _F, _F, _F, _I]),
     "albedo_occluded_host": (c_int32, [c_void_p, _F, _F, c_int64, _I]),
     "albedo_probe_pixel_stream": (c_int32, [c_uint64, c_int32, c_int32, c_int32, c_int32, _U, _F]),

@@ -3,6 +3,7 @@
 // thread-local message; CUDA errors become ALBEDO_DEVICE_ERROR.
 #include "../../include/albedo_b200.h"
 
+#include "autotune.hpp"
 #include "host/flatten.hpp"
 #include "host/scene_file.hpp"
 #include "kernels/launch.hpp"
@@ -10,6 +11,7 @@
 
 #include <algorithm>
 #include <deque>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <set>
@@ -187,6 +189,9 @@ struct albedo_scene {
     int stack_capacity{0};
     std::vector<DeviceBuffer> buffers;
     DeviceBuffer error_flag;
+    // Megakernel launch shape the autotuner kept for this scene (0: default).
+    int mega_tile_width{0};
+    int mega_blocks_per_sm{0};
 
     void requireOpen() const
     {
@@ -301,6 +306,13 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     if (job.method == ALBEDO_WAVEFRONT && job.estimator != ALBEDO_PATH) {
         throw Unsupported{"the wavefront renderer implements the path estimator only"};
     }
+    if (job.accumulation != ALBEDO_ACCUMULATE_FP64 && job.accumulation != ALBEDO_ACCUMULATE_KAHAN_FP32) {
+        throw std::invalid_argument{"unknown accumulation"};
+    }
+    if (job.accumulation == ALBEDO_ACCUMULATE_KAHAN_FP32 &&
+        (job.method != ALBEDO_MEGAKERNEL || job.estimator != ALBEDO_PATH)) {
+        throw Unsupported{"compensated FP32 accumulation is implemented for the megakernel's path estimator only"};
+    }
     RenderArgs args{};
     args.width = job.width;
     args.height = job.height;
@@ -309,7 +321,25 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     args.seed = job.seed;
     args.max_depth = job.max_depth;
     args.roulette_start = job.roulette_start;
+    args.tile_width = scene.mega_tile_width;
+    args.blocks_per_sm = scene.mega_blocks_per_sm;
+    args.accumulation = job.accumulation;
     return args;
+}
+
+CameraSettings cameraFrom(const albedo_camera& c)
+{
+    const auto v = [](const double* p) { return Vec3{p[0], p[1], p[2]}; };
+    return CameraSettings{v(c.look_from), v(c.look_at), v(c.up), c.vertical_fov_degrees};
+}
+
+// The device camera of a render: the request's view, else the scene's camera.
+DevCamera cameraFor(const albedo_scene& scene, const albedo_render_job& job, const albedo_camera* view)
+{
+    if (view != nullptr) {
+        return deviceCamera(cameraFrom(*view), job.width, job.height);
+    }
+    return deviceCamera(scene.host, job.width, job.height);
 }
 
 // The process's wavefront engine on the current device, created on first use.
@@ -318,9 +348,9 @@ constexpr int kBatchJobCapacity{4096};
 std::mutex g_engine_mutex;
 std::unique_ptr<WavefrontEngine> g_engine;
 int g_engine_slots{kDefaultSlots};
-int g_engine_blocks_per_sm{8};
-int g_engine_iterations_per_graph{4};
+WfShape g_engine_shape{};
 unsigned long long g_last_iterations{0};
+unsigned long long g_last_rays{0};
 
 void configureEngine(int slots, int blocks_per_sm, int iterations_per_graph)
 {
@@ -332,8 +362,14 @@ void configureEngine(int slots, int blocks_per_sm, int iterations_per_graph)
         g_engine.reset();
     }
     g_engine_slots = slots;
-    g_engine_blocks_per_sm = blocks_per_sm;
-    g_engine_iterations_per_graph = iterations_per_graph;
+    g_engine_shape.blocks_per_sm = blocks_per_sm;
+    g_engine_shape.iterations_per_graph = iterations_per_graph;
+}
+
+WfShape engineShape()
+{
+    const std::lock_guard lock{g_engine_mutex};
+    return g_engine_shape;
 }
 
 unsigned long long lastEngineIterations()
@@ -342,14 +378,15 @@ unsigned long long lastEngineIterations()
     return g_last_iterations;
 }
 
-WfJob wavefrontJob(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum)
+WfJob wavefrontJob(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum,
+                   const albedo_camera* view = nullptr)
 {
     albedo_render_job wf{job};
     wf.method = ALBEDO_WAVEFRONT;
     static_cast<void>(renderArgsFor(scene, wf));
     WfJob j{};
     j.scene = scene.dev;
-    j.camera = deviceCamera(scene.host, job.width, job.height);
+    j.camera = cameraFor(scene, job, view);
     j.accum = accum;
     j.width = job.width;
     j.height = job.height;
@@ -367,9 +404,10 @@ void runWavefront(const std::vector<WfJob>& jobs, int stack, unsigned int* error
         if (!g_engine) {
             g_engine = std::make_unique<WavefrontEngine>(g_engine_slots, kBatchJobCapacity);
         }
-        g_engine->setLaunch(g_engine_blocks_per_sm, g_engine_iterations_per_graph);
+        g_engine->setShape(g_engine_shape);
         g_engine->render(jobs, stack, error_flag, stream);
         g_last_iterations = g_engine->lastIterations();
+        g_last_rays = g_engine->lastRays();
     } catch (const std::bad_alloc&) {
         throw;
     } catch (const std::invalid_argument&) {
@@ -442,18 +480,84 @@ struct albedo_server {
 
 namespace {
 
-void renderOnDevice(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum, cudaStream_t stream)
+void renderOnDevice(const albedo_scene& scene, const albedo_render_job& job, PixelAccum* accum, cudaStream_t stream,
+                    const albedo_camera* view = nullptr)
 {
     const RenderArgs args{renderArgsFor(scene, job)};
     if (job.method == ALBEDO_WAVEFRONT) {
-        runWavefront({wavefrontJob(scene, job, accum)}, scene.stack_capacity, scene.error_flag.as<unsigned int>(),
-                     stream);
+        runWavefront({wavefrontJob(scene, job, accum, view)}, scene.stack_capacity,
+                     scene.error_flag.as<unsigned int>(), stream);
         return;
     }
-    const DevCamera camera{deviceCamera(scene.host, job.width, job.height)};
+    const DevCamera camera{cameraFor(scene, job, view)};
     check(launchMegakernel(scene.dev, camera, args, accum, scene.error_flag.as<unsigned int>(), scene.stack_capacity,
                            stream),
           "render launch");
+}
+
+} // namespace
+
+namespace {
+
+// Events and a stream for timing candidate shapes.
+class TuneTimer {
+public:
+    TuneTimer()
+    {
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "tuning stream");
+        check(cudaEventCreate(&start_), "tuning event");
+        check(cudaEventCreate(&stop_), "tuning event");
+    }
+    ~TuneTimer()
+    {
+        cudaStreamSynchronize(stream_);
+        cudaEventDestroy(start_);
+        cudaEventDestroy(stop_);
+        cudaStreamDestroy(stream_);
+    }
+    TuneTimer(const TuneTimer&) = delete;
+    TuneTimer& operator=(const TuneTimer&) = delete;
+
+    cudaStream_t stream() const { return stream_; }
+
+    // One untimed run, then the fastest of `repeats` timed runs, in ms.
+    template <typename Run>
+    double time(Run&& run, int repeats)
+    {
+        run();
+        check(cudaStreamSynchronize(stream_), "tuning run");
+        double best{std::numeric_limits<double>::infinity()};
+        for (int i{0}; i < repeats; ++i) {
+            check(cudaEventRecord(start_, stream_), "event record");
+            run();
+            check(cudaEventRecord(stop_, stream_), "event record");
+            check(cudaEventSynchronize(stop_), "event sync");
+            float ms{0};
+            check(cudaEventElapsedTime(&ms, start_, stop_), "event time");
+            best = std::min(best, static_cast<double>(ms));
+        }
+        return best;
+    }
+
+private:
+    cudaStream_t stream_{nullptr};
+    cudaEvent_t start_{nullptr};
+    cudaEvent_t stop_{nullptr};
+};
+
+// The tuning work: the caller's job at a quarter of its samples.
+albedo_render_job tuningJob(const albedo_render_job& job)
+{
+    albedo_render_job probe{job};
+    probe.samples_per_axis = std::max(1, job.samples_per_axis / 2);
+    return probe;
+}
+
+void fillTuning(albedo_tuning* out, const TuneOutcome& outcome)
+{
+    out->evaluations = outcome.evaluations;
+    out->best_ms = outcome.best_ms;
+    out->default_ms = outcome.start_ms;
 }
 
 } // namespace
@@ -687,6 +791,15 @@ int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albed
     });
 }
 
+int albedo_render_view(const albedo_scene* scene, const albedo_render_job* job, const albedo_camera* camera,
+                       albedo_accumulator* accumulators, void* stream)
+{
+    return guarded([&] {
+        renderOnDevice(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators), static_cast<cudaStream_t>(stream),
+                       camera);
+    });
+}
+
 int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators)
 {
     return guarded([&] {
@@ -748,6 +861,134 @@ int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_
     return guarded([&] { configureEngine(slot_count, blocks_per_sm, iterations_per_graph); });
 }
 
+int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out)
+{
+    return guarded([&] {
+        *out = albedo_tuning{};
+        albedo_render_job probe{tuningJob(*job)};
+        probe.method = ALBEDO_MEGAKERNEL;
+        static_cast<void>(renderArgsFor(*scene, probe));
+        const std::size_t pixels{static_cast<std::size_t>(probe.width) * static_cast<std::size_t>(probe.height)};
+        DeviceBuffer scratch{pixels * sizeof(PixelAccum)};
+        TuneTimer timer;
+        const std::vector<TuneKnob> knobs{{"tile_width", {8, 16, 32}}, {"blocks_per_sm", {3, 4}}};
+        const int kept_tile{scene->mega_tile_width};
+        const int kept_blocks{scene->mega_blocks_per_sm};
+        TuneOutcome outcome;
+        try {
+            outcome = tuneExhaustive(knobs, {16, 3}, [&](const std::vector<int>& v) {
+                scene->mega_tile_width = v[0];
+                scene->mega_blocks_per_sm = v[1];
+                return timer.time([&] { renderOnDevice(*scene, probe, scratch.as<PixelAccum>(), timer.stream()); },
+                                  2);
+            });
+        } catch (...) {
+            scene->mega_tile_width = kept_tile;
+            scene->mega_blocks_per_sm = kept_blocks;
+            throw;
+        }
+        scene->mega_tile_width = outcome.best[0];
+        scene->mega_blocks_per_sm = outcome.best[1];
+        scene->collectKernelError();
+        out->tile_width = outcome.best[0];
+        out->blocks_per_sm = outcome.best[1];
+        fillTuning(out, outcome);
+    });
+}
+
+int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_tuning* out)
+{
+    return guarded([&] {
+        *out = albedo_tuning{};
+        if (count <= 0) {
+            throw std::invalid_argument{"tuning needs at least one job"};
+        }
+        std::size_t pixels{0};
+        int stack{32};
+        for (int32_t i{0}; i < count; ++i) {
+            const albedo_render_job probe{tuningJob(items[i].job)};
+            static_cast<void>(wavefrontJob(*items[i].scene, probe, nullptr));
+            pixels += static_cast<std::size_t>(probe.width) * static_cast<std::size_t>(probe.height);
+            stack = std::max(stack, items[i].scene->stack_capacity);
+        }
+        DeviceBuffer scratch{pixels * sizeof(PixelAccum)};
+        std::vector<WfJob> jobs;
+        std::size_t offset{0};
+        for (int32_t i{0}; i < count; ++i) {
+            const albedo_render_job probe{tuningJob(items[i].job)};
+            jobs.push_back(wavefrontJob(*items[i].scene, probe, scratch.as<PixelAccum>() + offset));
+            offset += static_cast<std::size_t>(probe.width) * static_cast<std::size_t>(probe.height);
+        }
+        unsigned int* error_flag{items[0].scene->error_flag.as<unsigned int>()};
+        TuneTimer timer;
+        const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {2, 3, 4}},
+                                          {"fetch_batch", {16, 32, 64, 128}},
+                                          {"blocks_per_sm", {4, 8, 16}},
+                                          {"iterations_per_graph", {2, 4, 8}},
+                                          {"slot_count", {1 << 19, 1 << 20, 1 << 21}}};
+        const WfShape kept_shape{engineShape()};
+        int kept_slots{0};
+        {
+            const std::lock_guard lock{g_engine_mutex};
+            kept_slots = g_engine_slots;
+        }
+        const auto apply = [](const std::vector<int>& v) {
+            WfShape shape{};
+            shape.trace_blocks_per_sm = v[0];
+            shape.fetch_batch = v[1];
+            shape.blocks_per_sm = v[2];
+            shape.iterations_per_graph = v[3];
+            const std::lock_guard lock{g_engine_mutex};
+            if (g_engine && g_engine->slotCount() != v[4]) {
+                g_engine.reset();
+            }
+            g_engine_slots = v[4];
+            g_engine_shape = shape;
+        };
+        const std::vector<int> start{kept_shape.trace_blocks_per_sm > 0 ? kept_shape.trace_blocks_per_sm : 4,
+                                     kept_shape.fetch_batch, kept_shape.blocks_per_sm,
+                                     kept_shape.iterations_per_graph, kept_slots};
+        TuneOutcome outcome;
+        try {
+            outcome = tuneCoordinateDescent(knobs, start, [&](const std::vector<int>& v) {
+                apply(v);
+                return timer.time([&] { runWavefront(jobs, stack, error_flag, timer.stream()); }, 2);
+            }, 1);
+        } catch (...) {
+            apply(start);
+            throw;
+        }
+        apply(outcome.best);
+        for (int32_t i{0}; i < count; ++i) {
+            items[i].scene->collectKernelError();
+        }
+        out->trace_blocks_per_sm = outcome.best[0];
+        out->fetch_batch = outcome.best[1];
+        out->blocks_per_sm = outcome.best[2];
+        out->iterations_per_graph = outcome.best[3];
+        out->slot_count = outcome.best[4];
+        fillTuning(out, outcome);
+    });
+}
+
+int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out)
+{
+    return guarded([&] {
+        *out = albedo_tuning{};
+        if (scene != nullptr) {
+            out->tile_width = scene->mega_tile_width > 0 ? scene->mega_tile_width : 16;
+            out->blocks_per_sm = scene->mega_blocks_per_sm > 0 ? scene->mega_blocks_per_sm : 3;
+            return;
+        }
+        const std::lock_guard lock{g_engine_mutex};
+        out->trace_blocks_per_sm = g_engine_shape.trace_blocks_per_sm;
+        out->fetch_batch = g_engine_shape.fetch_batch;
+        out->blocks_per_sm = g_engine_shape.blocks_per_sm;
+        out->iterations_per_graph = g_engine_shape.iterations_per_graph;
+        out->slot_count = g_engine_slots;
+    });
+}
+
 int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo_server** out)
 {
     *out = nullptr;
@@ -758,6 +999,7 @@ int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo
         auto server{std::make_unique<albedo_server>()};
         try {
             server->engine = std::make_unique<WavefrontEngine>(slot_count, kBatchJobCapacity);
+            server->engine->setShape(engineShape());
         } catch (const std::bad_alloc&) {
             throw;
         } catch (const std::exception& e) {
@@ -776,11 +1018,17 @@ int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo
 int albedo_server_submit(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
                          albedo_accumulator* accumulators, int64_t* out_ticket)
 {
+    return albedo_server_submit_view(server, scene, job, nullptr, accumulators, out_ticket);
+}
+
+int albedo_server_submit_view(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
+                              const albedo_camera* camera, albedo_accumulator* accumulators, int64_t* out_ticket)
+{
     return guarded([&] {
         albedo_server::Request request;
+        request.job = wavefrontJob(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators), camera);
         request.ticket = server->next_ticket++;
         request.scene = scene;
-        request.job = wavefrontJob(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators));
         request.bytes = static_cast<std::int64_t>(job->width) * job->height * static_cast<std::int64_t>(sizeof(PixelAccum));
         const std::int64_t fixed{static_cast<std::int64_t>(server->engine->deviceBytes())};
         if (fixed + request.bytes + static_cast<std::int64_t>(scene->deviceBytes()) > server->budget) {
@@ -851,6 +1099,19 @@ void albedo_server_destroy(albedo_server* server) { delete server; }
 int albedo_wavefront_last_iterations(int64_t* out)
 {
     return guarded([&] { *out = static_cast<int64_t>(lastEngineIterations()); });
+}
+
+int albedo_wavefront_last_rays(int64_t* out)
+{
+    return guarded([&] {
+        const std::lock_guard lock{g_engine_mutex};
+        *out = static_cast<int64_t>(g_last_rays);
+    });
+}
+
+int albedo_server_rays(const albedo_server* server, int64_t* out)
+{
+    return guarded([&] { *out = static_cast<int64_t>(server->engine->lastRays()); });
 }
 
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,

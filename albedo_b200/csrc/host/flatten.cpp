@@ -388,7 +388,12 @@ DeviceImage flattenScene(const HostScene& scene)
 
 DevCamera deviceCamera(const HostScene& scene, int width, int height)
 {
-    const CameraFrame frame{scene.cameraFrame(static_cast<double>(width) / static_cast<double>(height))};
+    return deviceCamera(scene.camera, width, height);
+}
+
+DevCamera deviceCamera(const CameraSettings& settings, int width, int height)
+{
+    const CameraFrame frame{buildCameraFrame(settings, static_cast<double>(width) / static_cast<double>(height))};
     DevCamera cam{};
     const auto put = [](float* out, Vec3 v) {
         out[0] = f32(v.x);

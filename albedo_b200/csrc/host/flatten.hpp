@@ -34,5 +34,6 @@ DeviceImage flattenScene(const HostScene& scene);
 
 // The camera frame for an image of the given size, rounded to FP32.
 DevCamera deviceCamera(const HostScene& scene, int width, int height);
+DevCamera deviceCamera(const CameraSettings& settings, int width, int height);
 
 } // namespace albedo_b200

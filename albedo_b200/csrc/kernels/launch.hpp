@@ -28,7 +28,18 @@ struct RenderArgs {
     const int2* pixels;  // optional pixel subset (x, y); null renders the whole image
     int pixel_count;
     double* sum_squares; // optional per-pixel (or per-listed-pixel) sums of squared samples, 3 doubles each
+    // Launch shape of the megakernel (the autotuner's knobs): pixel tile width
+    // (8, 16 or 32; tiles hold 128 pixels) and register budget (resident blocks
+    // per SM the kernel is compiled for: 3 or 4). 0 picks the default (16, 3).
+    int tile_width;
+    int blocks_per_sm;
+    // Per-pixel sums inside the kernel: kAccumulateFp64, or kAccumulateKahan
+    // (compensated FP32, path estimator only). Either is added to the FP64
+    // accumulators at the end.
+    int accumulation;
 };
+
+enum Accumulation : int { kAccumulateFp64 = 0, kAccumulateKahan = 1 };
 
 // Stack capacity (entries per thread) of the kernel chosen for a scene, or 0 if
 // the scene's hierarchy is deeper than every compiled variant supports.

@@ -2,8 +2,8 @@
 //
 // renderPixel (render/render_image.cpp:27-44): each pixel owns one PCG32 stream
 // and draws its n x n stratified samples from it in row-major order, so one
-// thread runs one pixel's samples serially. Blocks cover 16 x 8 pixel tiles so a
-// warp's camera rays start coherent. The traversal stack of every thread sits in
+// thread runs one pixel's samples serially. Blocks cover tiles of 128 pixels
+// (16 x 8 by default) so a warp's camera rays start coherent. The traversal stack of every thread sits in
 // shared memory (STACK entries of 8 bytes).
 #include "estimator.cuh"
 
@@ -12,21 +12,58 @@ namespace albedo_b200 {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kTileW = 16;
-constexpr int kTileH = 8;
-// Resident blocks per SM the megakernel's register budget is sized for: 3
-// (168 registers a thread) measured 4-12% faster than 4 (128 registers, with
-// local-memory spills) on the room and trefoil scenes.
-#ifndef ALBEDO_MEGA_BLOCKS_PER_SM
-#define ALBEDO_MEGA_BLOCKS_PER_SM 3
-#endif
-constexpr int kMegaBlocksPerSm = ALBEDO_MEGA_BLOCKS_PER_SM;
+constexpr int kTileW = 16; // default tile: 16 x 8 pixels
+// Resident blocks per SM the megakernel's register budget is sized for by
+// default: 3 (168 registers a thread) measured 4-12% faster than 4 (128
+// registers, with local-memory spills) on the room and trefoil scenes. The
+// path estimator is also compiled for 4; the autotuner picks per scene.
+constexpr int kMegaBlocksPerSm = 3;
 
-template <int STACK, int EST, bool COUNT = false>
-__global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const DevScene scene, const DevCamera camera,
-                                                     const RenderArgs args, PixelAccum* accum,
-                                                     unsigned int* error_flag,
-                                                     unsigned long long* totals = nullptr)
+// Per-pixel running sums: FP64, or FP32 with Kahan compensation.
+template <int ACC>
+struct PixelSums;
+
+template <>
+struct PixelSums<kAccumulateFp64> {
+    double r = 0.0, g = 0.0, b = 0.0;
+    ALB_DEV void add(float3 v)
+    {
+        r += v.x;
+        g += v.y;
+        b += v.z;
+    }
+    ALB_DEV double3 total() const { return make_double3(r, g, b); }
+};
+
+template <>
+struct PixelSums<kAccumulateKahan> {
+    float r = 0.0f, g = 0.0f, b = 0.0f;
+    float cr = 0.0f, cg = 0.0f, cb = 0.0f;
+    // Kahan 1965: c carries the low-order part lost by the previous addition.
+    static ALB_DEV void kahan(float& sum, float& c, float v)
+    {
+        const float y = __fsub_rn(v, c);
+        const float t = __fadd_rn(sum, y);
+        c = __fsub_rn(__fsub_rn(t, sum), y);
+        sum = t;
+    }
+    ALB_DEV void add(float3 v)
+    {
+        kahan(r, cr, v.x);
+        kahan(g, cg, v.y);
+        kahan(b, cb, v.z);
+    }
+    ALB_DEV double3 total() const
+    {
+        return make_double3(static_cast<double>(r) - cr, static_cast<double>(g) - cg, static_cast<double>(b) - cb);
+    }
+};
+
+template <int STACK, int EST, bool COUNT = false, int MINB = kMegaBlocksPerSm, int ACC = kAccumulateFp64>
+__global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene, const DevCamera camera,
+                                                          const RenderArgs args, PixelAccum* accum,
+                                                          unsigned int* error_flag,
+                                                          unsigned long long* totals = nullptr)
 {
     extern __shared__ uint2 stack[];
     TraversalCounts counts{0, 0, 0, 0, 0};
@@ -40,9 +77,11 @@ __global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const Dev
         x = args.pixels[slot].x;
         y = args.pixels[slot].y;
     } else {
-        const int tiles_x = (args.width + kTileW - 1) / kTileW;
-        x = (blockIdx.x % tiles_x) * kTileW + static_cast<int>(threadIdx.x % kTileW);
-        y = (blockIdx.x / tiles_x) * kTileH + static_cast<int>(threadIdx.x / kTileW);
+        const int tile_w = args.tile_width > 0 ? args.tile_width : kTileW;
+        const int tile_h = kBlock / tile_w;
+        const int tiles_x = (args.width + tile_w - 1) / tile_w;
+        x = (blockIdx.x % tiles_x) * tile_w + static_cast<int>(threadIdx.x) % tile_w;
+        y = (blockIdx.x / tiles_x) * tile_h + static_cast<int>(threadIdx.x) / tile_w;
         if (x >= args.width || y >= args.height) {
             return;
         }
@@ -54,7 +93,7 @@ __global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const Dev
     const float inv_n = 1.0f / static_cast<float>(n);
     const float width = static_cast<float>(args.width);
     const float height = static_cast<float>(args.height);
-    double sr = 0.0, sg = 0.0, sb = 0.0;
+    PixelSums<ACC> sums;
     double qr = 0.0, qg = 0.0, qb = 0.0;
     // One bounce per iteration: a lane whose path ends starts the pixel's next
     // sample at once (drawing its jitter next from the same stream, as the
@@ -69,9 +108,7 @@ __global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const Dev
             continue;
         }
         const float3 L = path.result;
-        sr += L.x;
-        sg += L.y;
-        sb += L.z;
+        sums.add(L);
         qr += static_cast<double>(L.x) * L.x;
         qg += static_cast<double>(L.y) * L.y;
         qb += static_cast<double>(L.z) * L.z;
@@ -81,9 +118,10 @@ __global__ void __launch_bounds__(kBlock, kMegaBlocksPerSm) megakernel(const Dev
         startSample(camera, path, g, x, y, sample, n, inv_n, width, height);
     }
     PixelAccum& a = accum[slot];
-    a.r += sr;
-    a.g += sg;
-    a.b += sb;
+    const double3 total_sum = sums.total();
+    a.r += total_sum.x;
+    a.g += total_sum.y;
+    a.b += total_sum.z;
     a.count += static_cast<long long>(n) * n;
     if (args.sum_squares != nullptr) {
         args.sum_squares[3 * slot] += qr;
@@ -167,7 +205,9 @@ int megaBlocks(const RenderArgs& args)
     if (args.pixels != nullptr) {
         return (args.pixel_count + kBlock - 1) / kBlock;
     }
-    return ((args.width + kTileW - 1) / kTileW) * ((args.height + kTileH - 1) / kTileH);
+    const int tile_w = args.tile_width > 0 ? args.tile_width : kTileW;
+    const int tile_h = kBlock / tile_w;
+    return ((args.width + tile_w - 1) / tile_w) * ((args.height + tile_h - 1) / tile_h);
 }
 
 // Launches `kernel` over `blocks` blocks with a STACK-entry shared-memory stack.
@@ -226,6 +266,14 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
             return launchStacked<S>(megakernel<S, kEstimatorNormals>, megaBlocks(args), stream, scene, camera, args,
                                     accum, error_flag, no_totals);
         default:
+            if (args.accumulation == kAccumulateKahan) {
+                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan>,
+                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
+            }
+            if (args.blocks_per_sm == 4) {
+                return launchStacked<S>(megakernel<S, kEstimatorPath, false, 4>, megaBlocks(args), stream, scene,
+                                        camera, args, accum, error_flag, no_totals);
+            }
             return launchStacked<S>(megakernel<S, kEstimatorPath>, megaBlocks(args), stream, scene, camera, args,
                                     accum, error_flag, no_totals);
         }

@@ -60,9 +60,8 @@ ALB_DEV unsigned long long claimItem(unsigned long long* next, bool want)
 }
 
 // Deals queue entries [0, count) to the lanes of a warp that need a ray, in
-// lane order; the warp claims kFetchBatch entries at a time with one atomicAdd.
+// lane order; the warp claims `batch` entries at a time with one atomicAdd.
 // All 32 lanes call take() together.
-constexpr int kFetchBatch = 32;
 
 // Resident blocks per SM the traversal kernels' register budget is sized for.
 #ifndef ALBEDO_TRACE_BLOCKS_PER_SM
@@ -73,6 +72,7 @@ constexpr int kTraceBlocksPerSm = ALBEDO_TRACE_BLOCKS_PER_SM;
 struct WarpFetch {
     int next;
     int end;
+    int batch;
     bool drained;
 
     ALB_DEV int take(int* counter, int count, bool want)
@@ -85,7 +85,7 @@ struct WarpFetch {
             if (next >= end) {
                 int base = 0;
                 if (lane == 0) {
-                    base = atomicAdd(counter, kFetchBatch);
+                    base = atomicAdd(counter, batch);
                 }
                 base = __shfl_sync(0xFFFFFFFFu, base, 0);
                 if (base >= count) {
@@ -93,7 +93,7 @@ struct WarpFetch {
                     break;
                 }
                 next = base;
-                end = base + kFetchBatch < count ? base + kFetchBatch : count;
+                end = base + batch < count ? base + batch : count;
             }
             const int avail = end - next;
             const int rank = __popc(need & below);
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
 // same order, as a query traced alone.
 template <int STACK>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
-                                                    unsigned int* error_flag)
+                                                                        unsigned int* error_flag, int fetch_batch)
 {
     extern __shared__ uint2 stack[];
     WfControl* ctl = b.control;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJ
     const WfSlots& sl = b.slots;
     uint2* const lane_stack = stack + threadIdx.x;
     const int stride = static_cast<int>(blockDim.x);
-    WarpFetch fetch{0, 0, false};
+    WarpFetch fetch{0, 0, fetch_batch, false};
     TraceState q;
     SkipRule skip = SkipRule::none();
     const DevScene* scene = nullptr;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(128) shadeKernel(const WfJob* __restrict__ job
 // their path. Persistent, like extendKernel.
 template <int STACK>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
-                                                    unsigned int* error_flag)
+                                                                        unsigned int* error_flag, int fetch_batch)
 {
     extern __shared__ uint2 stack[];
     WfControl* ctl = b.control;
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJ
     const WfSlots& sl = b.slots;
     uint2* const lane_stack = stack + threadIdx.x;
     const int stride = static_cast<int>(blockDim.x);
-    WarpFetch fetch{0, 0, false};
+    WarpFetch fetch{0, 0, fetch_batch, false};
     TraceState q;
     SkipRule skip = SkipRule::none();
     const DevScene* scene = nullptr;
@@ -421,6 +421,8 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJ
 __global__ void advanceKernel(WfControl* ctl)
 {
     const int parity = ctl->parity;
+    ctl->rays_traced += static_cast<unsigned long long>(ctl->count[kQExtend0 + parity]) +
+                        static_cast<unsigned long long>(ctl->count[kQShadow]);
     ctl->count[kQExtend0 + parity] = 0;
     ctl->count[kQRegen0 + parity] = 0;
     ctl->count[kQDiffuse] = 0;
@@ -458,6 +460,7 @@ __global__ void resetKernel(WfBuffers b, unsigned long long total_items, int job
         ctl->job_count = job_count;
         ctl->fetch_extend = 0;
         ctl->fetch_shadow = 0;
+        ctl->rays_traced = 0;
     }
 }
 
@@ -544,11 +547,12 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
 {
     const int g = launch.blocks;
     const int tg = launch.trace_blocks > 0 ? launch.trace_blocks : launch.blocks;
+    const int fetch = launch.fetch_batch > 0 ? launch.fetch_batch : 32;
     const auto smemFor = [](int entries) { return static_cast<std::size_t>(entries) * 128 * sizeof(uint2); };
     regenKernel<<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        extendKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        extendKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
         return 0;
     });
     shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
@@ -557,7 +561,7 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        shadowKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag);
+        shadowKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
         return 0;
     });
     advanceKernel<<<1, 1, 0, stream>>>(b.control);

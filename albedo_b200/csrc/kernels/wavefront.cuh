@@ -74,6 +74,7 @@ struct WfControl {
     // kernels (which take rays in warp batches as lanes finish).
     int fetch_extend;
     int fetch_shadow;
+    unsigned long long rays_traced; // closest-hit plus shadow queries since the batch opened
 };
 
 struct WfBuffers {
@@ -89,6 +90,7 @@ struct WfLaunch {
     int threads;      // threads per block
     int stack;        // traversal stack entries per thread
     int trace_blocks; // grid of the persistent traversal kernels (blocks resident at once), or 0 for `blocks`
+    int fetch_batch;  // queue entries a traversal warp claims at once (0: 32)
 };
 
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call

@@ -100,13 +100,13 @@ WavefrontEngine::~WavefrontEngine()
     cudaFreeHost(host_control_);
 }
 
-void WavefrontEngine::setLaunch(int blocks_per_sm, int iterations_per_graph)
+void WavefrontEngine::setShape(const WfShape& shape)
 {
-    if (blocks_per_sm <= 0 || iterations_per_graph <= 0) {
-        throw std::invalid_argument{"launch shape must be positive"};
+    if (shape.blocks_per_sm <= 0 || shape.iterations_per_graph <= 0 || shape.trace_blocks_per_sm < 0 ||
+        shape.fetch_batch <= 0) {
+        throw std::invalid_argument{"wavefront launch shape values must be positive"};
     }
-    blocks_per_sm_ = blocks_per_sm;
-    iterations_per_graph_ = iterations_per_graph;
+    shape_ = shape;
 }
 
 void WavefrontEngine::open(int stack, unsigned int* error_flag)
@@ -128,11 +128,14 @@ void WavefrontEngine::open(int stack, unsigned int* error_flag)
     cudaCheck(wfPrepare(stack), "wavefront kernel attributes");
     int trace_per_sm{1};
     cudaCheck(wfTraceBlocksPerSm(stack, &trace_per_sm), "traversal residency");
-    const WfLaunch launch{sm_count_ * blocks_per_sm_, 128, stack, sm_count_ * trace_per_sm};
+    if (shape_.trace_blocks_per_sm > 0) {
+        trace_per_sm = std::min(trace_per_sm, shape_.trace_blocks_per_sm);
+    }
+    const WfLaunch launch{sm_count_ * shape_.blocks_per_sm, 128, stack, sm_count_ * trace_per_sm, shape_.fetch_batch};
     cudaGraph_t graph{nullptr};
     cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};
-    for (int i{0}; i < iterations_per_graph_ && captured == cudaSuccess; ++i) {
+    for (int i{0}; i < shape_.iterations_per_graph && captured == cudaSuccess; ++i) {
         captured = wfIteration(device_jobs_, buffers_, launch, error_flag, stream_);
     }
     const cudaError_t ended{cudaStreamEndCapture(stream_, &graph)};
@@ -206,6 +209,7 @@ std::vector<int> WavefrontEngine::poll()
     const WfControl& snapshot{host_control_[slot]};
     const unsigned long long* done{host_done_ + static_cast<std::size_t>(slot) * job_capacity_};
     last_iterations_ = snapshot.iterations;
+    last_rays_ = snapshot.rays_traced;
     std::vector<int> still;
     for (const int j : in_flight_) {
         // A job submitted after this snapshot was taken is not in it yet.
@@ -273,6 +277,7 @@ void WavefrontEngine::render(const std::vector<WfJob>& jobs, int stack, unsigned
     // Drain the graph still queued after the last poll.
     cudaCheck(cudaStreamSynchronize(stream_), "engine stream");
     last_iterations_ = host_control_[(steps_launched_ - 1) & 1].iterations;
+    last_rays_ = host_control_[(steps_launched_ - 1) & 1].rays_traced;
     close();
     cudaCheck(cudaEventRecord(ordering_, stream_), "ordering event");
     cudaCheck(cudaStreamWaitEvent(caller, ordering_, 0), "ordering wait");

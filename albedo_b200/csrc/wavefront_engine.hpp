@@ -13,6 +13,14 @@
 
 namespace albedo_b200 {
 
+// Launch shape of the wavefront iteration (the autotuner's knobs).
+struct WfShape {
+    int blocks_per_sm{8};         // queue kernels (regenerate, shade): blocks per SM
+    int iterations_per_graph{4};  // iterations captured in one CUDA graph
+    int trace_blocks_per_sm{0};   // persistent traversal kernels: blocks per SM, 0 = as many as fit
+    int fetch_batch{32};          // queue entries a traversal warp claims at once
+};
+
 class WavefrontEngine {
 public:
     // `slot_count` path slots (about 240 bytes each) and a table of `job_capacity`
@@ -48,14 +56,16 @@ public:
     int jobCapacity() const { return job_capacity_; }
     std::size_t deviceBytes() const { return device_bytes_; }
     unsigned long long lastIterations() const { return last_iterations_; }
+    // Ray queries (closest hit and shadow) the last render traced, or the open
+    // batch has traced as of the last poll.
+    unsigned long long lastRays() const { return last_rays_; }
 
-    // Launch shape of the queue kernels; the autotuner sets it. Takes effect at
-    // the next open() or render().
-    void setLaunch(int blocks_per_sm, int iterations_per_graph);
+    // Launch shape; the autotuner sets it. Takes effect at the next open() or
+    // render().
+    void setShape(const WfShape& shape);
+    const WfShape& shape() const { return shape_; }
 
 private:
-    void checkStall();
-
     cudaStream_t stream_{nullptr};
     cudaEvent_t ordering_{nullptr};
     cudaEvent_t step_done_[2]{nullptr, nullptr};
@@ -67,10 +77,10 @@ private:
     WfControl* host_control_{nullptr}; // pinned: a snapshot per step parity
     unsigned long long* host_done_{nullptr}; // pinned: per step parity, job_capacity counters
     int job_capacity_{0};
-    int blocks_per_sm_{8};
-    int iterations_per_graph_{4};
+    WfShape shape_{};
     int sm_count_{148};
     unsigned long long last_iterations_{0};
+    unsigned long long last_rays_{0};
 
     // The open batch.
     bool open_{false};

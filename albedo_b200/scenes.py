@@ -351,3 +351,29 @@ def batch_jobs(directory: Path, count: int = 64, seed: int = 17, scenes: int | N
         n = int(np.clip(round(math.sqrt(spp)), 2, 8))
         jobs.append(BatchJob(scene_paths[j % scene_count], w, h, n, j))
     return jobs
+
+
+def scene_camera(path: Path) -> tuple:
+    """(look_from, look_at, up, fov) of a scene file's `camera from .. at .. up .. fov ..` line."""
+    words = next(line for line in Path(path).read_text().splitlines() if line.startswith("camera")).split()
+    values: dict[str, list[float]] = {}
+    key = None
+    for w in words[1:]:
+        if w in ("from", "at", "up", "fov"):
+            key = w
+            values[key] = []
+        else:
+            values[key].append(float(w))
+    return (tuple(values["from"]), tuple(values["at"]), tuple(values.get("up", (0.0, 1.0, 0.0))),
+            values.get("fov", [60.0])[0])
+
+
+def request_view(base: tuple, rng: np.random.Generator) -> tuple:
+    """A seeded per-request camera around a scene's own: the eye moves up to 1.5
+    units sideways, 0.5 down / 1 up and 1 forward or back; the target up to 0.5
+    sideways and 0.3 vertically; up and field of view stay."""
+    eye, target, up, fov = base
+    eye = (eye[0] + rng.uniform(-1.5, 1.5), eye[1] + rng.uniform(-0.5, 1.0), eye[2] + rng.uniform(-1.0, 1.0))
+    target = (target[0] + rng.uniform(-0.5, 0.5), target[1] + rng.uniform(-0.3, 0.3),
+              target[2] + rng.uniform(-0.5, 0.5))
+    return eye, target, up, fov

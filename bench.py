@@ -65,15 +65,47 @@ def parse_args():
                         "served: Poisson request streams over 16 resident scenes")
     p.add_argument("--rates", default="10,50,100,200,500", help="served: arrival rates (requests/s) to sweep")
     p.add_argument("--requests", type=int, default=96, help="served: requests per rate")
+    p.add_argument("--no-forms", action="store_true",
+                   help="trefoil: skip the wavefront frame and the 64-job batched comparison in the line")
     return p.parse_args()
 
 
-def run_served(args) -> None:
+def wavefront_frame(scene, flush, steps: int = 3) -> dict:
+    """The same frame rendered by the wavefront form (autotuned on it), timed
+    with CUDA events per step, L2 flushed between steps."""
+    import torch
+
+    import albedo_b200 as ab
+
+    job = ab.RenderJob(WIDTH, HEIGHT, samples_per_axis=SAMPLES_PER_AXIS, seed=SEED, max_depth=MAX_DEPTH,
+                       roulette_start=ROULETTE_START, method=ab.WAVEFRONT)
+    accum = torch.zeros((WIDTH * HEIGHT, 4), dtype=torch.float64, device="cuda")
+    shape = ab.autotune_batch([(scene, job, accum.data_ptr())])
+    ab.render_device(scene, job, accum.data_ptr())
+    torch.cuda.synchronize()
+    ms = []
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        ab.render_device(scene, job, accum.data_ptr())
+        end.record()
+        end.synchronize()
+        ms.append(start.elapsed_time(end))
+    scene.check()
+    s = statistics.mean(ms) / 1e3
+    return {"mpaths_per_s": PATHS_PER_STEP / s / 1e6, "mrays_per_s": ab.wavefront_last_rays() / s / 1e6,
+            "ms_per_step": s * 1e3, "steps": steps, "iterations": ab.wavefront_last_iterations(), "autotune": shape}
+
+
+def served_figures(rates: list[float], requests: int) -> list[dict]:
     """Poisson request streams (seeded) drawn from the batched-job distribution
-    over 16 resident scenes, served under a 150 GB device budget: the
-    continuous-batching server against the plain megakernel serving one request
-    at a time in arrival order. Latency is completion minus arrival; throughput
-    is paths over the time from the first arrival to the last completion."""
+    over 16 resident scenes, each request with its own seeded camera around its
+    scene's, served under a 150 GB device budget: the continuous-batching server
+    against the plain megakernel serving one request at a time in arrival order.
+    Both use autotuned shapes (tuned before the streams start). Latency is
+    completion minus arrival (wall clock); throughput is paths over the time from
+    the first arrival to the last completion."""
     import torch
 
     import albedo_b200 as ab
@@ -82,32 +114,36 @@ def run_served(args) -> None:
     tmp = tempfile.TemporaryDirectory()
     pool = scenes.batch_jobs(Path(tmp.name), count=16, scenes=16)
     loaded = [ab.Scene.load(j.scene) for j in pool]
-    # Warm-up: module load, kernel attributes and one graph capture per form.
-    warm = torch.zeros((128 * 72, 4), dtype=torch.float64, device="cuda")
-    for scene in loaded:
-        ab.render_device(scene, ab.RenderJob(128, 72, samples_per_axis=1, max_depth=8), warm.data_ptr())
-    server = ab.Server(memory_budget_bytes=150 << 30, slots=1 << 20)
-    server.submit(loaded[0], ab.RenderJob(128, 72, samples_per_axis=1, max_depth=8, method=ab.WAVEFRONT),
-                  warm.data_ptr())
-    while server.pending() != (0, 0):
-        server.step()
-    server.close()
-    torch.cuda.synchronize()
+    base_views = [scenes.scene_camera(j.scene) for j in pool]
+    # Tuning (and warm-up): the megakernel per scene on its pool job, the
+    # wavefront on the pool's jobs as one batch.
+    tune_start = time.perf_counter()
+    warm = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for j in pool]
+    for scene, j in zip(loaded, pool):
+        ab.autotune_megakernel(scene, ab.RenderJob(j.width, j.height, samples_per_axis=j.samples_per_axis,
+                                                   max_depth=8))
+    wave_shape = ab.autotune_batch([(scene, ab.RenderJob(j.width, j.height, samples_per_axis=j.samples_per_axis,
+                                                         max_depth=8, method=ab.WAVEFRONT), a.data_ptr())
+                                    for scene, j, a in zip(loaded, pool, warm)])
+    tune_s = time.perf_counter() - tune_start
+    del warm
     rng = np.random.default_rng(2024)
     results = []
-    for rate in [float(r) for r in args.rates.split(",")]:
-        gaps = rng.exponential(1.0 / rate, size=args.requests)
+    for rate in rates:
+        gaps = rng.exponential(1.0 / rate, size=requests)
         arrivals = np.cumsum(gaps) - gaps[0]
         reqs = []
-        for k in range(args.requests):
+        for k in range(requests):
             w, h = scenes.RESOLUTIONS[int(rng.integers(0, 4))]
             n = int(np.clip(round(np.sqrt(np.exp(rng.uniform(np.log(4), np.log(64))))), 2, 8))
-            reqs.append((int(rng.integers(0, 16)), w, h, n, k))
-        paths = sum(w * h * n * n for _, w, h, n, _ in reqs)
-        accs = [torch.zeros((w * h, 4), dtype=torch.float64, device="cuda") for _, w, h, _, _ in reqs]
+            sid = int(rng.integers(0, 16))
+            view = ab.Camera(*scenes.request_view(base_views[sid], rng))
+            reqs.append((sid, w, h, n, k, view))
+        paths = sum(w * h * n * n for _, w, h, n, _, _ in reqs)
+        accs = [torch.zeros((w * h, 4), dtype=torch.float64, device="cuda") for _, w, h, _, _, _ in reqs]
 
         def job(r, method):
-            _, w, h, n, seed = r
+            _, w, h, n, seed, _ = r
             return ab.RenderJob(w, h, samples_per_axis=n, seed=seed, max_depth=8, method=method)
 
         # Continuous batching.
@@ -115,18 +151,24 @@ def run_served(args) -> None:
         done_at = {}
         ticket_of = {}
         submitted = 0
+        rays = 0
+        last_rays = 0
         torch.cuda.synchronize()
         start = time.perf_counter()
         while len(done_at) < len(reqs):
             now = time.perf_counter() - start
             while submitted < len(reqs) and arrivals[submitted] <= now:
                 r = reqs[submitted]
-                ticket_of[server.submit(loaded[r[0]], job(r, ab.WAVEFRONT), accs[submitted].data_ptr())] = submitted
+                ticket = server.submit(loaded[r[0]], job(r, ab.WAVEFRONT), accs[submitted].data_ptr(), camera=r[5])
+                ticket_of[ticket] = submitted
                 submitted += 1
             finished = server.step()
             now = time.perf_counter() - start
             for t in finished:
                 done_at[ticket_of[t]] = now
+            count = server.rays()
+            rays += count - last_rays if count >= last_rays else count
+            last_rays = count
             waiting, running = server.pending()
             if waiting == 0 and running == 0 and submitted < len(reqs):
                 time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - start)))
@@ -142,43 +184,55 @@ def run_served(args) -> None:
             now = time.perf_counter() - start
             if now < arrivals[k]:
                 time.sleep(arrivals[k] - now)
-            ab.render_device(loaded[r[0]], job(r, ab.MEGAKERNEL), accs[k].data_ptr())
+            ab.render_device(loaded[r[0]], job(r, ab.MEGAKERNEL), accs[k].data_ptr(), camera=r[5])
             torch.cuda.synchronize()
             finish.append(time.perf_counter() - start)
         lat_mega = np.array(finish) - arrivals
         span_mega = finish[-1] - arrivals[0]
         results.append({
             "rate_per_s": rate, "requests": len(reqs), "paths": paths,
-            "server": {"mpaths_per_s": paths / span_server / 1e6, "p50_ms": float(np.percentile(lat_server, 50) * 1e3),
+            "server": {"mpaths_per_s": paths / span_server / 1e6, "mrays_per_s": rays / span_server / 1e6,
+                       "p50_ms": float(np.percentile(lat_server, 50) * 1e3),
                        "p99_ms": float(np.percentile(lat_server, 99) * 1e3)},
             "megakernel_one_at_a_time": {"mpaths_per_s": paths / span_mega / 1e6,
                                          "p50_ms": float(np.percentile(lat_mega, 50) * 1e3),
-                                         "p99_ms": float(np.percentile(lat_mega, 99) * 1e3)}})
+                                         "p99_ms": float(np.percentile(lat_mega, 99) * 1e3)},
+            "speedup_over_megakernel": span_mega / span_server})
     for s in loaded:
         s.check()
+    return [{"autotune": {"seconds": tune_s, "wavefront": wave_shape}}] + results
+
+
+def run_served(args) -> None:
+    """The served form as its own bench line: value is the server's best Mpaths/s
+    over the swept arrival rates (see served_figures)."""
+    with ClockSampler(0) as clocks:
+        figures = served_figures([float(r) for r in args.rates.split(",")], args.requests)
+    tuning, results = figures[0], figures[1:]
     best = max(r["server"]["mpaths_per_s"] for r in results)
     line = {"metric": METRIC, "value": best, "unit": "Mpaths/s", "n_gpus": 1, "steps": len(results), "warmup": 0,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded scene files, seeded Poisson arrivals)",
+            "data": "synthetic (seeded scene files, seeded Poisson arrivals and cameras)",
             "config": {"workload": "served_poisson_16_scenes", "budget_bytes": 150 << 30, "slots": 1 << 20,
                        "max_depth": 8, "timing": "wall clock from arrival to observed completion"},
-            "sweep": results}
+            "autotune": tuning["autotune"], "sweep": results, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args) -> None:
-    """64 seeded jobs of uneven size (displaced icospheres of 1k-500k triangles,
-    0-8 spheres, mixed materials, 128x72..1024x576, 4-64 spp), one scene each:
-    the plain megakernel serving them one at a time (a synchronize after each)
-    against one batched wavefront run of all of them. Each step renders every job
-    once; value is the batched form's Mpaths/s."""
+def batched_figures(steps: int, warmup: int, count: int = 64) -> dict:
+    """`count` seeded jobs of uneven size (displaced icospheres of 1k-500k
+    triangles, 0-8 spheres, mixed materials, 128x72..1024x576, 4-64 spp), one
+    scene each: one batched wavefront run of all of them against the plain
+    megakernel serving them one at a time (a synchronize after each). Both forms
+    run with the shapes the autotuner picked (per scene for the megakernel, for
+    the batch for the wavefront); tuning is outside the timed region."""
     import torch
 
     import albedo_b200 as ab
     from albedo_b200 import scenes
 
     tmp = tempfile.TemporaryDirectory()
-    jobs = scenes.batch_jobs(Path(tmp.name), count=64)
+    jobs = scenes.batch_jobs(Path(tmp.name), count=count)
     loaded = {j.scene: ab.Scene.load(j.scene) for j in jobs}
     paths = sum(j.width * j.height * j.samples_per_axis ** 2 for j in jobs)
     accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for j in jobs]
@@ -187,20 +241,28 @@ def run_batched(args) -> None:
         return ab.RenderJob(j.width, j.height, samples_per_axis=j.samples_per_axis, seed=j.seed, max_depth=8,
                             method=method)
 
+    items = [(loaded[j.scene], rjob(j, ab.WAVEFRONT), a.data_ptr()) for j, a in zip(jobs, accs)]
+    tune_start = time.perf_counter()
+    mega_shapes = [ab.autotune_megakernel(loaded[j.scene], rjob(j, ab.MEGAKERNEL)) for j in jobs]
+    wave_shape = ab.autotune_batch(items)
+    tune_s = time.perf_counter() - tune_start
+    counts = [ab.work_counts(loaded[j.scene], rjob(j, ab.MEGAKERNEL)) for j in jobs]
+    alg_bytes = sum(ab.algorithmic_bytes(c) for c in counts)
+
     def one_at_a_time():
         for j, a in zip(jobs, accs):
             ab.render_device(loaded[j.scene], rjob(j, ab.MEGAKERNEL), a.data_ptr())
             torch.cuda.synchronize()
 
     def batched():
-        ab.render_batch([(loaded[j.scene], rjob(j, ab.WAVEFRONT), a.data_ptr()) for j, a in zip(jobs, accs)])
+        ab.render_batch(items)
         torch.cuda.synchronize()
 
     def timed(fn):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         ms = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             torch.cuda.synchronize()
             start = time.perf_counter()
             fn()
@@ -209,21 +271,44 @@ def run_batched(args) -> None:
 
     with ClockSampler(0) as clocks:
         batch_ms = timed(batched)
+        rays = ab.wavefront_last_rays()
         mega_ms = timed(one_at_a_time)
     for s in loaded.values():
         s.check()
-    value = paths * args.steps / (sum(batch_ms) / 1e3) / 1e6
-    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": statistics.mean(batch_ms), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene files)",
-            "config": {"workload": "batched_64_jobs_mixed", "jobs": len(jobs), "paths_per_step": paths,
-                       "max_depth": 8, "method": "wavefront batch (one run for all jobs)",
-                       "jobs_detail": [[j.width, j.height, j.samples_per_axis ** 2] for j in jobs]},
-            "megakernel_one_at_a_time": {"value": paths * args.steps / (sum(mega_ms) / 1e3) / 1e6,
-                                         "unit": "Mpaths/s", "ms_per_step": statistics.mean(mega_ms)},
-            "wavefront_iterations": ab.wavefront_last_iterations(),
-            "timing": "wall clock around each step, device synchronized on both sides",
-            "clocks": clocks.summary()}
+    batch_s = statistics.mean(batch_ms) / 1e3
+    mega_s = statistics.mean(mega_ms) / 1e3
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    tiles = {}
+    for shape in mega_shapes:
+        key = f"{shape['tile_width']}x{128 // shape['tile_width']}/{shape['blocks_per_sm']}"
+        tiles[key] = tiles.get(key, 0) + 1
+    return {
+        "jobs": len(jobs), "paths_per_step": paths,
+        "wavefront": {"mpaths_per_s": paths / batch_s / 1e6, "mrays_per_s": rays / batch_s / 1e6,
+                      "ms_per_step": batch_s * 1e3, "rays_per_step": rays,
+                      "traversal_gbs": alg_bytes / batch_s / 1e9, "traversal_frac_of_hbm": alg_bytes / batch_s / 1e9 / peak,
+                      "iterations": ab.wavefront_last_iterations()},
+        "megakernel_one_at_a_time": {"mpaths_per_s": paths / mega_s / 1e6, "ms_per_step": mega_s * 1e3},
+        "speedup_over_megakernel": mega_s / batch_s,
+        "autotune": {"seconds": tune_s, "wavefront": wave_shape, "megakernel_shapes": tiles},
+        "algorithmic_bytes_per_step": alg_bytes,
+        "timing": "wall clock around each step, device synchronized on both sides",
+        "clocks": clocks.summary(),
+        "jobs_detail": [[j.width, j.height, j.samples_per_axis ** 2] for j in jobs],
+    }
+
+
+def run_batched(args) -> None:
+    """The batched form as its own bench line: value is the batched wavefront's
+    Mpaths/s over 64 seeded jobs (see batched_figures)."""
+    fig = batched_figures(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": fig["wavefront"]["mpaths_per_s"], "unit": "Mpaths/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": fig["wavefront"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene files)",
+            "config": {"workload": "batched_64_jobs_mixed", "max_depth": 8,
+                       "method": "wavefront batch (one run for all jobs), autotuned"},
+            "batched": fig, "clocks": fig["clocks"]}
     print(json.dumps(line), flush=True)
 
 
@@ -411,6 +496,11 @@ def main():
                        roulette_start=ROULETTE_START, method=method)
     accum = torch.zeros((WIDTH * HEIGHT, 4), dtype=torch.float64, device="cuda")
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    # Launch shape from the autotuner (untimed; renders into scratch accumulators).
+    if method == ab.MEGAKERNEL:
+        tuned = ab.autotune_megakernel(scene, job)
+    else:
+        tuned = ab.autotune_batch([(scene, job, accum.data_ptr())])
 
     for _ in range(args.warmup):
         ab.render_device(scene, job, accum.data_ptr())
@@ -481,13 +571,18 @@ def main():
                     "d2h_bytes_per_step": frame_bytes},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "megakernel<32, path>", "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel": f"megakernel<{scene.info()['stack_capacity']}, path>",
+                         "algorithmic_bytes_per_launch": alg_bytes,
                          "work_per_launch": counts, "peak_source": peak_source,
                          "traffic_source": traffic_source},
             "clocks": clocks.summary(),
+            "autotune": tuned,
         }
         if world == 1:
             line["cpu_baseline"] = cpu_baseline_sample(scene_path)
+            if not args.no_forms:
+                line["forms"] = {"wavefront_frame": wavefront_frame(scene, flush),
+                                 "batched_64_jobs": batched_figures(1, 1)}
         print(json.dumps(line), flush=True)
     scene.close()
     if dist is not None:

@@ -70,6 +70,13 @@ typedef enum albedo_method {
     ALBEDO_WAVEFRONT = 1   /* path slots advanced bounce by bounce through compacted queues */
 } albedo_method;
 
+/* How the megakernel sums a pixel's samples before adding them to the FP64
+ * accumulators. The reference sums in FP64 (render/render_image.cpp:27-44). */
+typedef enum albedo_accumulation {
+    ALBEDO_ACCUMULATE_FP64 = 0,      /* FP64 running sums (all methods) */
+    ALBEDO_ACCUMULATE_KAHAN_FP32 = 1 /* FP32 with Kahan compensation (megakernel, path estimator) */
+} albedo_accumulation;
+
 /* RenderJob (src/albedo/render/render_image.hpp:17-32) minus the camera and scene. */
 typedef struct albedo_render_job {
     int32_t width;
@@ -80,8 +87,18 @@ typedef struct albedo_render_job {
     int32_t max_depth;        /* PathEstimator::max_depth (default 64) */
     int32_t roulette_start;   /* PathEstimator::roulette_start (default 3) */
     int32_t method;           /* albedo_method */
-    int32_t reserved;
+    int32_t accumulation;     /* albedo_accumulation */
 } albedo_render_job;
+
+/* A view for one render in place of the scene's camera: CameraSettings
+ * (src/albedo/camera/perspective_camera.hpp:13-26), validated as the
+ * PerspectiveCamera constructor does. */
+typedef struct albedo_camera {
+    double look_from[3];
+    double look_at[3];
+    double up[3];
+    double vertical_fov_degrees;
+} albedo_camera;
 
 /* BasicMaterial: kind 0 diffuse (texture 0 constant color a, 1 checker even a /
  * odd b / frequency, 2 Perlin low a / high b / scale / veins), kind 1 conductor
@@ -167,6 +184,12 @@ int albedo_scene_get_info(const albedo_scene* scene, albedo_scene_info* out);
 int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
                   void* stream);
 int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators);
+/* albedo_render from the given camera instead of the scene's (NULL: the
+ * scene's). The reference builds one PerspectiveCamera per render from the
+ * settings it is given (app/main.cpp); this is that call with a per-request
+ * camera on a resident scene. */
+int albedo_render_view(const albedo_scene* scene, const albedo_render_job* job, const albedo_camera* camera,
+                       albedo_accumulator* accumulators, void* stream);
 /* Renders only the listed pixels (x, y pairs) into one host accumulator each,
  * optionally also returning per-pixel sums of squared samples (3 doubles each). */
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
@@ -217,6 +240,9 @@ int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo
  * fits. The ticket identifies it in albedo_server_step's results. */
 int albedo_server_submit(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
                          albedo_accumulator* accumulators, int64_t* out_ticket);
+/* albedo_server_submit with the request's own camera (NULL: the scene's). */
+int albedo_server_submit_view(albedo_server* server, const albedo_scene* scene, const albedo_render_job* job,
+                              const albedo_camera* camera, albedo_accumulator* accumulators, int64_t* out_ticket);
 /* Advances the device by one graph of iterations and reports (up to `capacity`)
  * tickets whose accumulators are now complete; tickets beyond `capacity` are
  * reported by later calls. */
@@ -226,8 +252,43 @@ void albedo_server_destroy(albedo_server* server);
 /* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
  * iterations per captured CUDA graph (the autotuner's knobs). */
 int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph);
+/* Autotuner. No counterpart in the reference (a CPU renderer with no launch
+ * shapes). Candidate launch shapes are timed with CUDA events on the caller's
+ * work rendered at a quarter of its samples (samples per axis halved) into
+ * scratch accumulators; the caller's accumulators are not touched. The fastest
+ * shape is kept and used by later renders: per scene for the megakernel, by the
+ * process's wavefront engine and servers created afterwards for batches.
+ * Images do not depend on the shape. Synchronous. */
+typedef struct albedo_tuning {
+    int32_t tile_width;           /* megakernel: pixel tile width (8, 16 or 32; 128-pixel tiles) */
+    int32_t blocks_per_sm;        /* megakernel: register budget (3 or 4 resident blocks per SM);
+                                     wavefront: blocks per SM of the queue kernels */
+    int32_t trace_blocks_per_sm;  /* wavefront: persistent traversal blocks per SM */
+    int32_t fetch_batch;          /* wavefront: queue entries a traversal warp claims at once */
+    int32_t iterations_per_graph; /* wavefront: iterations per captured CUDA graph */
+    int32_t slot_count;           /* wavefront: path slots */
+    int32_t evaluations;          /* shapes timed */
+    int32_t reserved;
+    double best_ms;               /* the kept shape's time on the tuning work */
+    double default_ms;            /* the default shape's time on the same work */
+} albedo_tuning;
+/* Tunes the megakernel for `scene` (tile width x register budget, every
+ * combination) on `job` and keeps the result in the scene. */
+int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
+/* Tunes the wavefront engine on a batch (coordinate descent over traversal
+ * blocks per SM, fetch batch, queue-kernel blocks per SM, iterations per graph
+ * and slot count) and keeps the result for the process. */
+int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_tuning* out);
+/* The shape renders use now: the scene's megakernel shape (scene not NULL) or
+ * the process's wavefront shape (scene NULL); timing fields are zero. */
+int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
 /* Iterations the last wavefront run took. */
 int albedo_wavefront_last_iterations(int64_t* out);
+/* Ray queries (closest hit plus shadow) the last wavefront run traced. */
+int albedo_wavefront_last_rays(int64_t* out);
+/* Ray queries the server's current batch has traced, as of the last step whose
+ * results were polled (the count restarts when the engine reopens a batch). */
+int albedo_server_rays(const albedo_server* server, int64_t* out);
 /* Renders the job once (path estimator, into scratch accumulators) while counting
  * traversal work: out_counts[0..4] = child boxes tested, triangles tested,
  * spheres tested, instances entered, ray queries traced. Synchronous. */
