@@ -1,11 +1,13 @@
 """Fixed render cases for profiling under ncu: one render, nothing else.
 
-    python -m albedo_b200.profiling megakernel --width 480 --height 270 --spp 64
-    python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16
+    python -m albedo_b200.profiling megakernel --width 480 --height 270 --spp 64 [--autotune]
+    python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16 [--autotune]
 
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene), max
-depth 10, seed 0. A warm-up render precedes the profiled one unless --no-warmup;
-pass `-k regex:<kernel> -s <skip>` to ncu to pick the launch.
+depth 10, seed 0. With --autotune the launch shape is tuned first (as bench.py
+does); a warm-up render precedes the profiled one unless --no-warmup. The case
+prints how many launches of the render kernels come before the profiled render,
+for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel).
 """
 
 from __future__ import annotations
@@ -15,6 +17,10 @@ import math
 import tempfile
 from pathlib import Path
 
+# Megakernel launches one tuning pass makes: every shape (3 tile widths x 2
+# register budgets) once untimed and twice timed.
+MEGAKERNEL_TUNING_LAUNCHES = 6 * 3
+
 
 def main() -> None:
     parser = argparse.ArgumentParser()
@@ -23,6 +29,7 @@ def main() -> None:
     parser.add_argument("--height", type=int, default=270)
     parser.add_argument("--spp", type=int, default=16)
     parser.add_argument("--no-warmup", action="store_true")
+    parser.add_argument("--autotune", action="store_true")
     args = parser.parse_args()
 
     import torch
@@ -36,12 +43,27 @@ def main() -> None:
         method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
         job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=10, method=method)
         acc = torch.zeros((args.width * args.height, 4), dtype=torch.float64, device="cuda")
-        for _ in range(1 if args.no_warmup else 2):
+        before = 0
+        shape = None
+        if args.autotune:
+            if method == ab.MEGAKERNEL:
+                shape = ab.autotune_megakernel(scene, job)
+                before += MEGAKERNEL_TUNING_LAUNCHES
+            else:
+                shape = ab.autotune_batch([(scene, job, acc.data_ptr())])
+        warmups = 0 if args.no_warmup else 1
+        for _ in range(warmups + 1):
             ab.render_device(scene, job, acc.data_ptr())
         torch.cuda.synchronize()
         scene.check()
-        counts = ab.work_counts(scene, job) if method == ab.MEGAKERNEL else None
-        print(f"rendered {args.width}x{args.height} at {n * n} spp ({args.method})", counts or "")
+        if method == ab.MEGAKERNEL:
+            before += warmups
+            counts = ab.work_counts(scene, job)
+            print(f"rendered {args.width}x{args.height} at {n * n} spp (megakernel); megakernel launches before the "
+                  f"profiled render: {before}; shape {ab.tuning(scene)}; work {counts}")
+        else:
+            print(f"rendered {args.width}x{args.height} at {n * n} spp (wavefront, {ab.wavefront_last_iterations()} "
+                  f"iterations, {ab.wavefront_last_rays()} rays per render); tuned shape {shape or ab.tuning()}")
         scene.close()
 
 
