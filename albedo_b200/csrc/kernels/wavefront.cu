@@ -16,6 +16,7 @@
 // in the same order as the megakernel (jitter, then per bounce 3 NEE, 3 BSDF,
 // 1 roulette), so each pixel's stream matches the reference's.
 #include "estimator.cuh"
+#include "fetch.cuh"
 #include "wavefront.cuh"
 
 namespace albedo_b200 {
@@ -59,54 +60,11 @@ ALB_DEV unsigned long long claimItem(unsigned long long* next, bool want)
     return want ? base + static_cast<unsigned long long>(__popc(mask & ((1u << lane) - 1u))) : ~0ull;
 }
 
-// Deals queue entries [0, count) to the lanes of a warp that need a ray, in
-// lane order; the warp claims `batch` entries at a time with one atomicAdd.
-// All 32 lanes call take() together.
-
 // Resident blocks per SM the traversal kernels' register budget is sized for.
 #ifndef ALBEDO_TRACE_BLOCKS_PER_SM
 #define ALBEDO_TRACE_BLOCKS_PER_SM 4
 #endif
 constexpr int kTraceBlocksPerSm = ALBEDO_TRACE_BLOCKS_PER_SM;
-
-struct WarpFetch {
-    int next;
-    int end;
-    int batch;
-    bool drained;
-
-    ALB_DEV int take(int* counter, int count, bool want)
-    {
-        const int lane = static_cast<int>(threadIdx.x & 31u);
-        const unsigned below = (1u << lane) - 1u;
-        unsigned need = __ballot_sync(0xFFFFFFFFu, want);
-        int got = -1;
-        while (need != 0u && !drained) {
-            if (next >= end) {
-                int base = 0;
-                if (lane == 0) {
-                    base = atomicAdd(counter, batch);
-                }
-                base = __shfl_sync(0xFFFFFFFFu, base, 0);
-                if (base >= count) {
-                    drained = true;
-                    break;
-                }
-                next = base;
-                end = base + batch < count ? base + batch : count;
-            }
-            const int avail = end - next;
-            const int rank = __popc(need & below);
-            if (((need >> lane) & 1u) != 0u && rank < avail) {
-                got = next + rank;
-            }
-            const int wanted = __popc(need);
-            next += wanted < avail ? wanted : avail;
-            need = __ballot_sync(0xFFFFFFFFu, want && got < 0);
-        }
-        return got;
-    }
-};
 
 ALB_DEV int findJob(const WfJob* jobs, int job_count, long long item)
 {
