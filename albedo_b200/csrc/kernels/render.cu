@@ -267,6 +267,11 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                                     accum, error_flag, no_totals);
         default:
             if (args.accumulation == kAccumulateKahan) {
+                if (args.blocks_per_sm == 4) {
+                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, 4, kAccumulateKahan>,
+                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
+                                            no_totals);
+                }
                 return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan>,
                                         megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
             }

@@ -60,9 +60,10 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--method", choices=["megakernel", "wavefront"], default="megakernel")
-    p.add_argument("--workload", choices=["trefoil", "batched", "served"], default="trefoil",
+    p.add_argument("--workload", choices=["trefoil", "batched", "served", "precision"], default="trefoil",
                    help="trefoil: the instanced-mesh frame (default); batched: 64 seeded jobs of uneven size; "
-                        "served: Poisson request streams over 16 resident scenes")
+                        "served: Poisson request streams over 16 resident scenes; precision: 1.31M- and "
+                        "1M-triangle meshes at 1920x1080, 256 spp, FP64 vs compensated FP32 sums")
     p.add_argument("--rates", default="10,50,100,200,500", help="served: arrival rates (requests/s) to sweep")
     p.add_argument("--requests", type=int, default=96, help="served: requests per rate")
     p.add_argument("--no-forms", action="store_true",
@@ -216,6 +217,98 @@ def run_served(args) -> None:
             "config": {"workload": "served_poisson_16_scenes", "budget_bytes": 150 << 30, "slots": 1 << 20,
                        "max_depth": 8, "timing": "wall clock from arrival to observed completion"},
             "autotune": tuning["autotune"], "sweep": results, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_precision(args) -> None:
+    """The precision form at full size: a displaced icosphere of 8 levels
+    (1,310,720 triangles) in rough glass and a 1,000,000-triangle random soup,
+    1920 x 1080 at 16 x 16 = 256 spp, PathEstimator max_depth 16. For each scene:
+    megakernel frames with FP64 and with Kahan-compensated FP32 per-pixel sums
+    (the same autotuned shape for both, CUDA events, L2 flushed between steps)
+    and a wavefront frame; the error of every image against the FP64 oracle (the
+    reference renderer at 65,536 spp on 256 seeded pixels, host cores) next to
+    the reference renderer's own error at 256 spp on the same pixels; and the
+    largest relative difference between the two accumulation modes."""
+    import torch
+
+    import albedo_b200 as ab
+    from albedo_b200 import scenes
+    from oracle import reference as ref
+
+    width, height, n, depth = 1920, 1080, 16, 16
+    paths = width * height * n * n
+    rng = np.random.default_rng(91)
+    pixels = np.stack([rng.integers(0, width, 256), rng.integers(0, height, 256)], axis=1).astype(np.int32)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    tmp = tempfile.TemporaryDirectory()
+    results = []
+    with ClockSampler(0) as clocks:
+        for name, make in (("icosphere_8_levels", scenes.icosphere_scene), ("soup_1M", scenes.soup_scene)):
+            path = make(Path(tmp.name) / name)
+            t0 = time.perf_counter()
+            scene = ab.Scene.load(path)
+            load_s = time.perf_counter() - t0
+            info = scene.info()
+            frames = {}
+            images = {}
+            for label, method, accumulation in (("megakernel_fp64", ab.MEGAKERNEL, ab.ACCUMULATE_FP64),
+                                                ("megakernel_kahan_fp32", ab.MEGAKERNEL, ab.ACCUMULATE_KAHAN_FP32),
+                                                ("wavefront_fp64", ab.WAVEFRONT, ab.ACCUMULATE_FP64)):
+                job = ab.RenderJob(width, height, samples_per_axis=n, seed=0, max_depth=depth, method=method,
+                                   accumulation=accumulation)
+                acc = torch.zeros((width * height, 4), dtype=torch.float64, device="cuda")
+                if label == "megakernel_fp64":
+                    ab.autotune_megakernel(scene, job)
+                elif method == ab.WAVEFRONT:
+                    ab.autotune_batch([(scene, job, acc.data_ptr())])
+                steps = args.steps if method == ab.MEGAKERNEL else 1
+                ms = []
+                for i in range(steps):
+                    acc.zero_()
+                    flush.fill_(i & 0xFF)
+                    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    start.record()
+                    ab.render_device(scene, job, acc.data_ptr())
+                    end.record()
+                    end.synchronize()
+                    ms.append(start.elapsed_time(end))
+                scene.check()
+                frames[label] = {"mpaths_per_s": paths / (statistics.mean(ms) / 1e3) / 1e6,
+                                 "ms_per_frame": statistics.mean(ms), "steps": steps}
+                images[label] = acc.cpu().numpy()
+            reference = ref.RefScene(path)
+            t0 = time.perf_counter()
+            oracle_sum, _ = reference.render_pixels(width, height, 256, pixels, seed=1000003, max_depth=depth)
+            oracle_s = time.perf_counter() - t0
+            oracle = oracle_sum / 65536.0
+            theirs_sum, _ = reference.render_pixels(width, height, n, pixels, seed=0, max_depth=depth)
+            lum = oracle.mean(axis=1)
+            keep = lum > 1e-3
+
+            def errors(rgb):
+                err = (rgb - oracle)[keep] / lum[keep, None]
+                return {"rel_rmse": float(np.sqrt(np.mean(err ** 2))), "mean_rel": float(np.mean(np.abs(err)))}
+
+            index = pixels[:, 1] * width + pixels[:, 0]
+            err = {label: errors(img[index, :3] / (n * n)) for label, img in images.items()}
+            err["reference_cpu_256spp"] = errors(theirs_sum / (n * n))
+            fp64, kahan = images["megakernel_fp64"][:, :3], images["megakernel_kahan_fp32"][:, :3]
+            lit = np.abs(fp64) > 1e-9
+            results.append({"scene": name, "triangles": info["triangles"], "bvh_nodes": info["nodes"],
+                            "device_bytes": info["device_bytes"], "load_s": load_s, "frames": frames,
+                            "error_vs_fp64_oracle": err,
+                            "oracle": {"pixels": 256, "spp": 65536, "seconds": oracle_s},
+                            "kahan_vs_fp64_max_rel": float(np.max(np.abs(kahan - fp64)[lit] / np.abs(fp64)[lit])),
+                            "tuned_megakernel": {k: ab.tuning(scene)[k] for k in ("tile_width", "blocks_per_sm")}})
+            scene.close()
+    value = statistics.mean(r["frames"]["megakernel_fp64"]["mpaths_per_s"] for r in results)
+    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps, "warmup": 0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded meshes written as OBJ)",
+            "config": {"workload": "precision_large_meshes_1920x1080_256spp", "max_depth": depth,
+                       "value": "mean over the two scenes of the FP64-accumulation megakernel"},
+            "scenes": results, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -467,6 +560,10 @@ def main():
     if args.workload == "served":
         if rank == 0:
             run_served(args)
+        return
+    if args.workload == "precision":
+        if rank == 0:
+            run_precision(args)
         return
 
     import torch
