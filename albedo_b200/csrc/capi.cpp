@@ -79,6 +79,9 @@ int guarded(F&& body)
     } catch (const Unsupported& e) {
         g_last_error = e.what();
         return ALBEDO_UNSUPPORTED;
+    } catch (const LayoutLimitError& e) {
+        g_last_error = e.what();
+        return ALBEDO_UNSUPPORTED;
     } catch (const TraversalError& e) {
         g_last_error = e.what();
         return ALBEDO_TRAVERSAL_ERROR;

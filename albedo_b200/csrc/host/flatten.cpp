@@ -270,6 +270,53 @@ bool needsWideSphere(const SphereDesc& s)
     return extent >= 256.0;
 }
 
+bool allFinite(const float* v, std::size_t n)
+{
+    for (std::size_t i{0}; i < n; ++i) {
+        if (!std::isfinite(v[i])) {
+            return false;
+        }
+    }
+    return true;
+}
+
+// The reference stores geometry in FP64; the device tables hold FP32, so a
+// value beyond FP32's range (about 3.4e38) would become infinite there.
+void checkFp32Range(const DeviceImage& image)
+{
+    const auto fail = [](const char* what, std::size_t index) {
+        throw LayoutLimitError{std::format("{} {} has a coordinate beyond the FP32 range of the device tables "
+                                           "(magnitude above 3.4e38)",
+                                           what, index)};
+    };
+    for (std::size_t i{0}; i < image.spheres.size(); ++i) {
+        const DevSphere& s{image.spheres[i]};
+        const float v[4]{s.cx, s.cy, s.cz, s.r};
+        if (!allFinite(v, 4)) {
+            fail("sphere", i);
+        }
+    }
+    for (std::size_t i{0}; i < image.triangles.size(); ++i) {
+        const DevTriangle& t{image.triangles[i]};
+        const float v[9]{t.v0x, t.v0y, t.v0z, t.v1x, t.v1y, t.v1z, t.v2x, t.v2y, t.v2z};
+        if (!allFinite(v, 9)) {
+            fail("triangle", i);
+        }
+    }
+    for (std::size_t i{0}; i < image.instances.size(); ++i) {
+        if (!allFinite(image.instances[i].to_object, 12) || !allFinite(image.instances[i].to_world, 12)) {
+            fail("instance", i);
+        }
+    }
+    for (std::size_t i{0}; i < image.lights.size(); ++i) {
+        const DevLight& l{image.lights[i]};
+        const float v[4]{l.p[0], l.p[1], l.p[2], l.radius};
+        if (!allFinite(v, 4)) {
+            fail("light", i);
+        }
+    }
+}
+
 } // namespace
 
 DeviceImage flattenScene(const HostScene& scene)
@@ -383,6 +430,7 @@ DeviceImage flattenScene(const HostScene& scene)
         image.lights.push_back(d);
     }
     image.sky_light = scene.sky_light;
+    checkFp32Range(image);
     return image;
 }
 
@@ -404,6 +452,10 @@ DevCamera deviceCamera(const CameraSettings& settings, int width, int height)
     put(cam.forward, frame.forward);
     put(cam.half_width, frame.half_width);
     put(cam.half_height, frame.half_height);
+    if (!allFinite(cam.origin, 3) || !allFinite(cam.forward, 3) || !allFinite(cam.half_width, 3) ||
+        !allFinite(cam.half_height, 3)) {
+        throw LayoutLimitError{"the camera has a coordinate beyond the FP32 range of the device"};
+    }
     return cam;
 }
 

@@ -4,9 +4,18 @@
 #include "../device_layout.hpp"
 #include "host_scene.hpp"
 
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace albedo_b200 {
+
+// A scene the device tables cannot hold as given (FP32 range), though the
+// reference, which works in FP64, accepts it.
+class LayoutLimitError : public std::runtime_error {
+public:
+    explicit LayoutLimitError(const std::string& what) : std::runtime_error{what} {}
+};
 
 struct DeviceImage {
     std::vector<DevNode> nodes;
@@ -29,10 +38,12 @@ struct DeviceImage {
 };
 
 // Throws std::invalid_argument if the scene exceeds the device layout's limits
-// (leaf positions must fit 28 bits).
+// (leaf positions must fit 28 bits), and LayoutLimitError if a coordinate of
+// its geometry, instance maps or lights is beyond FP32's range.
 DeviceImage flattenScene(const HostScene& scene);
 
-// The camera frame for an image of the given size, rounded to FP32.
+// The camera frame for an image of the given size, rounded to FP32 (throws
+// LayoutLimitError if it leaves FP32's range).
 DevCamera deviceCamera(const HostScene& scene, int width, int height);
 DevCamera deviceCamera(const CameraSettings& settings, int width, int height);
 

@@ -91,3 +91,20 @@ def test_builder_rejects_what_the_reference_rejects():
         scene.add_mesh([[0, 0, 0], [1, 0, 0], [0, 1, 0]], [[0, 1, 5]])
     with pytest.raises(ValueError, match="at least one triangle"):
         scene.add_mesh([[0, 0, 0], [1, 0, 0], [2, 0, 0]], [[0, 1, 2]])
+
+
+def test_geometry_beyond_fp32_range_is_refused_not_rendered_wrong():
+    # The reference (FP64) accepts a sphere at 1e300; the device tables are FP32,
+    # so preparing the scene reports ALBEDO_UNSUPPORTED instead of storing inf.
+    scene = ab.Scene.create()
+    white = scene.add_material(ab.BasicMaterial(a=(0.5, 0.5, 0.5)))
+    scene.set_camera((0, 0, 5), (0, 0, 0))
+    scene.add_sphere((0, 0, 0), 1.0, white)
+    scene.add_sphere((1e300, 0, 0), 1.0, white)
+    with pytest.raises(ab.Unsupported, match="sphere 1 has a coordinate beyond the FP32 range"):
+        scene.prepare()
+    huge_but_finite = ab.Scene.create()
+    white = huge_but_finite.add_material(ab.BasicMaterial(a=(0.5, 0.5, 0.5)))
+    huge_but_finite.set_camera((0, 0, 5), (0, 0, 0))
+    huge_but_finite.add_sphere((1e30, 0, 0), 1e29, white)
+    huge_but_finite.prepare()
