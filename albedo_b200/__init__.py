@@ -379,6 +379,18 @@ def autotune_batch(items) -> dict:
     return _tuning_dict(out)
 
 
+def set_tuning(scene: Scene | None = None, **shape) -> None:
+    """Pins a launch shape: tile_width and blocks_per_sm for a scene's megakernel,
+    or (no scene) blocks_per_sm, trace_blocks_per_sm, fetch_batch,
+    iterations_per_graph and slot_count for the wavefront engine."""
+    t = TuningC()
+    for k, v in shape.items():
+        if k not in _TUNING_FIELDS[:6]:
+            raise ValueError(f"unknown shape field {k}")
+        setattr(t, k, int(v))
+    _raise(library().albedo_tuning_set(None if scene is None else scene.handle, byref(t)))
+
+
 def tuning(scene: Scene | None = None) -> dict:
     """The shape renders use now: the scene's megakernel shape, or (no scene) the wavefront engine's."""
     out = TuningC()
@@ -479,5 +491,5 @@ __all__ = [
     "ACCUMULATE_FP64", "ACCUMULATE_KAHAN_FP32", "ACCUMULATOR_DTYPE", "BasicMaterial", "Camera", "DeviceError",
     "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
     "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
-    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "tuning", "wavefront_last_rays",
+    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "set_tuning", "tuning", "wavefront_last_rays",
 ]

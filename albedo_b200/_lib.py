@@ -93,6 +93,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_autotune_megakernel": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(TuningC)]),
     "albedo_autotune_batch": (c_int32, [c_void_p, c_int32, POINTER(TuningC)]),
     "albedo_tuning_get": (c_int32, [c_void_p, POINTER(TuningC)]),
+    "albedo_tuning_set": (c_int32, [c_void_p, POINTER(TuningC)]),
     "albedo_wavefront_last_iterations": (c_int32, [POINTER(c_int64)]),
     "albedo_wavefront_last_rays": (c_int32, [POINTER(c_int64)]),
     "albedo_server_rays": (c_int32, [c_void_p, POINTER(c_int64)]),

@@ -365,6 +365,7 @@ void configureEngine(int slots, int blocks_per_sm, int iterations_per_graph)
         g_engine.reset();
     }
     g_engine_slots = slots;
+    g_engine_shape = WfShape{};
     g_engine_shape.blocks_per_sm = blocks_per_sm;
     g_engine_shape.iterations_per_graph = iterations_per_graph;
 }
@@ -971,6 +972,40 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         out->iterations_per_graph = outcome.best[3];
         out->slot_count = outcome.best[4];
         fillTuning(out, outcome);
+    });
+}
+
+int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
+{
+    return guarded([&] {
+        if (scene != nullptr) {
+            if (shape->tile_width != 8 && shape->tile_width != 16 && shape->tile_width != 32) {
+                throw std::invalid_argument{std::format("megakernel tile width must be 8, 16 or 32, got {}",
+                                                        shape->tile_width)};
+            }
+            if (shape->blocks_per_sm != 3 && shape->blocks_per_sm != 4) {
+                throw std::invalid_argument{std::format("megakernel blocks per SM must be 3 or 4, got {}",
+                                                        shape->blocks_per_sm)};
+            }
+            scene->mega_tile_width = shape->tile_width;
+            scene->mega_blocks_per_sm = shape->blocks_per_sm;
+            return;
+        }
+        if (shape->blocks_per_sm <= 0 || shape->trace_blocks_per_sm <= 0 || shape->fetch_batch <= 0 ||
+            shape->iterations_per_graph <= 0 || shape->slot_count <= 0) {
+            throw std::invalid_argument{"wavefront shape values must be positive"};
+        }
+        WfShape next{};
+        next.blocks_per_sm = shape->blocks_per_sm;
+        next.trace_blocks_per_sm = shape->trace_blocks_per_sm;
+        next.fetch_batch = shape->fetch_batch;
+        next.iterations_per_graph = shape->iterations_per_graph;
+        const std::lock_guard lock{g_engine_mutex};
+        if (g_engine && g_engine->slotCount() != shape->slot_count) {
+            g_engine.reset();
+        }
+        g_engine_slots = shape->slot_count;
+        g_engine_shape = next;
     });
 }
 

@@ -1,6 +1,7 @@
 """Fixed render cases for profiling under ncu: one render, nothing else.
 
     python -m albedo_b200.profiling megakernel --width 480 --height 270 --spp 64 [--autotune]
+                                   [--accumulation fp64|kahan]
     python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16 [--autotune]
 
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene), max
@@ -30,6 +31,8 @@ def main() -> None:
     parser.add_argument("--spp", type=int, default=16)
     parser.add_argument("--no-warmup", action="store_true")
     parser.add_argument("--autotune", action="store_true")
+    parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
+                        help="megakernel per-pixel sums: FP64 or Kahan-compensated FP32")
     args = parser.parse_args()
 
     import torch
@@ -41,7 +44,9 @@ def main() -> None:
     with tempfile.TemporaryDirectory() as tmp:
         scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
         method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
-        job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=10, method=method)
+        accumulation = ab.ACCUMULATE_KAHAN_FP32 if args.accumulation == "kahan" else ab.ACCUMULATE_FP64
+        job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=10, method=method,
+                           accumulation=accumulation)
         acc = torch.zeros((args.width * args.height, 4), dtype=torch.float64, device="cuda")
         before = 0
         shape = None

@@ -129,7 +129,7 @@ typedef struct albedo_scene_info {
     int64_t objects;
     int64_t lights;
     int64_t triangles;       /* scene triangles plus every mesh's triangles */
-    int64_t nodes;           /* device BVH nodes (child-box form) */
+    int64_t nodes;           /* device BVH nodes (4-wide form) */
     int64_t device_bytes;    /* device memory held by the committed scene */
     int32_t stack_need;      /* traversal stack entries a query can need */
     int32_t stack_capacity;  /* entries of the kernel variant chosen */
@@ -250,7 +250,8 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
 int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int32_t* out_running);
 void albedo_server_destroy(albedo_server* server);
 /* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
- * iterations per captured CUDA graph (the autotuner's knobs). */
+ * iterations per captured CUDA graph; the traversal kernels' blocks per SM and
+ * fetch batch return to their defaults (as many as fit, 32). */
 int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_t iterations_per_graph);
 /* Autotuner. No counterpart in the reference (a CPU renderer with no launch
  * shapes). Candidate launch shapes are timed with CUDA events on the caller's
@@ -282,6 +283,12 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
 /* The shape renders use now: the scene's megakernel shape (scene not NULL) or
  * the process's wavefront shape (scene NULL); timing fields are zero. */
 int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
+/* Pins a shape, as the autotuner would keep it: the scene's megakernel shape
+ * (scene not NULL: tile_width 8, 16 or 32 and blocks_per_sm 3 or 4) or the
+ * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
+ * fetch_batch, iterations_per_graph and slot_count, all positive). Timing fields
+ * are ignored. Images do not depend on the shape. */
+int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */
 int albedo_wavefront_last_iterations(int64_t* out);
 /* Ray queries (closest hit plus shadow) the last wavefront run traced. */

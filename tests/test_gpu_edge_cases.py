@@ -1,0 +1,340 @@
+"""Edge cases the reference's own tests pin, on the device path (GPU).
+
+Each case builds a scene file in the reference's grammar and compares the device
+with the reference library on the same file, or checks an exact property:
+
+  watertight triangles   rays aimed at shared edges and a shared vertex all hit
+                         (tests/geometry/triangle_test.cpp:291-335), identity and
+                         rotated instances
+  dominant axes          rays along and near all six axis directions hit a cube
+                         with the reference's t (triangle_test.cpp:268-289)
+  spheres                origins inside, rays grazing just inside and outside, a
+                         distant small sphere (sphere_test.cpp:139-250)
+  coincident boxes       identical spheres: the same object wins the tie as in the
+                         reference's visiting order (bvh_test.cpp:235-275); boxes
+                         of exponentially growing size
+  NaN slabs              axis-parallel rays whose origin lies on a box face
+                         (bvh_test.cpp:299-323)
+  instances              uniform, non-uniform and mirrored scaling: t in world
+                         units, normals, front faces (mesh_instance_test.cpp)
+  estimator              a point light over a plane and a mirror (deterministic
+                         paths: per pixel as the reference), a white furnace (mean 1),
+                         MIS against the scatter-only estimator
+                         (path_estimator_test.cpp:76-184, 208-233)
+  render loop            the same job twice gives the same image, and every launch
+                         shape of a kernel gives the same image bit for bit
+                         (render_image_test.cpp:169-187, 287-320)
+
+Query tolerance, as the ray-query parity test: identical hit flags and object
+ids, t within 2 FP32 ulps (all within 64 where a case allows a tie).
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import albedo_b200 as ab
+from albedo_b200 import scenes
+from oracle import reference as ref
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not ref.available(), reason="reference library not built")]
+
+MATERIALS = """\
+material white diffuse color 0.73 0.73 0.73
+material perfect diffuse color 1 1 1
+material mirror conductor eta 0.155 0.117 0.138  k 4.83 3.12 2.15  roughness 0
+material glass dielectric ior 1.5 roughness 0
+"""
+
+
+def write_scene(directory, lines, meshes=None, camera="camera from 0 0 6 at 0 0 0 up 0 1 0 fov 40"):
+    directory.mkdir(parents=True, exist_ok=True)
+    for name, (points, faces) in (meshes or {}).items():
+        scenes.write_obj(directory / f"{name}.obj", np.asarray(points, np.float32), np.asarray(faces))
+    path = directory / "case.scene"
+    path.write_text("\n".join([camera, MATERIALS] + lines) + "\n")
+    return path
+
+
+def ulps(ours_f32, reference_f64):
+    a = ours_f32.astype(np.float32).view(np.int32).astype(np.int64)
+    b = reference_f64.astype(np.float32).view(np.int32).astype(np.int64)
+    return np.abs(a - b)
+
+
+def queries(path, rays):
+    rays = np.asarray(rays, np.float32)
+    ours = ab.Scene.load(path).intersect(rays, geometry=True)
+    theirs = ref.RefScene(path).intersect(rays.astype(np.float64))
+    return ours, theirs
+
+
+def assert_queries_match(ours, theirs, max_ulps=2):
+    np.testing.assert_array_equal(ours["hit"], theirs["hit"])
+    hit = ours["hit"] == 1
+    np.testing.assert_array_equal(ours["object"][hit], theirs["object"][hit])
+    d = ulps(ours["t"][hit], theirs["t"][hit])
+    assert np.all(d <= max_ulps), (d.max(), np.argmax(d))
+    np.testing.assert_array_equal(ours["front"][hit], theirs["front"][hit])
+    dots = np.sum(ours["normal"][hit] * theirs["normal"][hit], axis=1)
+    assert np.all(dots > 0.9999), dots.min()
+
+
+def rays_at(origins, targets):
+    d = targets - origins
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([origins, d], axis=1).astype(np.float32)
+
+
+# A square of two triangles split along its diagonal, and a fan of 8 triangles
+# around the origin: the shared edges are the diagonal and the fan's spokes.
+SQUARE = ([[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]], [[0, 1, 2], [0, 2, 3]])
+FAN_POINTS = [[0, 0, 0]] + [[math.cos(2 * math.pi * k / 8) * 0.9, math.sin(2 * math.pi * k / 8) * 0.9, 0]
+                            for k in range(8)]
+FAN = (FAN_POINTS, [[0, 1 + k, 1 + (k + 1) % 8] for k in range(8)])
+
+
+@pytest.mark.parametrize("placement", ["", "rotate 1 1 0 37  translate 0.25 -0.5 0.125"])
+def test_shared_edges_and_vertices_leave_no_gaps(tmp_path, placement):
+    path = write_scene(tmp_path, [f"mesh square square.obj", f"mesh fan fan.obj",
+                                  f"instance square material white {placement}",
+                                  f"instance fan material white translate 3 0 0 {placement}"],
+                       meshes={"square": SQUARE, "fan": FAN})
+    rng = np.random.default_rng(3)
+    n = 4000
+    # Points on the square's diagonal and on the fan's spokes, in object space.
+    s = rng.uniform(0.02, 0.98, n)
+    diagonal = np.stack([-1 + 2 * s, -1 + 2 * s, np.zeros(n)], axis=1)
+    k = rng.integers(0, 8, n)
+    r = rng.uniform(0.02, 0.88, n)
+    spokes = np.stack([np.cos(2 * np.pi * k / 8) * r + 3, np.sin(2 * np.pi * k / 8) * r, np.zeros(n)], axis=1)
+    center = np.tile([[3.0, 0.0, 0.0]], (n, 1))
+    targets = np.concatenate([diagonal, spokes, center])
+    if placement:
+        # The placement's map: rotation about (1, 1, 0) by 37 degrees, then the
+        # translation; the fan's own translation comes first.
+        axis = np.array([1.0, 1.0, 0.0]) / math.sqrt(2)
+        a = math.radians(37)
+        kx = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+        rot = np.eye(3) + math.sin(a) * kx + (1 - math.cos(a)) * kx @ kx
+        targets = targets @ rot.T + np.array([0.25, -0.5, 0.125])
+    normal = np.array([0.0, 0.0, 1.0]) if not placement else rot @ np.array([0.0, 0.0, 1.0])
+    origins = targets + normal * rng.uniform(0.5, 3.0, (len(targets), 1)) + rng.normal(0, 0.3, targets.shape)
+    rays = rays_at(origins, targets)
+    ours, theirs = queries(path, rays)
+    assert ours["hit"].sum() == len(rays), len(rays) - ours["hit"].sum()
+    assert theirs["hit"].sum() == len(rays)
+
+
+def test_every_dominant_axis_and_sign(tmp_path):
+    corners = np.array([[x, y, z] for x in (-1.5, 1.5) for y in (-1.5, 1.5) for z in (-1.5, 1.5)])
+    faces = [[0, 1, 3], [0, 3, 2], [4, 6, 7], [4, 7, 5], [0, 4, 5], [0, 5, 1], [2, 3, 7], [2, 7, 6],
+             [0, 2, 6], [0, 6, 4], [1, 5, 7], [1, 7, 3]]
+    path = write_scene(tmp_path, ["mesh cube cube.obj", "instance cube material white"],
+                       meshes={"cube": (corners, faces)})
+    rng = np.random.default_rng(4)
+    dirs = []
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            exact = np.zeros(3)
+            exact[axis] = sign
+            tilted = exact + rng.normal(0, 0.2, (500, 3))
+            dirs += [exact[None, :], tilted]
+    d = np.concatenate(dirs)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = rng.uniform(-0.5, 0.5, (len(d), 3))
+    exact = [501 * g for g in range(6)]  # the six exactly axis-aligned rays, from the center
+    o[exact] = 0.0
+    rays = np.concatenate([o, d], axis=1).astype(np.float32)
+    ours, theirs = queries(path, rays)
+    assert ours["hit"].all()
+    assert_queries_match(ours, theirs)
+    np.testing.assert_array_equal(ours["t"][exact], np.float32(1.5))
+
+
+def test_sphere_origins_inside_grazing_and_far(tmp_path):
+    path = write_scene(tmp_path, ["sphere 0 0 0 radius 1 material white",
+                                  "sphere 0 0 -10000 radius 0.001 material white"])
+    rng = np.random.default_rng(5)
+    inside_o = rng.uniform(-0.5, 0.5, (2000, 3))
+    inside_d = rng.normal(size=(2000, 3))
+    inside_d /= np.linalg.norm(inside_d, axis=1, keepdims=True)
+    # Rays parallel to z passing at distance 1 -/+ 1e-3 from the axis of the unit sphere.
+    phi = rng.uniform(0, 2 * np.pi, 1000)
+    radius = np.where(np.arange(1000) % 2 == 0, 1 - 1e-3, 1 + 1e-3)
+    grazing_o = np.stack([np.cos(phi) * radius, np.sin(phi) * radius, np.full(1000, 5.0)], axis=1)
+    grazing_d = np.tile([[0.0, 0.0, -1.0]], (1000, 1))
+    # The distant small sphere, seen from (0, 0, -5) straight down -z; the unit
+    # sphere is behind the origin.
+    far_o = np.tile([[0.0, 0.0, -5.0]], (200, 1)) + np.concatenate(
+        [rng.uniform(-5e-4, 5e-4, (200, 2)), np.zeros((200, 1))], axis=1)
+    far_d = np.tile([[0.0, 0.0, -1.0]], (200, 1))
+    rays = np.concatenate([np.concatenate([inside_o, inside_d], 1), np.concatenate([grazing_o, grazing_d], 1),
+                           np.concatenate([far_o, far_d], 1)]).astype(np.float32)
+    ours, theirs = queries(path, rays)
+    assert ours["hit"][:2000].all()
+    assert (ours["hit"][2000:3000] == (np.arange(1000) % 2 == 0)).all()
+    assert ours["hit"][3000:].all() and (ours["object"][3000:] == 1).all()
+    assert_queries_match(ours, theirs)
+
+
+def test_coincident_and_exponential_boxes(tmp_path):
+    lines = [f"sphere 0.5 0.25 0 radius 0.75 material white" for _ in range(16)]
+    lines += [f"sphere {scenes.num(2.0 ** k)} -3 0 radius {scenes.num(2.0 ** (k - 2))} material white"
+              for k in range(-8, 9)]
+    path = write_scene(tmp_path, lines, camera="camera from 0 0 400 at 0 0 0 up 0 1 0 fov 40")
+    rng = np.random.default_rng(6)
+    targets = np.concatenate([rng.uniform([-0.3, -0.5, -0.5], [1.3, 1.0, 0.5], (3000, 3)),
+                              np.stack([2.0 ** rng.uniform(-8, 8, 3000), np.full(3000, -3.0),
+                                        np.zeros(3000)], axis=1)])
+    origins = targets + rng.normal(0, 1, targets.shape) * 4 + np.array([0, 0, 6])
+    ours, theirs = queries(path, rays_at(origins, targets))
+    assert ours["hit"][:3000].mean() > 0.5
+    assert_queries_match(ours, theirs)
+    # Ties among the coincident spheres go to the same object as in the reference.
+    tie = (ours["hit"] == 1) & (ours["object"] < 16)
+    assert tie.sum() > 1000
+    np.testing.assert_array_equal(ours["object"][tie], theirs["object"][tie])
+
+
+def test_axis_parallel_rays_on_box_faces(tmp_path):
+    # One triangle whose bounding box has the face x = 0; rays parallel to z
+    # with x = 0 exactly run inside that face (0 * inf = NaN in the slab test),
+    # and along the triangle's edge x = 0, which the watertight test counts as inside.
+    tri = ([[0, -1, 0], [2, -1, 0], [0, 1, 0]], [[0, 1, 2]])
+    path = write_scene(tmp_path, ["mesh tri tri.obj", "instance tri material white",
+                                  "sphere 0 3 0 radius 1 material white"], meshes={"tri": tri})
+    ys = np.linspace(-0.9, 0.9, 64)
+    on_face = np.stack([np.zeros(64), ys, np.full(64, 5.0), np.zeros(64), np.zeros(64), -np.ones(64)], axis=1)
+    # Rays along x on the plane y = 3 - 1 (the sphere's box face y = 2) and on y = 4.
+    xs = np.linspace(-0.5, 0.5, 32)
+    on_sphere_faces = np.concatenate([
+        np.stack([xs, np.full(32, 2.0), np.full(32, 5.0), np.zeros(32), np.zeros(32), -np.ones(32)], axis=1),
+        np.stack([np.full(32, -5.0), np.full(32, 4.0), xs, np.ones(32), np.zeros(32), np.zeros(32)], axis=1)])
+    rays = np.concatenate([on_face, on_sphere_faces]).astype(np.float32)
+    ours, theirs = queries(path, rays)
+    assert ours["hit"][:64].all()
+    assert_queries_match(ours, theirs)
+
+
+def test_scaled_nonuniform_and_mirrored_instances(tmp_path):
+    points, faces = scenes.icosphere(2)
+    path = write_scene(tmp_path, ["mesh ball ball.obj smooth",
+                                  "instance ball material white scale 2 translate -5 0 0",
+                                  "instance ball material white scale 1 3 0.5",
+                                  "instance ball material white scale -1 1 1 rotate 0 1 0 30 translate 5 0 0"],
+                       meshes={"ball": (points, faces)}, camera="camera from 0 0 20 at 0 0 0 up 0 1 0 fov 40")
+    rng = np.random.default_rng(8)
+    centers = np.array([[-5, 0, 0], [0, 0, 0], [5, 0, 0]])[rng.integers(0, 3, 6000)]
+    targets = centers + rng.normal(0, 0.8, (6000, 3))
+    origins = targets + rng.normal(0, 1, (6000, 3)) * 6
+    rays = rays_at(origins, targets)
+    ours, theirs = queries(path, rays)
+    assert ours["hit"].mean() > 0.3
+    assert_queries_match(ours, theirs)
+    assert set(np.unique(ours["object"][ours["hit"] == 1])) == {0, 1, 2}
+
+
+def render(scene, job):
+    acc = torch.zeros((job.width * job.height, 4), dtype=torch.float64, device="cuda")
+    ab.render_device(scene, job, acc.data_ptr())
+    torch.cuda.synchronize()
+    scene.check()
+    return acc.cpu().numpy()
+
+
+def reference_image(path, job):
+    pixels = np.stack(np.meshgrid(np.arange(job.width), np.arange(job.height)), axis=-1).reshape(-1, 2)
+    sums, squares = ref.RefScene(path).render_pixels(job.width, job.height, job.samples_per_axis, pixels,
+                                                     seed=job.seed, estimator=job.estimator,
+                                                     max_depth=job.max_depth, roulette_start=job.roulette_start)
+    return sums, squares
+
+
+FLOOR_CAMERA = "camera from 0 3 0.5 at 0 0 0.5 up 0 0 -1 fov 60"
+
+
+@pytest.mark.parametrize("method", [ab.MEGAKERNEL, ab.WAVEFRONT])
+def test_point_light_over_a_plane_is_deterministic_per_pixel(tmp_path, method):
+    scenes.write_floor(tmp_path / "floor.obj")
+    path = write_scene(tmp_path, ["mesh floor floor.obj", "instance floor material white",
+                                  "point_light 0 2 0.5 intensity 3 2 1"], camera=FLOOR_CAMERA)
+    job = ab.RenderJob(48, 48, samples_per_axis=2, seed=3, max_depth=8, method=method)
+    ours = render(ab.Scene.load(path), job)[:, :3]
+    theirs, _ = reference_image(path, job)
+    lit = theirs.sum(axis=1) > 0
+    assert lit.mean() > 0.99
+    rel = np.abs(ours - theirs)[lit] / theirs[lit]
+    assert np.max(rel) < 1e-4, np.max(rel)
+    # The pixel straight below the light: albedo / pi * I / h^2 per sample, near the
+    # image center (the jitter moves the hit point by at most half a pixel).
+    center = (24 * 48 + 24)
+    expected = 0.73 / math.pi * np.array([3, 2, 1]) / 4.0 * 4
+    np.testing.assert_allclose(ours[center], expected, rtol=0.01)
+
+
+@pytest.mark.parametrize("method", [ab.MEGAKERNEL, ab.WAVEFRONT])
+def test_mirror_reflects_the_light_exactly(tmp_path, method):
+    scenes.write_floor(tmp_path / "floor.obj")
+    path = write_scene(tmp_path, ["mesh floor floor.obj", "instance floor material mirror",
+                                  "area_light 0 2 0.5 radius 0.8 radiance 4 3 2"],
+                       camera="camera from 0 1 3 at 0 0 0 up 0 1 0 fov 60")
+    job = ab.RenderJob(64, 48, samples_per_axis=2, seed=5, max_depth=8, method=method)
+    ours = render(ab.Scene.load(path), job)[:, :3]
+    theirs, _ = reference_image(path, job)
+    lit = theirs.sum(axis=1) > 0
+    assert lit.mean() > 0.05
+    rel = np.abs(ours - theirs) / np.maximum(np.abs(theirs), 1e-6)
+    # Pixels whose jittered rays graze the light's silhouette may round the other way.
+    assert np.mean(rel.max(axis=1) > 1e-4) < 0.01, np.mean(rel.max(axis=1) > 1e-4)
+
+
+def test_white_furnace_averages_one(tmp_path):
+    path = write_scene(tmp_path, ["sphere 0 0 0 radius 1 material perfect", "sky 1 1 1"])
+    job = ab.RenderJob(64, 48, samples_per_axis=8, seed=9, max_depth=64)
+    scene = ab.Scene.load(path)
+    pixels = np.stack(np.meshgrid(np.arange(64), np.arange(48)), axis=-1).reshape(-1, 2).astype(np.int32)
+    acc, squares = ab.render_pixels(scene, job, pixels, with_squares=True)
+    s = 64
+    mean = np.stack([acc["r"], acc["g"], acc["b"]], axis=1) / s
+    var = np.maximum(squares / s - mean**2, 0)
+    total = mean.mean()
+    se = math.sqrt(var.mean() / (s * len(pixels)))
+    assert abs(total - 1.0) < 4 * se + 1e-6, (total, se)
+
+
+def test_mis_agrees_with_the_scatter_only_estimator(tmp_path):
+    scenes.write_floor(tmp_path / "floor.obj")
+    path = write_scene(tmp_path, ["mesh floor floor.obj", "instance floor material white",
+                                  "sphere 0 0.8 0 radius 0.8 material white",
+                                  "area_light 0 3 0 radius 0.6 radiance 6 6 6", "sky 0.3 0.35 0.4"],
+                       camera="camera from 0 2 5 at 0 0.5 0 up 0 1 0 fov 50")
+    scene = ab.Scene.load(path)
+    means = []
+    for estimator in (ab.PATH, ab.SCATTER_ONLY):
+        img = render(scene, ab.RenderJob(64, 36, samples_per_axis=16, seed=2, estimator=estimator, max_depth=16))
+        means.append(img[:, :3].sum() / (64 * 36 * 256))
+    assert abs(means[0] - means[1]) / means[1] < 0.03, means
+
+
+def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
+    scene = ab.Scene.load(trefoil_path)
+    job = ab.RenderJob(160, 90, samples_per_axis=3, seed=4, max_depth=10)
+    base = render(scene, job)
+    np.testing.assert_array_equal(render(scene, job), base)
+    for tile in (8, 32, 16):
+        ab.set_tuning(scene, tile_width=tile, blocks_per_sm=3)
+        np.testing.assert_array_equal(render(scene, job), base)
+    wave_job = ab.RenderJob(160, 90, samples_per_axis=3, seed=4, max_depth=10, method=ab.WAVEFRONT)
+    wave = render(scene, wave_job)
+    for shape in (dict(blocks_per_sm=4, trace_blocks_per_sm=2, fetch_batch=16, iterations_per_graph=2,
+                       slot_count=1 << 14),
+                  dict(blocks_per_sm=16, trace_blocks_per_sm=4, fetch_batch=128, iterations_per_graph=8,
+                       slot_count=1 << 20)):
+        ab.set_tuning(**shape)
+        np.testing.assert_array_equal(render(scene, wave_job), wave)
+    ab.wavefront_configure()
+    with pytest.raises(ValueError):
+        ab.set_tuning(scene, tile_width=12, blocks_per_sm=3)
