@@ -355,7 +355,7 @@ def render_batch(items, stream: int = 0) -> None:
 
 
 _TUNING_FIELDS = ["tile_width", "blocks_per_sm", "trace_blocks_per_sm", "fetch_batch", "iterations_per_graph",
-                  "slot_count", "evaluations", "best_ms", "default_ms"]
+                  "slot_count", "inline_traversal", "evaluations", "best_ms", "default_ms"]
 
 
 def _tuning_dict(t: TuningC) -> dict:
@@ -380,12 +380,12 @@ def autotune_batch(items) -> dict:
 
 
 def set_tuning(scene: Scene | None = None, **shape) -> None:
-    """Pins a launch shape: tile_width and blocks_per_sm for a scene's megakernel,
+    """Pins a launch shape: tile_width, blocks_per_sm and inline_traversal for a scene's megakernel,
     or (no scene) blocks_per_sm, trace_blocks_per_sm, fetch_batch,
     iterations_per_graph and slot_count for the wavefront engine."""
     t = TuningC()
     for k, v in shape.items():
-        if k not in _TUNING_FIELDS[:6]:
+        if k not in _TUNING_FIELDS[:7]:
             raise ValueError(f"unknown shape field {k}")
         setattr(t, k, int(v))
     _raise(library().albedo_tuning_set(None if scene is None else scene.handle, byref(t)))
@@ -418,6 +418,10 @@ class Server:
         count = c_int32()
         _raise(library().albedo_server_step(self._handle, out, capacity, byref(count)))
         return [out[i] for i in range(count.value)]
+
+    def release_scene(self, scene: Scene) -> None:
+        """Stops counting `scene` against the budget; it must have no requests left in the server."""
+        _raise(library().albedo_server_release_scene(self._handle, scene.handle))
 
     def rays(self) -> int:
         """Ray queries the current batch has traced as of the last polled step."""

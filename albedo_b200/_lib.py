@@ -27,7 +27,8 @@ class CameraC(ctypes.Structure):
 class TuningC(ctypes.Structure):
     _fields_ = [("tile_width", c_int32), ("blocks_per_sm", c_int32), ("trace_blocks_per_sm", c_int32),
                 ("fetch_batch", c_int32), ("iterations_per_graph", c_int32), ("slot_count", c_int32),
-                ("evaluations", c_int32), ("reserved", c_int32), ("best_ms", c_double), ("default_ms", c_double)]
+                ("evaluations", c_int32), ("inline_traversal", c_int32), ("best_ms", c_double),
+                ("default_ms", c_double)]
 
 
 class BatchItemC(ctypes.Structure):
@@ -89,6 +90,7 @@ PROTOTYPES: dict[str, tuple] = {
                                             POINTER(c_int64)]),
     "albedo_server_step": (c_int32, [c_void_p, POINTER(c_int64), c_int32, POINTER(c_int32)]),
     "albedo_server_pending": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
+    "albedo_server_release_scene": (c_int32, [c_void_p, c_void_p]),
     "albedo_server_destroy": (None, [c_void_p]),
     "albedo_autotune_megakernel": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(TuningC)]),
     "albedo_autotune_batch": (c_int32, [c_void_p, c_int32, POINTER(TuningC)]),

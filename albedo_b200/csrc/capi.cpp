@@ -195,6 +195,7 @@ struct albedo_scene {
     // Megakernel launch shape the autotuner kept for this scene (0: default).
     int mega_tile_width{0};
     int mega_blocks_per_sm{0};
+    bool mega_inline{false};
 
     void requireOpen() const
     {
@@ -327,6 +328,10 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     args.tile_width = scene.mega_tile_width;
     args.blocks_per_sm = scene.mega_blocks_per_sm;
     args.accumulation = job.accumulation;
+    // The inlined-traversal kernel exists for the path estimator with FP64 sums;
+    // other renders keep the out-of-line traversal (images do not depend on it).
+    args.inline_traversal =
+        scene.mega_inline && job.estimator == ALBEDO_PATH && job.accumulation == ALBEDO_ACCUMULATE_FP64 ? 1 : 0;
     return args;
 }
 
@@ -875,27 +880,38 @@ int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job
         const std::size_t pixels{static_cast<std::size_t>(probe.width) * static_cast<std::size_t>(probe.height)};
         DeviceBuffer scratch{pixels * sizeof(PixelAccum)};
         TuneTimer timer;
-        const std::vector<TuneKnob> knobs{{"tile_width", {8, 16, 32}}, {"blocks_per_sm", {3, 4}}};
+        // Kernel variants: 0 = 3 blocks/SM, 1 = 4 blocks/SM (both with the
+        // out-of-line traversal), 2 = 3 blocks/SM with the traversal inlined
+        // (path estimator with FP64 sums only).
+        const bool can_inline{probe.estimator == ALBEDO_PATH && probe.accumulation == ALBEDO_ACCUMULATE_FP64};
+        const std::vector<TuneKnob> knobs{{"tile_width", {8, 16, 32}},
+                                          {"variant", can_inline ? std::vector<int>{0, 1, 2} : std::vector<int>{0, 1}}};
         const int kept_tile{scene->mega_tile_width};
         const int kept_blocks{scene->mega_blocks_per_sm};
+        const bool kept_inline{scene->mega_inline};
+        const auto apply = [&](const std::vector<int>& v) {
+            scene->mega_tile_width = v[0];
+            scene->mega_blocks_per_sm = v[1] == 1 ? 4 : 3;
+            scene->mega_inline = v[1] == 2;
+        };
         TuneOutcome outcome;
         try {
-            outcome = tuneExhaustive(knobs, {16, 3}, [&](const std::vector<int>& v) {
-                scene->mega_tile_width = v[0];
-                scene->mega_blocks_per_sm = v[1];
+            outcome = tuneExhaustive(knobs, {16, 0}, [&](const std::vector<int>& v) {
+                apply(v);
                 return timer.time([&] { renderOnDevice(*scene, probe, scratch.as<PixelAccum>(), timer.stream()); },
                                   2);
             });
         } catch (...) {
             scene->mega_tile_width = kept_tile;
             scene->mega_blocks_per_sm = kept_blocks;
+            scene->mega_inline = kept_inline;
             throw;
         }
-        scene->mega_tile_width = outcome.best[0];
-        scene->mega_blocks_per_sm = outcome.best[1];
+        apply(outcome.best);
         scene->collectKernelError();
-        out->tile_width = outcome.best[0];
-        out->blocks_per_sm = outcome.best[1];
+        out->tile_width = scene->mega_tile_width;
+        out->blocks_per_sm = scene->mega_blocks_per_sm;
+        out->inline_traversal = scene->mega_inline ? 1 : 0;
         fillTuning(out, outcome);
     });
 }
@@ -987,8 +1003,12 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
                 throw std::invalid_argument{std::format("megakernel blocks per SM must be 3 or 4, got {}",
                                                         shape->blocks_per_sm)};
             }
+            if (shape->inline_traversal != 0 && (shape->inline_traversal != 1 || shape->blocks_per_sm != 3)) {
+                throw std::invalid_argument{"the inlined-traversal megakernel runs at 3 blocks per SM"};
+            }
             scene->mega_tile_width = shape->tile_width;
             scene->mega_blocks_per_sm = shape->blocks_per_sm;
+            scene->mega_inline = shape->inline_traversal == 1;
             return;
         }
         if (shape->blocks_per_sm <= 0 || shape->trace_blocks_per_sm <= 0 || shape->fetch_batch <= 0 ||
@@ -1016,6 +1036,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out)
         if (scene != nullptr) {
             out->tile_width = scene->mega_tile_width > 0 ? scene->mega_tile_width : 16;
             out->blocks_per_sm = scene->mega_blocks_per_sm > 0 ? scene->mega_blocks_per_sm : 3;
+            out->inline_traversal = scene->mega_inline ? 1 : 0;
             return;
         }
         const std::lock_guard lock{g_engine_mutex};
@@ -1120,6 +1141,22 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
             throw;
         } catch (const std::exception& e) {
             throw DeviceError{e.what()};
+        }
+    });
+}
+
+int albedo_server_release_scene(albedo_server* server, const albedo_scene* scene)
+{
+    return guarded([&] {
+        const auto uses = [&](const albedo_server::Request& r) { return r.scene == scene; };
+        if (std::any_of(server->waiting.begin(), server->waiting.end(), uses) ||
+            std::any_of(server->running.begin(), server->running.end(),
+                        [&](const auto& entry) { return uses(entry.second); })) {
+            throw std::invalid_argument{"the scene still has requests waiting or running in the server"};
+        }
+        if (server->resident.erase(scene) > 0) {
+            server->used -= static_cast<std::int64_t>(scene->deviceBytes());
+            server->admit();
         }
     });
 }

@@ -15,7 +15,11 @@
 
 namespace albedo_b200 {
 
+// Where a thread's queries keep their stack, and how they are traced: INLINE
+// places the traversal in the calling kernel (traceScene).
+template <bool INLINE>
 struct TraceContext {
+    static constexpr bool kInline = INLINE;
     uint2* stack;
     int stride;
     int capacity;
@@ -23,17 +27,20 @@ struct TraceContext {
     TraversalCounts* counts; // null except in the counting variants
 };
 
-ALB_DEV bool closestHit(const DevScene& s, const TraceContext& c, float3 o, float3 d, const SkipRule& skip,
-                        TraceHit& hit)
+template <typename Ctx>
+ALB_DEV bool closestHit(const DevScene& s, const Ctx& c, float3 o, float3 d, const SkipRule& skip, TraceHit& hit)
 {
     float tmax = INFINITY;
-    return traceScene<false>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag, c.counts);
+    return traceScene<false, Ctx::kInline>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity,
+                                           c.error_flag, c.counts);
 }
 
-ALB_DEV bool occluded(const DevScene& s, const TraceContext& c, float3 o, float3 d, float tmax, const SkipRule& skip)
+template <typename Ctx>
+ALB_DEV bool occluded(const DevScene& s, const Ctx& c, float3 o, float3 d, float tmax, const SkipRule& skip)
 {
     TraceHit hit;
-    return traceScene<true>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity, c.error_flag, c.counts);
+    return traceScene<true, Ctx::kInline>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity,
+                                          c.error_flag, c.counts);
 }
 
 // Next-event estimation from one uniformly chosen light, MIS-weighted, before
@@ -91,7 +98,8 @@ ALB_DEV NeeCandidate directLightCandidate(const DevScene& s, const Surface& sf, 
 }
 
 // sampleDirectLight: the candidate, confirmed by a shadow query.
-ALB_DEV float3 sampleDirectLight(const DevScene& s, const TraceContext& c, const Surface& sf, const Scattering& sc,
+template <typename Ctx>
+ALB_DEV float3 sampleDirectLight(const DevScene& s, const Ctx& c, const Surface& sf, const Scattering& sc,
                                  float3 wo, Pcg32& g)
 {
     const NeeCandidate nc = directLightCandidate(s, sf, sc, wo, g);
@@ -160,7 +168,8 @@ ALB_DEV float3 weightedSky(const DevScene& s, const PathState& p)
 
 // The part of a bounce after the surface is known: next-event estimation, BSDF
 // sampling and roulette. Returns false when the path ends.
-ALB_DEV bool scatterAtSurface(const DevScene& s, const TraceContext& c, PathState& p, const Surface& sf, Pcg32& g,
+template <typename Ctx>
+ALB_DEV bool scatterAtSurface(const DevScene& s, const Ctx& c, PathState& p, const Surface& sf, Pcg32& g,
                               int roulette_start)
 {
     const Scattering sc = scatteringAt(s, sf);
@@ -195,7 +204,8 @@ ALB_DEV bool scatterAtSurface(const DevScene& s, const TraceContext& c, PathStat
 
 // One iteration of PathEstimator::radiance's loop. Returns false when the path
 // has ended; p.result then holds its radiance.
-ALB_DEV bool pathBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, int max_depth,
+template <typename Ctx>
+ALB_DEV bool pathBounce(const DevScene& s, const Ctx& c, PathState& p, Pcg32& g, int max_depth,
                         int roulette_start)
 {
     TraceHit hit;
@@ -214,7 +224,8 @@ ALB_DEV bool pathBounce(const DevScene& s, const TraceContext& c, PathState& p, 
 
 // One iteration of ScatterOnlyEstimator::radiance's loop
 // (estimator/scatter_only_estimator.cpp:14-48).
-ALB_DEV bool scatterOnlyBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, int max_scatter)
+template <typename Ctx>
+ALB_DEV bool scatterOnlyBounce(const DevScene& s, const Ctx& c, PathState& p, Pcg32& g, int max_scatter)
 {
     TraceHit hit;
     if (!closestHit(s, c, p.o, p.d, p.skip, hit)) {
@@ -250,7 +261,8 @@ ALB_DEV bool scatterOnlyBounce(const DevScene& s, const TraceContext& c, PathSta
 }
 
 // NormalsEstimator::radiance (estimator/normals_estimator.cpp:32-38): one query.
-ALB_DEV bool normalsBounce(const DevScene& s, const TraceContext& c, PathState& p)
+template <typename Ctx>
+ALB_DEV bool normalsBounce(const DevScene& s, const Ctx& c, PathState& p)
 {
     TraceHit hit;
     if (closestHit(s, c, p.o, p.d, SkipRule::none(), hit)) {
@@ -264,8 +276,8 @@ ALB_DEV bool normalsBounce(const DevScene& s, const TraceContext& c, PathState& 
     return false;
 }
 
-template <int EST>
-ALB_DEV bool estimatorBounce(const DevScene& s, const TraceContext& c, PathState& p, Pcg32& g, const RenderArgs& a)
+template <int EST, typename Ctx>
+ALB_DEV bool estimatorBounce(const DevScene& s, const Ctx& c, PathState& p, Pcg32& g, const RenderArgs& a)
 {
     if constexpr (EST == kEstimatorPath) {
         return pathBounce(s, c, p, g, a.max_depth, a.roulette_start);

@@ -17,7 +17,10 @@ constexpr int kTileW = 16; // default tile: 16 x 8 pixels
 // default: 3 (168 registers a thread) measured 4-12% faster than 4 (128
 // registers, with local-memory spills) on the room and trefoil scenes. The
 // path estimator is also compiled for 4; the autotuner picks per scene.
-constexpr int kMegaBlocksPerSm = 3;
+#ifndef ALBEDO_MEGA_BLOCKS_PER_SM
+#define ALBEDO_MEGA_BLOCKS_PER_SM 3
+#endif
+constexpr int kMegaBlocksPerSm = ALBEDO_MEGA_BLOCKS_PER_SM;
 
 // Per-pixel running sums: FP64, or FP32 with Kahan compensation.
 template <int ACC>
@@ -59,7 +62,8 @@ struct PixelSums<kAccumulateKahan> {
     }
 };
 
-template <int STACK, int EST, bool COUNT = false, int MINB = kMegaBlocksPerSm, int ACC = kAccumulateFp64>
+template <int STACK, int EST, bool COUNT = false, int MINB = kMegaBlocksPerSm, int ACC = kAccumulateFp64,
+          bool INL = false>
 __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene, const DevCamera camera,
                                                           const RenderArgs args, PixelAccum* accum,
                                                           unsigned int* error_flag,
@@ -67,7 +71,7 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
 {
     extern __shared__ uint2 stack[];
     TraversalCounts counts{0, 0, 0, 0, 0};
-    const TraceContext ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
+    const TraceContext<INL> ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
         slot = blockIdx.x * kBlock + threadIdx.x;
@@ -273,6 +277,10 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                                             no_totals);
                 }
                 return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan>,
+                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
+            }
+            if (args.inline_traversal != 0) {
+                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, true>,
                                         megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
             }
             if (args.blocks_per_sm == 4) {

@@ -508,19 +508,16 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
     return step == kStepDescend || popNext(q, stack, stride);
 }
 
-// Traverses the scene for the nearest hit in (tmin, tmax) (ANY = false), or for
-// any hit (ANY = true). On return `tmax` is the nearest hit distance. The stack
+// Traverses the scene for the nearest hit in (tmin, tmax) (any = false), or for
+// any hit (any = true). On return `tmax` is the nearest hit distance. The stack
 // overflow bound (TLAS depth + BLAS depth + 2) is checked on the host before
-// launch, so pushes never exceed `stack_size`.
-// One out-of-line copy serves closest-hit and any-hit queries alike (`any`
-// stops at the first hit), which keeps the kernels that call it small enough
-// for the instruction cache. It takes one step (a node or a leaf) per loop
-// turn: inside the megakernel, the nested node/leaf loops of traceAdvance
-// measured 3.4x slower.
-static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 origin, float3 dir, float tmin,
-                                                   float& tmax, const SkipRule& skip, TraceHit& hit, uint2* stack,
-                                                   int stride, int stack_size, unsigned int* error_flag,
-                                                   TraversalCounts* counts, bool any)
+// launch, so pushes never exceed `stack_size`. It takes one step (a node or a
+// leaf) per loop turn: inside the megakernel, the nested node/leaf loops of
+// traceAdvance measured 3.4x slower.
+__device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
+                                               const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
+                                               int stack_size, unsigned int* error_flag, TraversalCounts* counts,
+                                               bool any)
 {
     if (counts != nullptr) {
         counts->rays += 1;
@@ -544,12 +541,32 @@ static __device__ __noinline__ bool traceSceneImpl(const DevScene& s, float3 ori
     return q.found;
 }
 
-template <bool ANY>
+// One out-of-line copy serving closest-hit and any-hit queries alike, which
+// keeps the kernels that call it small enough for the instruction cache.
+static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
+                                                        float& tmax, const SkipRule& skip, TraceHit& hit,
+                                                        uint2* stack, int stride, int stack_size,
+                                                        unsigned int* error_flag, TraversalCounts* counts, bool any)
+{
+    return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts, any);
+}
+
+// A query from a caller that keeps its state across the call (the megakernel).
+// INLINE places the traversal in the caller instead of calling the shared copy:
+// no call, no registers saved around it, but a larger kernel. Which is faster
+// depends on the scene (the megakernel's autotuner picks).
+template <bool ANY, bool INLINE = false>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
                         TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts = nullptr)
 {
-    return traceSceneImpl(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts, ANY);
+    if constexpr (INLINE) {
+        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts,
+                              ANY);
+    } else {
+        return traceSceneOutOfLine(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                                   counts, ANY);
+    }
 }
 
 } // namespace albedo_b200

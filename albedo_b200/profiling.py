@@ -18,9 +18,9 @@ import math
 import tempfile
 from pathlib import Path
 
-# Megakernel launches one tuning pass makes: every shape (3 tile widths x 2
-# register budgets) once untimed and twice timed.
-MEGAKERNEL_TUNING_LAUNCHES = 6 * 3
+# Megakernel launches one tuning pass makes: every shape (3 tile widths x 3
+# kernel variants) once untimed and twice timed.
+MEGAKERNEL_TUNING_LAUNCHES = 9 * 3
 
 
 def main() -> None:

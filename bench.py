@@ -373,7 +373,8 @@ def batched_figures(steps: int, warmup: int, count: int = 64) -> dict:
     peak = measured_peaks().get("hbm_gbs") or 6650.0
     tiles = {}
     for shape in mega_shapes:
-        key = f"{shape['tile_width']}x{128 // shape['tile_width']}/{shape['blocks_per_sm']}"
+        key = (f"{shape['tile_width']}x{128 // shape['tile_width']}/{shape['blocks_per_sm']}"
+               + ("/inline" if shape["inline_traversal"] else ""))
         tiles[key] = tiles.get(key, 0) + 1
     return {
         "jobs": len(jobs), "paths_per_step": paths,

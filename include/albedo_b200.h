@@ -248,6 +248,11 @@ int albedo_server_submit_view(albedo_server* server, const albedo_scene* scene, 
  * reported by later calls. */
 int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacity, int32_t* out_finished);
 int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int32_t* out_running);
+/* Stops counting a scene's tables against the server's budget (and admits what
+ * then fits). The server counts each scene once, from its first admitted
+ * request until this call; call it before destroying a scene the server has
+ * rendered. A scene with requests still waiting or running is refused. */
+int albedo_server_release_scene(albedo_server* server, const albedo_scene* scene);
 void albedo_server_destroy(albedo_server* server);
 /* Wavefront engine shape: path slots, blocks per SM of the queue kernels, and
  * iterations per captured CUDA graph; the traversal kernels' blocks per SM and
@@ -269,12 +274,15 @@ typedef struct albedo_tuning {
     int32_t iterations_per_graph; /* wavefront: iterations per captured CUDA graph */
     int32_t slot_count;           /* wavefront: path slots */
     int32_t evaluations;          /* shapes timed */
-    int32_t reserved;
+    int32_t inline_traversal;     /* megakernel: 1 = traversal inlined into the kernel (3 blocks per SM;
+                                     path estimator with FP64 sums), 0 = one out-of-line copy */
     double best_ms;               /* the kept shape's time on the tuning work */
     double default_ms;            /* the default shape's time on the same work */
 } albedo_tuning;
-/* Tunes the megakernel for `scene` (tile width x register budget, every
- * combination) on `job` and keeps the result in the scene. */
+/* Tunes the megakernel for `scene` on `job` and keeps the result in the scene:
+ * every tile width with every kernel variant (3 or 4 blocks per SM with an
+ * out-of-line traversal, or 3 with the traversal inlined, which is faster on
+ * some scenes and slower on others). */
 int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
 /* Tunes the wavefront engine on a batch (coordinate descent over traversal
  * blocks per SM, fetch batch, queue-kernel blocks per SM, iterations per graph
@@ -284,7 +292,8 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
  * the process's wavefront shape (scene NULL); timing fields are zero. */
 int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
 /* Pins a shape, as the autotuner would keep it: the scene's megakernel shape
- * (scene not NULL: tile_width 8, 16 or 32 and blocks_per_sm 3 or 4) or the
+ * (scene not NULL: tile_width 8, 16 or 32, blocks_per_sm 3 or 4, and
+ * inline_traversal 0 or 1, the latter with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive). Timing fields
  * are ignored. Images do not depend on the shape. */

@@ -106,3 +106,38 @@ def test_a_request_larger_than_the_budget_is_refused(room_path):
     with pytest.raises(ValueError, match="exceeds the server's memory budget"):
         server.submit(room, ab.RenderJob(1024, 576, method=ab.WAVEFRONT), acc.data_ptr())
     server.close()
+
+
+def test_releasing_a_scene_frees_its_share_of_the_budget(trefoil_path, tmp_path):
+    from albedo_b200 import scenes
+
+    first_scene = ab.Scene.load(trefoil_path)
+    second_scene = ab.Scene.load(scenes.trefoil_scene(tmp_path / "other", seed=8))
+    sizes = [first_scene.info()["device_bytes"], second_scene.info()["device_bytes"]]
+    slots = 1 << 14
+    # Budget: the slot pool and job table (256 B a slot plus about 1 MB), one
+    # scene and two small frames; the 1 MB of slack is smaller than either scene,
+    # so both scenes never fit at once.
+    frame = 64 * 36 * 32
+    budget = slots * 256 + (2 << 20) + max(sizes) + 2 * frame
+    assert min(sizes) > (1 << 20) + 2 * frame
+    server = ab.Server(memory_budget_bytes=budget, slots=slots)
+    job = ab.RenderJob(64, 36, samples_per_axis=2, max_depth=8, method=ab.WAVEFRONT)
+    a = torch.zeros((64 * 36, 4), dtype=torch.float64, device="cuda")
+    b = torch.zeros((64 * 36, 4), dtype=torch.float64, device="cuda")
+    first = server.submit(first_scene, job, a.data_ptr())
+    with pytest.raises(ValueError, match="still has requests"):
+        server.release_scene(first_scene)
+    done = []
+    while first not in done:
+        done += server.step()
+    second = server.submit(second_scene, job, b.data_ptr())
+    assert server.pending() == (1, 0)  # the first scene's tables still count
+    server.release_scene(first_scene)
+    assert server.pending() == (0, 1)
+    while second not in done:
+        done += server.step()
+    torch.cuda.synchronize()
+    assert_same_image(a.cpu().numpy(), alone(first_scene, job))
+    assert_same_image(b.cpu().numpy(), alone(second_scene, job))
+    server.close()
