@@ -464,19 +464,34 @@ def wavefront_last_rays() -> int:
     return out.value
 
 
+_COUNT_NAMES = ["boxes", "triangles", "spheres", "instances", "rays", "reference_boxes"]
+
+
 def work_counts(scene: Scene, job: RenderJob) -> dict:
-    """Traversal work of one render of `job` (path estimator), counted on the device."""
-    out = (ctypes.c_int64 * 5)()
+    """Traversal work of one render of `job` (path estimator), counted on the device:
+    child boxes the 4-wide traversal tested, triangles, spheres, instances entered,
+    queries, and the boxes the reference's binary traversal tests for the same queries."""
+    out = (ctypes.c_int64 * 6)()
     c = job.to_c()
     _raise(library().albedo_render_work_counts(scene.handle, byref(c), out))
-    return dict(zip(["boxes", "triangles", "spheres", "instances", "rays"], [int(v) for v in out]))
+    return dict(zip(_COUNT_NAMES, [int(v) for v in out]))
 
 
-def algorithmic_bytes(counts: dict) -> int:
-    """Bytes a traversal must read for the counted work: 32 per box tested, 48 per
-    triangle, 32 per sphere (its 16-byte record and its object entry), 96 per
-    instance entered (its two 3x4 FP32 transforms)."""
-    return 32 * counts["boxes"] + 48 * counts["triangles"] + 32 * counts["spheres"] + 96 * counts["instances"]
+def trace_work_counts(scene: Scene, rays: np.ndarray, t_min: float = 0.0, t_max: float = float("inf")) -> dict:
+    """The same counts for closest-hit queries of (N, 6) float32 rays."""
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 6)
+    out = (ctypes.c_int64 * 6)()
+    _raise(library().albedo_trace_counts_host(scene.handle, _fptr(rays), len(rays), t_min, t_max, out))
+    return dict(zip(_COUNT_NAMES, [int(v) for v in out]))
+
+
+def algorithmic_bytes(counts: dict, boxes: str = "reference_boxes") -> int:
+    """Bytes the reference's traversal must read for the counted work: 32 per box
+    it tests (by default the boxes its binary traversal tests; `boxes="boxes"`
+    counts the 4-wide traversal's child boxes instead), 48 per triangle, 32 per
+    sphere (its 16-byte record and its object entry), 96 per instance entered
+    (its two 3x4 FP32 transforms)."""
+    return 32 * counts[boxes] + 48 * counts["triangles"] + 32 * counts["spheres"] + 96 * counts["instances"]
 
 
 def render_pixels(scene: Scene, job: RenderJob, pixels: np.ndarray, with_squares: bool = False):
@@ -495,5 +510,5 @@ __all__ = [
     "ACCUMULATE_FP64", "ACCUMULATE_KAHAN_FP32", "ACCUMULATOR_DTYPE", "BasicMaterial", "Camera", "DeviceError",
     "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
     "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
-    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "set_tuning", "tuning", "wavefront_last_rays",
+    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "set_tuning", "trace_work_counts", "tuning", "wavefront_last_rays",
 ]

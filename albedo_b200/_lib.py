@@ -81,6 +81,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
     "albedo_scene_check": (c_int32, [c_void_p]),
     "albedo_render_work_counts": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(c_int64)]),
+    "albedo_trace_counts_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, POINTER(c_int64)]),
     "albedo_render_batch": (c_int32, [c_void_p, c_int32, c_void_p]),
     "albedo_render_noalloc": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
     "albedo_wavefront_configure": (c_int32, [c_int32, c_int32, c_int32]),

@@ -1229,7 +1229,7 @@ int albedo_render_work_counts(const albedo_scene* scene, const albedo_render_job
         const RenderArgs args{renderArgsFor(*scene, *job)};
         const std::size_t pixels{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height)};
         DeviceBuffer accum{pixels * sizeof(PixelAccum)};
-        DeviceBuffer totals{5 * sizeof(unsigned long long)};
+        DeviceBuffer totals{6 * sizeof(unsigned long long)};
         check(cudaMemset(accum.ptr, 0, accum.bytes), "cudaMemset");
         check(cudaMemset(totals.ptr, 0, totals.bytes), "cudaMemset");
         const DevCamera camera{deviceCamera(scene->host, job->width, job->height)};
@@ -1238,9 +1238,35 @@ int albedo_render_work_counts(const albedo_scene* scene, const albedo_render_job
                                        totals.as<unsigned long long>(), nullptr),
               "counting launch");
         check(cudaDeviceSynchronize(), "counting");
-        unsigned long long host[5]{};
+        unsigned long long host[6]{};
         check(cudaMemcpy(host, totals.ptr, sizeof(host), cudaMemcpyDeviceToHost), "download");
-        for (int i{0}; i < 5; ++i) {
+        for (int i{0}; i < 6; ++i) {
+            out_counts[i] = static_cast<int64_t>(host[i]);
+        }
+        scene->collectKernelError();
+    });
+}
+
+int albedo_trace_counts_host(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                             int64_t* out_counts)
+{
+    return guarded([&] {
+        scene->requireCommitted();
+        if (count <= 0 || count > (int64_t{1} << 30)) {
+            throw std::invalid_argument{"ray count must be in 1..2^30"};
+        }
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer d_rays{uploadRaw(rays, 6 * n)};
+        DeviceBuffer totals{6 * sizeof(unsigned long long)};
+        check(cudaMemset(totals.ptr, 0, totals.bytes), "cudaMemset");
+        check(launchTraceCounting(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max,
+                                  scene->error_flag.as<unsigned int>(), scene->stack_capacity,
+                                  totals.as<unsigned long long>(), nullptr),
+              "counting trace launch");
+        check(cudaDeviceSynchronize(), "counting trace");
+        unsigned long long host[6]{};
+        check(cudaMemcpy(host, totals.ptr, sizeof(host), cudaMemcpyDeviceToHost), "download");
+        for (int i{0}; i < 6; ++i) {
             out_counts[i] = static_cast<int64_t>(host[i]);
         }
         scene->collectKernelError();

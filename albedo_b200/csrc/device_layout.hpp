@@ -41,8 +41,8 @@ struct alignas(16) DevNode {
     float hi_z[4];
     std::uint32_t child[4];
     std::uint8_t order[8];
-    std::uint32_t count; // children present (1..4); they are child[0..count-1]
-    std::uint32_t pad;
+    std::uint32_t count;  // children present (1..4); they are child[0..count-1]
+    std::uint32_t groups; // slots per binary child of the collapsed node (bits 0-1, 2-3); 0 for a leaf root
 };
 static_assert(sizeof(DevNode) == 128);
 

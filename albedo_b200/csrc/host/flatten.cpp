@@ -138,6 +138,10 @@ Emitted emitBvh(const BuiltBvh& bvh, std::uint64_t prim_base, std::vector<DevNod
             }
         }
         dev.count = static_cast<std::uint32_t>(slot);
+        // The binary structure this node collapses, for counting the boxes the
+        // reference's traversal tests: group g holds the first or second child of
+        // node i (1 slot if a leaf, else its 2 children).
+        dev.groups = static_cast<std::uint32_t>(groups[0].size) | (static_cast<std::uint32_t>(groups[1].size) << 2U);
         for (unsigned octant{0}; octant < 8; ++octant) {
             const bool swap{((octant >> bvh.nodes[i].axis) & 1U) != 0};
             std::uint8_t packed{0};

@@ -85,8 +85,9 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                              unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
 
 // The megakernel (path estimator) counting its traversal work into
-// totals[0..4] = child boxes tested, triangles tested, spheres tested,
-// instances entered, queries traced. Not used for timing.
+// totals[0..5] = child boxes tested, triangles tested, spheres tested,
+// instances entered, queries traced, boxes the reference's binary traversal
+// tests for the same queries. Not used for timing.
 cudaError_t launchMegakernelCounting(const DevScene& scene, const DevCamera& camera, const RenderArgs& args,
                                      PixelAccum* accum, unsigned int* error_flag, int stack_capacity,
                                      unsigned long long* totals, cudaStream_t stream);
@@ -104,6 +105,10 @@ struct TraceOutputs {
     float* shading_normal;
     int* front;
 };
+// Closest-hit queries of given rays counting their work into totals[0..5].
+cudaError_t launchTraceCounting(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
+                                unsigned int* error_flag, int stack_capacity, unsigned long long* totals,
+                                cudaStream_t stream);
 cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
                         const TraceOutputs& out, unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
 // Any hit in (0, t_max[i]).

@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
                                                           unsigned long long* totals = nullptr)
 {
     extern __shared__ uint2 stack[];
-    TraversalCounts counts{0, 0, 0, 0, 0};
+    TraversalCounts counts{0, 0, 0, 0, 0, 0};
     const TraceContext<INL> ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
@@ -138,7 +138,35 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
         atomicAdd(totals + 2, counts.spheres);
         atomicAdd(totals + 3, counts.instances);
         atomicAdd(totals + 4, counts.rays);
+        atomicAdd(totals + 5, counts.reference_boxes);
     }
+}
+
+// Closest-hit queries of given rays, counting their traversal work into
+// totals[0..5] (as the counting megakernel does). Not used for timing.
+template <int STACK>
+__global__ void __launch_bounds__(kBlock) traceCountKernel(const DevScene scene, const float* rays, int count,
+                                                           float t_min, float t_max, unsigned int* error_flag,
+                                                           unsigned long long* totals)
+{
+    extern __shared__ uint2 stack[];
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) {
+        return;
+    }
+    TraversalCounts counts{0, 0, 0, 0, 0, 0};
+    const float3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+    const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+    TraceHit hit;
+    float tmax = t_max;
+    static_cast<void>(traceScene<false>(scene, o, d, t_min, tmax, SkipRule::none(), hit, stack + threadIdx.x, kBlock,
+                                        STACK, error_flag, &counts));
+    atomicAdd(totals + 0, counts.boxes);
+    atomicAdd(totals + 1, counts.triangles);
+    atomicAdd(totals + 2, counts.spheres);
+    atomicAdd(totals + 3, counts.instances);
+    atomicAdd(totals + 4, counts.rays);
+    atomicAdd(totals + 5, counts.reference_boxes);
 }
 
 template <int STACK>
@@ -300,6 +328,17 @@ cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, flo
         constexpr int S = decltype(size)::value;
         return launchStacked<S>(traceKernel<S>, (count + kBlock - 1) / kBlock, stream, scene, rays, count, t_min,
                                 t_max, out, error_flag);
+    });
+}
+
+cudaError_t launchTraceCounting(const DevScene& scene, const float* rays, int count, float t_min, float t_max,
+                                unsigned int* error_flag, int stack_capacity, unsigned long long* totals,
+                                cudaStream_t stream)
+{
+    return withStack(stack_capacity, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        return launchStacked<S>(traceCountKernel<S>, (count + kBlock - 1) / kBlock, stream, scene, rays, count, t_min,
+                                t_max, error_flag, totals);
     });
 }
 

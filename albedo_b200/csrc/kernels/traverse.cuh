@@ -42,13 +42,16 @@ struct SkipRule {
 };
 
 // Work one query did, for the algorithmic-bytes figure: child boxes tested,
-// triangles and spheres tested, instances entered, queries traced.
+// triangles and spheres tested, instances entered, queries traced, and the
+// boxes the reference's binary traversal tests for the same query (one per node
+// it pops, accel/bvh.hpp:239-278).
 struct TraversalCounts {
     unsigned long long boxes;
     unsigned long long triangles;
     unsigned long long spheres;
     unsigned long long instances;
     unsigned long long rays;
+    unsigned long long reference_boxes;
 };
 
 struct TraceHit {
@@ -306,6 +309,42 @@ ALB_DEV bool traceBegin(const DevScene& s, TraceState& q, float3 origin, float3 
     return true;
 }
 
+// The boxes the reference's binary traversal tests below a 4-wide node: it pops
+// both binary children (one box each) and, for a binary child that is interior
+// and whose box the ray enters, both of its children. That child's box is the
+// union of the two slots it became.
+__device__ __forceinline__ float slotOf(const float4& v, int k)
+{
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void countReferenceBoxes(const float4& lx, const float4& hx, const float4& ly,
+                                                    const float4& hy, const float4& lz, const float4& hz,
+                                                    unsigned groups, const TravRay& r, float tmin, float tmax,
+                                                    TraversalCounts& counts)
+{
+    if (groups == 0u) {
+        return;
+    }
+    counts.reference_boxes += 2;
+    int first = 0;
+    for (int g = 0; g < 2; ++g) {
+        const int size = static_cast<int>((groups >> (2 * g)) & 3u);
+        if (size == 2) {
+            const int a = first;
+            const int b = first + 1;
+            float entry;
+            if (slabTest(fminf(slotOf(lx, a), slotOf(lx, b)), fmaxf(slotOf(hx, a), slotOf(hx, b)),
+                         fminf(slotOf(ly, a), slotOf(ly, b)), fmaxf(slotOf(hy, a), slotOf(hy, b)),
+                         fminf(slotOf(lz, a), slotOf(lz, b)), fmaxf(slotOf(hz, a), slotOf(hz, b)), r, tmin, tmax,
+                         entry)) {
+                counts.reference_boxes += 2;
+            }
+        }
+        first += size;
+    }
+}
+
 // A 4-wide node: tests every child box, continues with the hit child the
 // reference reaches first and pushes the other hit children, last first, so
 // leaves are reached in the reference's depth-first near-first order.
@@ -322,10 +361,11 @@ __device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, uint2*
     const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
     const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
     const int present = static_cast<int>(meta.z);
+    const TravRay& r = q.r;
     if (counts != nullptr) {
         counts->boxes += static_cast<unsigned>(present);
+        countReferenceBoxes(lx, hx, ly, hy, lz, hz, meta.w, r, q.tmin, q.tmax, *counts);
     }
-    const TravRay& r = q.r;
     float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
     unsigned mask = slabTest(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, q.tmin, q.tmax, e0) ? 1u : 0u;
     if (present > 1 && slabTest(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, q.tmin, q.tmax, e1)) {
@@ -397,6 +437,7 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
                 const DevInstance& inst = s.instances[obj.index];
                 if (counts != nullptr) {
                     counts->instances += 1;
+                    counts->reference_boxes += 1; // the BLAS root
                 }
                 q.r.setup(affinePoint(inst.to_object, q.origin), affineVector(inst.to_object, q.dir));
                 q.inst_pos = pos;
@@ -525,6 +566,9 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
     TraceState q;
     if (!traceBegin(s, q, origin, dir, tmin, tmax)) {
         return false;
+    }
+    if (counts != nullptr) {
+        counts->reference_boxes += 1; // the TLAS root
     }
     for (;;) {
         const int step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)

@@ -306,9 +306,16 @@ int albedo_wavefront_last_rays(int64_t* out);
  * results were polled (the count restarts when the engine reopens a batch). */
 int albedo_server_rays(const albedo_server* server, int64_t* out);
 /* Renders the job once (path estimator, into scratch accumulators) while counting
- * traversal work: out_counts[0..4] = child boxes tested, triangles tested,
- * spheres tested, instances entered, ray queries traced. Synchronous. */
+ * traversal work: out_counts[0..5] = child boxes the 4-wide traversal tested,
+ * triangles tested, spheres tested, instances entered, ray queries traced, and
+ * the boxes the reference's binary traversal (accel/bvh.hpp:239-278: one box
+ * per node popped) tests for the same queries. Synchronous. No counterpart in
+ * the reference. */
 int albedo_render_work_counts(const albedo_scene* scene, const albedo_render_job* job, int64_t* out_counts);
+/* The same six counts for closest-hit queries of given rays (6 floats each,
+ * as albedo_trace_host). Synchronous. */
+int albedo_trace_counts_host(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                             int64_t* out_counts);
 /* Reads and clears the scene's kernel error flag (synchronizes the device). */
 int albedo_scene_check(const albedo_scene* scene);
 

@@ -189,6 +189,31 @@ def test_ray_queries_match(which, room_path, trefoil_path):
     assert np.quantile(ndot, 0.001) > 0.9999
 
 
+@pytest.mark.parametrize("which", ["room", "trefoil"])
+def test_reference_box_counts_match_the_restatement(which, room_path, trefoil_path):
+    """The counting traversal's estimate of the boxes the reference's binary
+    traversal tests (one per node popped), and its primitive counts, against the
+    FP64 restatement of that traversal on the same rays. The device tests each
+    collapsed node's boxes when it reaches the node, the reference when it pops
+    them (possibly after the range shrank), and FP32 boxes are rounded outward:
+    both can only add work, so the device may count a few percent more."""
+    from oracle import restatement
+
+    path = room_path if which == "room" else trefoil_path
+    scene = ab.Scene.load(path)
+    rays = random_rays(50_000, 9, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    device = ab.trace_work_counts(scene, rays)
+    theirs = restatement.intersect(scene, rays.astype(np.float64))["counts"].sum(axis=0)
+    assert device["rays"] == len(rays)
+    ratio = device["reference_boxes"] / theirs[0]
+    assert 0.99 < ratio < 1.10, (ratio, device, theirs)
+    for k, i in (("triangles", 1), ("spheres", 2), ("instances", 3)):
+        if theirs[i] == 0:
+            assert device[k] == 0, (k, device, theirs)
+        else:
+            assert 0.99 < device[k] / theirs[i] < 1.05, (k, device, theirs)
+
+
 def test_occlusion_queries_match(room_path):
     scene = ab.Scene.load(room_path)
     rays = random_rays(50_000, 6, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
