@@ -16,10 +16,12 @@
 namespace albedo_b200 {
 
 // Where a thread's queries keep their stack, and how they are traced: INLINE
-// places the traversal in the calling kernel (traceScene).
-template <bool INLINE>
+// places the traversal in the calling kernel, COUNT counts its work into
+// `counts` (traceScene).
+template <bool INLINE, bool COUNT = false>
 struct TraceContext {
     static constexpr bool kInline = INLINE;
+    static constexpr bool kCount = COUNT;
     uint2* stack;
     int stride;
     int capacity;
@@ -31,16 +33,16 @@ template <typename Ctx>
 ALB_DEV bool closestHit(const DevScene& s, const Ctx& c, float3 o, float3 d, const SkipRule& skip, TraceHit& hit)
 {
     float tmax = INFINITY;
-    return traceScene<false, Ctx::kInline>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity,
-                                           c.error_flag, c.counts);
+    return traceScene<false, Ctx::kInline, Ctx::kCount>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride,
+                                                        c.capacity, c.error_flag, c.counts);
 }
 
 template <typename Ctx>
 ALB_DEV bool occluded(const DevScene& s, const Ctx& c, float3 o, float3 d, float tmax, const SkipRule& skip)
 {
     TraceHit hit;
-    return traceScene<true, Ctx::kInline>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride, c.capacity,
-                                          c.error_flag, c.counts);
+    return traceScene<true, Ctx::kInline, Ctx::kCount>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride,
+                                                       c.capacity, c.error_flag, c.counts);
 }
 
 // Next-event estimation from one uniformly chosen light, MIS-weighted, before

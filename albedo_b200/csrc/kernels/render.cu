@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
 {
     extern __shared__ uint2 stack[];
     TraversalCounts counts{0, 0, 0, 0, 0, 0};
-    const TraceContext<INL> ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
+    const TraceContext<INL, COUNT> ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
         slot = blockIdx.x * kBlock + threadIdx.x;
@@ -159,8 +159,8 @@ __global__ void __launch_bounds__(kBlock) traceCountKernel(const DevScene scene,
     const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
     TraceHit hit;
     float tmax = t_max;
-    static_cast<void>(traceScene<false>(scene, o, d, t_min, tmax, SkipRule::none(), hit, stack + threadIdx.x, kBlock,
-                                        STACK, error_flag, &counts));
+    static_cast<void>(traceScene<false, false, true>(scene, o, d, t_min, tmax, SkipRule::none(), hit,
+                                                     stack + threadIdx.x, kBlock, STACK, error_flag, &counts));
     atomicAdd(totals + 0, counts.boxes);
     atomicAdd(totals + 1, counts.triangles);
     atomicAdd(totals + 2, counts.spheres);

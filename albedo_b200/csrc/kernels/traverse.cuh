@@ -586,30 +586,35 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
 }
 
 // One out-of-line copy serving closest-hit and any-hit queries alike, which
-// keeps the kernels that call it small enough for the instruction cache.
+// keeps the kernels that call it small enough for the instruction cache. COUNT
+// selects the copy that counts work (the counting kernels); the timed kernels'
+// copy has no counting code at all.
+template <bool COUNT>
 static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
                                                         float& tmax, const SkipRule& skip, TraceHit& hit,
                                                         uint2* stack, int stride, int stack_size,
                                                         unsigned int* error_flag, TraversalCounts* counts, bool any)
 {
-    return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts, any);
+    return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                          COUNT ? counts : nullptr, any);
 }
 
 // A query from a caller that keeps its state across the call (the megakernel).
 // INLINE places the traversal in the caller instead of calling the shared copy:
 // no call, no registers saved around it, but a larger kernel. Which is faster
-// depends on the scene (the megakernel's autotuner picks).
-template <bool ANY, bool INLINE = false>
+// depends on the scene (the megakernel's autotuner picks). COUNT adds the work
+// counts into `counts`; without it `counts` is ignored.
+template <bool ANY, bool INLINE = false, bool COUNT = false>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
                         TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts = nullptr)
 {
     if constexpr (INLINE) {
-        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag, counts,
-                              ANY);
+        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                              COUNT ? counts : nullptr, ANY);
     } else {
-        return traceSceneOutOfLine(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
-                                   counts, ANY);
+        return traceSceneOutOfLine<COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size,
+                                          error_flag, counts, ANY);
     }
 }
 
