@@ -631,14 +631,15 @@ def main():
     e2e_ms = []
     barrier()
     torch.cuda.synchronize()
-    for i in range(args.steps):
-        flush.fill_(i & 0xFF)
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        ab.render_image_ptr(scene, job, host_accum.data_ptr())
-        e.record()
-        e.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
+    with ClockSampler(local_rank) as e2e_clocks:
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            ab.render_image_ptr(scene, job, host_accum.data_ptr())
+            e.record()
+            e.synchronize()
+            e2e_ms.append(s.elapsed_time(e))
     barrier()
     e2e_total = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
     if dist is not None:
@@ -666,7 +667,8 @@ def main():
             "mrays_per_s": world * counts["rays"] * args.steps / total_s / 1e6,
             "gpu_launches": args.steps,
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": frame_bytes,
-                    "d2h_bytes_per_step": frame_bytes},
+                    "d2h_bytes_per_step": frame_bytes, "ms_per_step": statistics.mean(e2e_ms),
+                    "clocks": e2e_clocks.summary()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": f"megakernel<{scene.info()['stack_capacity']}, path>",
