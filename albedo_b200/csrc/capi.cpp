@@ -328,10 +328,9 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     args.tile_width = scene.mega_tile_width;
     args.blocks_per_sm = scene.mega_blocks_per_sm;
     args.accumulation = job.accumulation;
-    // The inlined-traversal kernel exists for the path estimator with FP64 sums;
-    // other renders keep the out-of-line traversal (images do not depend on it).
-    args.inline_traversal =
-        scene.mega_inline && job.estimator == ALBEDO_PATH && job.accumulation == ALBEDO_ACCUMULATE_FP64 ? 1 : 0;
+    // The inlined-traversal kernel exists for the path estimator; the other
+    // estimators keep the out-of-line traversal (images do not depend on it).
+    args.inline_traversal = scene.mega_inline && job.estimator == ALBEDO_PATH ? 1 : 0;
     return args;
 }
 
@@ -882,8 +881,8 @@ int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job
         TuneTimer timer;
         // Kernel variants: 0 = 3 blocks/SM, 1 = 4 blocks/SM (both with the
         // out-of-line traversal), 2 = 3 blocks/SM with the traversal inlined
-        // (path estimator with FP64 sums only).
-        const bool can_inline{probe.estimator == ALBEDO_PATH && probe.accumulation == ALBEDO_ACCUMULATE_FP64};
+        // (path estimator only).
+        const bool can_inline{probe.estimator == ALBEDO_PATH};
         const std::vector<TuneKnob> knobs{{"tile_width", {8, 16, 32}},
                                           {"variant", can_inline ? std::vector<int>{0, 1, 2} : std::vector<int>{0, 1}}};
         const int kept_tile{scene->mega_tile_width};

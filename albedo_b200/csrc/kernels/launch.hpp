@@ -33,8 +33,8 @@ struct RenderArgs {
     // per SM the kernel is compiled for: 3 or 4). 0 picks the default (16, 3).
     int tile_width;
     int blocks_per_sm;
-    // Nonzero: the traversal is inlined into the kernel (3 blocks per SM, FP64
-    // sums, path estimator) instead of called out of line.
+    // Nonzero: the traversal is inlined into the kernel (3 blocks per SM, path
+    // estimator) instead of called out of line.
     int inline_traversal;
     // Per-pixel sums inside the kernel: kAccumulateFp64, or kAccumulateKahan
     // (compensated FP32, path estimator only). Either is added to the FP64

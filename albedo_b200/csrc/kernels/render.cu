@@ -299,6 +299,12 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                                     accum, error_flag, no_totals);
         default:
             if (args.accumulation == kAccumulateKahan) {
+                if (args.inline_traversal != 0) {
+                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan,
+                                                       true>,
+                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
+                                            no_totals);
+                }
                 if (args.blocks_per_sm == 4) {
                     return launchStacked<S>(megakernel<S, kEstimatorPath, false, 4, kAccumulateKahan>,
                                             megaBlocks(args), stream, scene, camera, args, accum, error_flag,

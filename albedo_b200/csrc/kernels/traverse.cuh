@@ -599,23 +599,33 @@ static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float
                           COUNT ? counts : nullptr, any);
 }
 
-// A query from a caller that keeps its state across the call (the megakernel).
-// INLINE places the traversal in the caller instead of calling the shared copy:
-// no call, no registers saved around it, but a larger kernel. Which is faster
-// depends on the scene (the megakernel's autotuner picks). COUNT adds the work
-// counts into `counts`; without it `counts` is ignored.
+// A query from a caller that keeps its state across the call (the megakernel),
+// closest hit or any hit as `any` says. INLINE places the traversal in the
+// caller instead of calling the shared copy: no call, no registers saved around
+// it, but a larger kernel. Which is faster depends on the scene (the
+// megakernel's autotuner picks). COUNT adds the work counts into `counts`;
+// without it `counts` is ignored.
+template <bool INLINE = false, bool COUNT = false>
+ALB_DEV bool traceQuery(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
+                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
+                        TraversalCounts* counts, bool any)
+{
+    if constexpr (INLINE) {
+        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                              COUNT ? counts : nullptr, any);
+    } else {
+        return traceSceneOutOfLine<COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size,
+                                          error_flag, counts, any);
+    }
+}
+
 template <bool ANY, bool INLINE = false, bool COUNT = false>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
                         TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts = nullptr)
 {
-    if constexpr (INLINE) {
-        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
-                              COUNT ? counts : nullptr, ANY);
-    } else {
-        return traceSceneOutOfLine<COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size,
-                                          error_flag, counts, ANY);
-    }
+    return traceQuery<INLINE, COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                                     counts, ANY);
 }
 
 } // namespace albedo_b200

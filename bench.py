@@ -259,6 +259,7 @@ def run_precision(args) -> None:
                                    accumulation=accumulation)
                 acc = torch.zeros((width * height, 4), dtype=torch.float64, device="cuda")
                 if label == "megakernel_fp64":
+                    # Both accumulation modes run the shape tuned here.
                     ab.autotune_megakernel(scene, job)
                 elif method == ab.WAVEFRONT:
                     ab.autotune_batch([(scene, job, acc.data_ptr())])
@@ -300,7 +301,8 @@ def run_precision(args) -> None:
                             "error_vs_fp64_oracle": err,
                             "oracle": {"pixels": 256, "spp": 65536, "seconds": oracle_s},
                             "kahan_vs_fp64_max_rel": float(np.max(np.abs(kahan - fp64)[lit] / np.abs(fp64)[lit])),
-                            "tuned_megakernel": {k: ab.tuning(scene)[k] for k in ("tile_width", "blocks_per_sm")}})
+                            "tuned_megakernel": {k: ab.tuning(scene)[k]
+                                                 for k in ("tile_width", "blocks_per_sm", "inline_traversal")}})
             scene.close()
     value = statistics.mean(r["frames"]["megakernel_fp64"]["mpaths_per_s"] for r in results)
     line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": 1, "steps": args.steps, "warmup": 0,
@@ -664,10 +666,11 @@ def main():
             "data": "synthetic (seeded scene files in the reference's formats)",
             "config": config(args.method, world),
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+            "steps_ms": step_ms,
             "mrays_per_s": world * counts["rays"] * args.steps / total_s / 1e6,
             "gpu_launches": args.steps,
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": frame_bytes,
-                    "d2h_bytes_per_step": frame_bytes, "ms_per_step": statistics.mean(e2e_ms),
+                    "d2h_bytes_per_step": frame_bytes, "ms_per_step": statistics.mean(e2e_ms), "steps_ms": e2e_ms,
                     "clocks": e2e_clocks.summary()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

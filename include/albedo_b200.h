@@ -275,7 +275,7 @@ typedef struct albedo_tuning {
     int32_t slot_count;           /* wavefront: path slots */
     int32_t evaluations;          /* shapes timed */
     int32_t inline_traversal;     /* megakernel: 1 = traversal inlined into the kernel (3 blocks per SM;
-                                     path estimator with FP64 sums), 0 = one out-of-line copy */
+                                     path estimator), 0 = one out-of-line copy */
     double best_ms;               /* the kept shape's time on the tuning work */
     double default_ms;            /* the default shape's time on the same work */
 } albedo_tuning;
