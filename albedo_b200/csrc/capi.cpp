@@ -159,6 +159,26 @@ void download(T* host, const DeviceBuffer& buffer, std::size_t count)
     }
 }
 
+// The staging buffer of albedo_render_host on one device.
+struct HostStaging {
+    std::mutex mutex;
+    DeviceBuffer buffer;
+};
+
+HostStaging& hostStaging(int device)
+{
+    static std::mutex table_mutex;
+    // Never destroyed: freeing device memory from a static destructor at exit
+    // would run after the CUDA runtime has shut down.
+    static auto* table{new std::map<int, std::unique_ptr<HostStaging>>};
+    const std::lock_guard lock{table_mutex};
+    std::unique_ptr<HostStaging>& entry{(*table)[device]};
+    if (!entry) {
+        entry = std::make_unique<HostStaging>();
+    }
+    return *entry;
+}
+
 Vec3 vec(const double* v) { return {v[0], v[1], v[2]}; }
 Rgb rgb(const double* v) { return {v[0], v[1], v[2]}; }
 
@@ -812,11 +832,24 @@ int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, 
 {
     return guarded([&] {
         static_cast<void>(renderArgsFor(*scene, *job));
-        const std::size_t pixels{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height)};
-        DeviceBuffer device{uploadRaw(accumulators, pixels)};
-        renderOnDevice(*scene, *job, device.as<PixelAccum>(), nullptr);
-        check(cudaDeviceSynchronize(), "render");
-        download(accumulators, device, pixels);
+        const std::size_t bytes{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height) *
+                                sizeof(PixelAccum)};
+        // One device staging buffer per device, kept and grown as needed: after
+        // the first call of a size, a host render allocates nothing (an
+        // allocation can wait on the driver for as long as a render takes).
+        // Host renders on one device take turns on it.
+        int device{0};
+        check(cudaGetDevice(&device), "cudaGetDevice");
+        HostStaging& staging{hostStaging(device)};
+        const std::lock_guard lock{staging.mutex};
+        if (staging.buffer.bytes < bytes) {
+            staging.buffer = DeviceBuffer{};
+            staging.buffer = DeviceBuffer{bytes};
+        }
+        check(cudaMemcpyAsync(staging.buffer.ptr, accumulators, bytes, cudaMemcpyHostToDevice, nullptr), "upload");
+        renderOnDevice(*scene, *job, staging.buffer.as<PixelAccum>(), nullptr);
+        check(cudaMemcpyAsync(accumulators, staging.buffer.ptr, bytes, cudaMemcpyDeviceToHost, nullptr), "download");
+        check(cudaStreamSynchronize(nullptr), "render");
         scene->collectKernelError();
     });
 }

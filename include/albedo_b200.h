@@ -180,7 +180,10 @@ int albedo_scene_get_info(const albedo_scene* scene, albedo_scene_info* out);
  * is a device array of width*height entries; `stream` is a cudaStream_t (NULL:
  * the default stream). Call albedo_scene_check after synchronizing to collect a
  * kernel-reported error. albedo_render_host takes a host array, copies it in,
- * renders, copies it back and synchronizes. */
+ * renders, copies it back and synchronizes; it stages the array in a device
+ * buffer kept per device (grown to the largest image seen, never freed), so
+ * repeated host renders allocate nothing, and host renders on one device run
+ * one at a time. */
 int albedo_render(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
                   void* stream);
 int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators);
