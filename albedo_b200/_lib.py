@@ -107,6 +107,8 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_probe_lobe_sample": (c_int32, [c_int32, _F, _F, c_int32, _I, _F, _F, _F, _I]),
     "albedo_probe_perlin": (c_int32, [_F, c_int32, _F, _F]),
     "albedo_probe_camera_rays": (c_int32, [c_void_p, c_int32, c_int32, _F, c_int32, _F]),
+    "albedo_probe_trace_modes": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, c_int32, c_int32, _I, _U, _U,
+                                           _U]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -1438,6 +1438,37 @@ int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, fl
     });
 }
 
+int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                             int32_t any, int32_t persistent, int32_t* out_hit, uint32_t* out_t_bits,
+                             uint32_t* out_object_position, uint32_t* out_triangle_position)
+{
+    return guarded([&] {
+        scene->requireCommitted();
+        if (count <= 0 || count > (int64_t{1} << 28)) {
+            throw std::invalid_argument{"ray count must be in 1..2^28"};
+        }
+        const auto n{static_cast<std::size_t>(count)};
+        DeviceBuffer d_rays{uploadRaw(rays, 6 * n)};
+        DeviceBuffer counter{sizeof(int)};
+        DeviceBuffer hit{n * sizeof(int)};
+        DeviceBuffer t{n * sizeof(unsigned int)};
+        DeviceBuffer obj{n * sizeof(unsigned int)};
+        DeviceBuffer tri{n * sizeof(unsigned int)};
+        check(cudaMemset(counter.ptr, 0, sizeof(int)), "cudaMemset");
+        check(launchTraceModes(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max, any != 0,
+                               persistent != 0, scene->stack_capacity, counter.as<int>(),
+                               scene->error_flag.as<unsigned int>(), hit.as<int>(), t.as<unsigned int>(),
+                               obj.as<unsigned int>(), tri.as<unsigned int>(), nullptr),
+              "probe");
+        check(cudaDeviceSynchronize(), "probe");
+        download(out_hit, hit, n);
+        download(out_t_bits, t, n);
+        download(out_object_position, obj, n);
+        download(out_triangle_position, tri, n);
+        scene->collectKernelError();
+    });
+}
+
 int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film, int32_t count,
                              float* out_rays)
 {

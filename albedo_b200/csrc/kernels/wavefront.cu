@@ -455,7 +455,86 @@ __global__ void appendFinishKernel(WfBuffers b, int first, int count, unsigned l
     ctl->job_count = first + count;
 }
 
+// Probe: queries of given rays traced either as the wavefront traces them
+// (persistent, warp fetch, node-then-leaf steps) or one query per thread through
+// the shared out-of-line traversal, writing the raw hits (hit flag, FP32 t bits,
+// object leaf position, triangle table position) for a bit-for-bit comparison.
+template <int STACK>
+__global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const DevScene scene, const float* rays,
+                                                                         int count, float t_min, float t_max,
+                                                                         bool any, bool persistent, int* counter,
+                                                                         unsigned int* error_flag, int* out_hit,
+                                                                         unsigned int* out_t, unsigned int* out_obj,
+                                                                         unsigned int* out_tri)
+{
+    extern __shared__ uint2 stack[];
+    uint2* const lane_stack = stack + threadIdx.x;
+    const int stride = static_cast<int>(blockDim.x);
+    const auto store = [&](int i, bool found, const TraceHit& hit) {
+        out_hit[i] = found ? 1 : 0;
+        out_t[i] = found ? __float_as_uint(hit.t) : 0u;
+        out_obj[i] = found ? hit.obj_pos : kNoPrim;
+        out_tri[i] = found ? hit.tri_pos : kNoPrim;
+    };
+    if (!persistent) {
+        const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+        if (i < count) {
+            TraceHit hit;
+            float tmax = t_max;
+            const float3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+            const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+            const bool found = traceQuery(scene, o, d, t_min, tmax, SkipRule::none(), hit, lane_stack, stride, STACK,
+                                          error_flag, nullptr, any);
+            store(i, found, hit);
+        }
+        return;
+    }
+    WarpFetch fetch{0, 0, 32, false};
+    TraceState q;
+    int i = -1;
+    bool active = false;
+    for (;;) {
+        const int next = fetch.take(counter, count, !active);
+        bool finished = false;
+        if (next >= 0) {
+            i = next;
+            const float3 o = mk(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+            const float3 d = mk(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+            active = traceBegin(scene, q, o, d, t_min, t_max);
+            finished = !active;
+        }
+        if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
+            break;
+        }
+        if (active && !traceAdvance(scene, q, SkipRule::none(), lane_stack, stride, STACK, error_flag, nullptr, any)) {
+            active = false;
+            finished = true;
+        }
+        if (finished) {
+            store(i, q.found, q.hit);
+        }
+    }
+}
+
 } // namespace
+
+cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count, float t_min, float t_max, bool any,
+                             bool persistent, int stack, int* counter, unsigned int* error_flag, int* out_hit,
+                             unsigned int* out_t, unsigned int* out_obj, unsigned int* out_tri, cudaStream_t stream)
+{
+    return withStack(stack, [&](auto size) {
+        constexpr int S = decltype(size)::value;
+        const std::size_t smem = static_cast<std::size_t>(S) * 128 * sizeof(uint2);
+        const cudaError_t e = allowStackMemory(traceModesKernel<S>, S);
+        if (e != cudaSuccess) {
+            return e;
+        }
+        const int blocks = persistent ? 148 * 4 : (count + 127) / 128;
+        traceModesKernel<S><<<blocks, 128, smem, stream>>>(scene, rays, count, t_min, t_max, any, persistent, counter,
+                                                           error_flag, out_hit, out_t, out_obj, out_tri);
+        return cudaGetLastError();
+    });
+}
 
 cudaError_t wfPrepare(int stack)
 {

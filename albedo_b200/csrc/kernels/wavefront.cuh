@@ -109,6 +109,12 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
 // Blocks per SM of the persistent traversal kernels that fit at once with
 // `stack` entries per thread (after wfPrepare).
 cudaError_t wfTraceBlocksPerSm(int stack, int* out);
+// Probe for parity tests: closest-hit (any = false) or any-hit queries of given
+// rays, traced the wavefront's way (persistent = true; `counter` is an int
+// zeroed before the launch) or one query per thread, writing raw hits.
+cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count, float t_min, float t_max, bool any,
+                             bool persistent, int stack, int* counter, unsigned int* error_flag, int* out_hit,
+                             unsigned int* out_t, unsigned int* out_obj, unsigned int* out_tri, cudaStream_t stream);
 cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
                         cudaStream_t stream);
 // Appends jobs [first, first + count) of the (already uploaded) job table to a

@@ -343,6 +343,14 @@ int albedo_probe_lobe_sample(int32_t kind, const float* params, const float* inp
 int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, float* out_turbulence);
 int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film,
                              int32_t count, float* out_rays);
+/* Closest-hit (any = 0) or any-hit queries of given rays, traced as the
+ * wavefront's persistent kernels trace them (persistent = 1) or one query per
+ * thread through the shared traversal (persistent = 0): raw hit flag, FP32 t
+ * bits, object leaf position and triangle table position (0xFFFFFFFF if none),
+ * so that tests can compare the two ways bit for bit. */
+int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
+                             int32_t any, int32_t persistent, int32_t* out_hit, uint32_t* out_t_bits,
+                             uint32_t* out_object_position, uint32_t* out_triangle_position);
 
 #ifdef __cplusplus
 }

@@ -249,3 +249,36 @@ def test_images_match_reference_at_equal_spp(which, width, height, n, depth, roo
     assert np.mean(np.abs(z) > 4) < 0.005, np.mean(np.abs(z) > 4)
     rel = np.abs(ours.mean() - theirs.mean()) / theirs.mean()
     assert rel < 0.01, rel
+
+
+def trace_modes(scene, rays, any_hit, persistent, t_max=float("inf")):
+    from ctypes import POINTER, c_float, c_int32, c_uint32
+
+    n = len(rays)
+    rays = np.ascontiguousarray(rays, dtype=np.float32)
+    out = {"hit": np.zeros(n, np.int32), "t": np.zeros(n, np.uint32), "object": np.zeros(n, np.uint32),
+           "triangle": np.zeros(n, np.uint32)}
+    lib = ab._lib.library()
+    status = lib.albedo_probe_trace_modes(
+        scene.handle, rays.ctypes.data_as(POINTER(c_float)), n, 0.0, t_max, int(any_hit), int(persistent),
+        out["hit"].ctypes.data_as(POINTER(c_int32)), out["t"].ctypes.data_as(POINTER(c_uint32)),
+        out["object"].ctypes.data_as(POINTER(c_uint32)), out["triangle"].ctypes.data_as(POINTER(c_uint32)))
+    assert status == 0, ab._lib.library().albedo_last_error()
+    return out
+
+
+@pytest.mark.parametrize("which", ["room", "trefoil"])
+@pytest.mark.parametrize("any_hit", [False, True])
+def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, room_path, trefoil_path):
+    """The wavefront's persistent kernels (warp fetch, node-then-leaf steps) trace
+    every query with the same steps as the per-thread traversal the ray-query
+    tests compare with the reference: hit flags, FP32 t, object and triangle are
+    identical bit for bit, for closest-hit and any-hit queries."""
+    scene = ab.Scene.load(room_path if which == "room" else trefoil_path)
+    rays = random_rays(100_000, 12, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    t_max = 3.0 if any_hit else float("inf")
+    per_thread = trace_modes(scene, rays, any_hit, False, t_max)
+    persistent = trace_modes(scene, rays, any_hit, True, t_max)
+    assert 0.05 < per_thread["hit"].mean() < 1.0
+    for key in ("hit", "t", "object", "triangle"):
+        np.testing.assert_array_equal(persistent[key], per_thread[key], err_msg=key)
