@@ -458,6 +458,9 @@ struct albedo_server {
     };
 
     std::unique_ptr<WavefrontEngine> engine;
+    // The engine's traversal error flag: the server's own, since requests of
+    // any scene share the engine and scenes may be released and destroyed.
+    DeviceBuffer error_flag;
     std::int64_t budget{0};
     std::int64_t used{0};
     int stack{32};
@@ -491,7 +494,7 @@ struct albedo_server {
             }
             if (!engine->isOpen()) {
                 stack = std::max(stack, head_stack);
-                engine->open(stack, head.scene->error_flag.as<unsigned int>());
+                engine->open(stack, error_flag.as<unsigned int>());
                 submitted_in_batch = 0;
             }
             used += need;
@@ -868,7 +871,9 @@ int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* str
             jobs.push_back(wavefrontJob(*item.scene, item.job, reinterpret_cast<PixelAccum*>(item.accumulators)));
             stack = std::max(stack, item.scene->stack_capacity);
         }
+        // The batch reports a traversal error through its first job's scene.
         runWavefront(jobs, stack, items[0].scene->error_flag.as<unsigned int>(), static_cast<cudaStream_t>(stream));
+        items[0].scene->collectKernelError();
     });
 }
 
@@ -1091,6 +1096,8 @@ int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo
         try {
             server->engine = std::make_unique<WavefrontEngine>(slot_count, kBatchJobCapacity);
             server->engine->setShape(engineShape());
+            server->error_flag = DeviceBuffer{sizeof(unsigned int)};
+            check(cudaMemset(server->error_flag.ptr, 0, sizeof(unsigned int)), "cudaMemset");
         } catch (const std::bad_alloc&) {
             throw;
         } catch (const std::exception& e) {
@@ -1173,6 +1180,14 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
             throw;
         } catch (const std::exception& e) {
             throw DeviceError{e.what()};
+        }
+        // A traversal stack overflow in any request (none can happen with the
+        // stack the engine sizes for its scenes) is reported, once, here.
+        unsigned int flag{0};
+        check(cudaMemcpy(&flag, server->error_flag.ptr, sizeof(flag), cudaMemcpyDeviceToHost), "error flag");
+        if (flag != 0) {
+            check(cudaMemset(server->error_flag.ptr, 0, sizeof(flag)), "cudaMemset");
+            throw TraversalError{"a traversal stack overflowed in a served request; the affected rays were ended"};
         }
     });
 }
