@@ -980,6 +980,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         TuneTimer timer;
         const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {2, 3, 4}},
                                           {"fetch_batch", {16, 32, 64, 128}},
+                                          {"trace_loop", {0, 1}},
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
                                           {"slot_count", {1 << 19, 1 << 20, 1 << 21}}};
@@ -993,17 +994,18 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
             WfShape shape{};
             shape.trace_blocks_per_sm = v[0];
             shape.fetch_batch = v[1];
-            shape.blocks_per_sm = v[2];
-            shape.iterations_per_graph = v[3];
+            shape.trace_loop = v[2];
+            shape.blocks_per_sm = v[3];
+            shape.iterations_per_graph = v[4];
             const std::lock_guard lock{g_engine_mutex};
-            if (g_engine && g_engine->slotCount() != v[4]) {
+            if (g_engine && g_engine->slotCount() != v[5]) {
                 g_engine.reset();
             }
-            g_engine_slots = v[4];
+            g_engine_slots = v[5];
             g_engine_shape = shape;
         };
         const std::vector<int> start{kept_shape.trace_blocks_per_sm > 0 ? kept_shape.trace_blocks_per_sm : 4,
-                                     kept_shape.fetch_batch, kept_shape.blocks_per_sm,
+                                     kept_shape.fetch_batch, kept_shape.trace_loop, kept_shape.blocks_per_sm,
                                      kept_shape.iterations_per_graph, kept_slots};
         TuneOutcome outcome;
         try {
@@ -1021,9 +1023,10 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         }
         out->trace_blocks_per_sm = outcome.best[0];
         out->fetch_batch = outcome.best[1];
-        out->blocks_per_sm = outcome.best[2];
-        out->iterations_per_graph = outcome.best[3];
-        out->slot_count = outcome.best[4];
+        out->trace_loop = outcome.best[2];
+        out->blocks_per_sm = outcome.best[3];
+        out->iterations_per_graph = outcome.best[4];
+        out->slot_count = outcome.best[5];
         fillTuning(out, outcome);
     });
 }
@@ -1052,10 +1055,14 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
             shape->iterations_per_graph <= 0 || shape->slot_count <= 0) {
             throw std::invalid_argument{"wavefront shape values must be positive"};
         }
+        if (shape->trace_loop != 0 && shape->trace_loop != 1) {
+            throw std::invalid_argument{"the traversal turn shape must be 0 or 1"};
+        }
         WfShape next{};
         next.blocks_per_sm = shape->blocks_per_sm;
         next.trace_blocks_per_sm = shape->trace_blocks_per_sm;
         next.fetch_batch = shape->fetch_batch;
+        next.trace_loop = shape->trace_loop;
         next.iterations_per_graph = shape->iterations_per_graph;
         const std::lock_guard lock{g_engine_mutex};
         if (g_engine && g_engine->slotCount() != shape->slot_count) {
@@ -1079,6 +1086,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out)
         const std::lock_guard lock{g_engine_mutex};
         out->trace_blocks_per_sm = g_engine_shape.trace_blocks_per_sm;
         out->fetch_batch = g_engine_shape.fetch_batch;
+        out->trace_loop = g_engine_shape.trace_loop;
         out->blocks_per_sm = g_engine_shape.blocks_per_sm;
         out->iterations_per_graph = g_engine_shape.iterations_per_graph;
         out->slot_count = g_engine_slots;
@@ -1470,8 +1478,11 @@ int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64
         DeviceBuffer obj{n * sizeof(unsigned int)};
         DeviceBuffer tri{n * sizeof(unsigned int)};
         check(cudaMemset(counter.ptr, 0, sizeof(int)), "cudaMemset");
+        if (persistent < 0 || persistent > 2) {
+            throw std::invalid_argument{"persistent must be 0, 1 or 2"};
+        }
         check(launchTraceModes(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max, any != 0,
-                               persistent != 0, scene->stack_capacity, counter.as<int>(),
+                               persistent, scene->stack_capacity, counter.as<int>(),
                                scene->error_flag.as<unsigned int>(), hit.as<int>(), t.as<unsigned int>(),
                                obj.as<unsigned int>(), tri.as<unsigned int>(), nullptr),
               "probe");

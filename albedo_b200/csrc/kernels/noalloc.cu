@@ -141,7 +141,7 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
         (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
         return e;
     }
-    const WfLaunch launch{blocks, 128, stack, per_sm * sms, 32};
+    const WfLaunch launch{blocks, 128, stack, per_sm * sms, 32, 0};
     // A slot finishes its pixel within n^2 (max_depth + 2) iterations.
     const unsigned long long bound = static_cast<unsigned long long>(job.samples_per_axis) * job.samples_per_axis *
                                          static_cast<unsigned long long>(job.max_depth + 2) +

@@ -529,19 +529,33 @@ __device__ __forceinline__ bool popNext(TraceState& q, const uint2* stack, int s
     }
 }
 
-// Runs one query to its end: descends through interior nodes, then handles the
-// leaf reached, so that the lanes of a warp move through each phase together.
-// Returns whether the query has more work (false: finished).
+// One turn of a query in a persistent kernel; returns whether the query has more
+// work (false: finished). LOOP picks how much a turn does (the wavefront's
+// autotuner chooses per workload; both visit the same nodes and leaves in the
+// same order):
+//   kLoopNodesThenLeaf  descend through interior nodes, then handle the leaf
+//                       reached, so the lanes of a warp move through each phase
+//                       together;
+//   kLoopOneStep        one node or one leaf, so lanes return to take new rays
+//                       sooner.
+enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1 };
+
+template <int LOOP>
 __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, uint2* stack,
                                              int stride, int stack_size, unsigned int* error_flag,
                                              TraversalCounts* counts, bool any)
 {
     int step = kStepDescend;
-    while (step == kStepDescend && (q.ref & kLeafBit) == 0u) {
-        step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
-    }
-    if (step == kStepDescend) {
-        step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+    if constexpr (LOOP == kLoopOneStep) {
+        step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
+                                        : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+    } else {
+        while (step == kStepDescend && (q.ref & kLeafBit) == 0u) {
+            step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
+        }
+        if (step == kStepDescend) {
+            step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+        }
     }
     if (step == kStepFinished) {
         return false;

@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
 // whose query ends files the result and takes the next queued ray, so a warp is
 // not held by its slowest ray. Each query runs the same traversal steps, in the
 // same order, as a query traced alone.
-template <int STACK>
+template <int STACK, int LOOP>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
                                                                         unsigned int* error_flag, int fetch_batch)
 {
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJ
         if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
             break;
         }
-        if (active && !traceAdvance(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, false)) {
+        if (active && !traceAdvance<LOOP>(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, false)) {
             active = false;
             finished = true;
         }
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(128) shadeKernel(const WfJob* __restrict__ job
 
 // Any-hit test of every shadow candidate; unoccluded candidates are added to
 // their path. Persistent, like extendKernel.
-template <int STACK>
+template <int STACK, int LOOP>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
                                                                         unsigned int* error_flag, int fetch_batch)
 {
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJ
         if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
             break;
         }
-        if (active && !traceAdvance(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, true)) {
+        if (active && !traceAdvance<LOOP>(*scene, q, skip, lane_stack, stride, STACK, error_flag, nullptr, true)) {
             active = false;
             finished = true;
         }
@@ -462,7 +462,7 @@ __global__ void appendFinishKernel(WfBuffers b, int first, int count, unsigned l
 template <int STACK>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const DevScene scene, const float* rays,
                                                                          int count, float t_min, float t_max,
-                                                                         bool any, bool persistent, int* counter,
+                                                                         bool any, int mode, int* counter,
                                                                          unsigned int* error_flag, int* out_hit,
                                                                          unsigned int* out_t, unsigned int* out_obj,
                                                                          unsigned int* out_tri)
@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const
         out_obj[i] = found ? hit.obj_pos : kNoPrim;
         out_tri[i] = found ? hit.tri_pos : kNoPrim;
     };
-    if (!persistent) {
+    if (mode == 0) {
         const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
         if (i < count) {
             TraceHit hit;
@@ -506,7 +506,14 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const
         if (__ballot_sync(0xFFFFFFFFu, active || finished) == 0u) {
             break;
         }
-        if (active && !traceAdvance(scene, q, SkipRule::none(), lane_stack, stride, STACK, error_flag, nullptr, any)) {
+        bool more = false;
+        if (active) {
+            more = mode == 2 ? traceAdvance<kLoopOneStep>(scene, q, SkipRule::none(), lane_stack, stride, STACK,
+                                                          error_flag, nullptr, any)
+                             : traceAdvance<kLoopNodesThenLeaf>(scene, q, SkipRule::none(), lane_stack, stride,
+                                                                STACK, error_flag, nullptr, any);
+        }
+        if (active && !more) {
             active = false;
             finished = true;
         }
@@ -519,7 +526,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const
 } // namespace
 
 cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count, float t_min, float t_max, bool any,
-                             bool persistent, int stack, int* counter, unsigned int* error_flag, int* out_hit,
+                             int mode, int stack, int* counter, unsigned int* error_flag, int* out_hit,
                              unsigned int* out_t, unsigned int* out_obj, unsigned int* out_tri, cudaStream_t stream)
 {
     return withStack(stack, [&](auto size) {
@@ -529,8 +536,8 @@ cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count
         if (e != cudaSuccess) {
             return e;
         }
-        const int blocks = persistent ? 148 * 4 : (count + 127) / 128;
-        traceModesKernel<S><<<blocks, 128, smem, stream>>>(scene, rays, count, t_min, t_max, any, persistent, counter,
+        const int blocks = mode != 0 ? 148 * 4 : (count + 127) / 128;
+        traceModesKernel<S><<<blocks, 128, smem, stream>>>(scene, rays, count, t_min, t_max, any, mode, counter,
                                                            error_flag, out_hit, out_t, out_obj, out_tri);
         return cudaGetLastError();
     });
@@ -540,8 +547,14 @@ cudaError_t wfPrepare(int stack)
 {
     return withStack(stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        const cudaError_t e = allowStackMemory(extendKernel<S>, S);
-        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S>, S);
+        cudaError_t e = allowStackMemory(extendKernel<S, kLoopNodesThenLeaf>, S);
+        if (e == cudaSuccess) {
+            e = allowStackMemory(shadowKernel<S, kLoopNodesThenLeaf>, S);
+        }
+        if (e == cudaSuccess) {
+            e = allowStackMemory(extendKernel<S, kLoopOneStep>, S);
+        }
+        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S, kLoopOneStep>, S);
     });
 }
 
@@ -553,9 +566,10 @@ cudaError_t wfTraceBlocksPerSm(int stack, int* out)
         const std::size_t smem = static_cast<std::size_t>(S) * 128 * sizeof(uint2);
         int extend = 0;
         int shadow = 0;
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend, extendKernel<S>, 128, smem);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend, extendKernel<S, kLoopNodesThenLeaf>,
+                                                                      128, smem);
         if (e == cudaSuccess) {
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow, shadowKernel<S>, 128, smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow, shadowKernel<S, kLoopNodesThenLeaf>, 128, smem);
         }
         const int blocks = extend < shadow ? extend : shadow;
         *out = blocks > 0 ? blocks : 1;
@@ -589,7 +603,11 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     regenKernel<<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        extendKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        if (launch.trace_loop == kLoopOneStep) {
+            extendKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        } else {
+            extendKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        }
         return 0;
     });
     shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
@@ -598,7 +616,11 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
-        shadowKernel<S><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        if (launch.trace_loop == kLoopOneStep) {
+            shadowKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        } else {
+            shadowKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+        }
         return 0;
     });
     advanceKernel<<<1, 1, 0, stream>>>(b.control);

@@ -91,6 +91,7 @@ struct WfLaunch {
     int stack;        // traversal stack entries per thread
     int trace_blocks; // grid of the persistent traversal kernels (blocks resident at once), or 0 for `blocks`
     int fetch_batch;  // queue entries a traversal warp claims at once (0: 32)
+    int trace_loop;   // traversal turn shape of the persistent kernels (TraceLoop)
 };
 
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call
@@ -110,10 +111,11 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
 // `stack` entries per thread (after wfPrepare).
 cudaError_t wfTraceBlocksPerSm(int stack, int* out);
 // Probe for parity tests: closest-hit (any = false) or any-hit queries of given
-// rays, traced the wavefront's way (persistent = true; `counter` is an int
-// zeroed before the launch) or one query per thread, writing raw hits.
+// rays, traced one query per thread (mode 0) or the wavefront's way (mode 1:
+// nodes then leaf per turn, 2: one step per turn; `counter` is an int zeroed
+// before the launch), writing raw hits.
 cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count, float t_min, float t_max, bool any,
-                             bool persistent, int stack, int* counter, unsigned int* error_flag, int* out_hit,
+                             int mode, int stack, int* counter, unsigned int* error_flag, int* out_hit,
                              unsigned int* out_t, unsigned int* out_obj, unsigned int* out_tri, cudaStream_t stream);
 cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
                         cudaStream_t stream);

@@ -103,7 +103,7 @@ WavefrontEngine::~WavefrontEngine()
 void WavefrontEngine::setShape(const WfShape& shape)
 {
     if (shape.blocks_per_sm <= 0 || shape.iterations_per_graph <= 0 || shape.trace_blocks_per_sm < 0 ||
-        shape.fetch_batch <= 0) {
+        shape.fetch_batch <= 0 || shape.trace_loop < 0 || shape.trace_loop > 1) {
         throw std::invalid_argument{"wavefront launch shape values must be positive"};
     }
     shape_ = shape;
@@ -131,7 +131,8 @@ void WavefrontEngine::open(int stack, unsigned int* error_flag)
     if (shape_.trace_blocks_per_sm > 0) {
         trace_per_sm = std::min(trace_per_sm, shape_.trace_blocks_per_sm);
     }
-    const WfLaunch launch{sm_count_ * shape_.blocks_per_sm, 128, stack, sm_count_ * trace_per_sm, shape_.fetch_batch};
+    const WfLaunch launch{sm_count_ * shape_.blocks_per_sm, 128, stack, sm_count_ * trace_per_sm, shape_.fetch_batch,
+                          shape_.trace_loop};
     cudaGraph_t graph{nullptr};
     cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};

@@ -279,6 +279,9 @@ typedef struct albedo_tuning {
     int32_t evaluations;          /* shapes timed */
     int32_t inline_traversal;     /* megakernel: 1 = traversal inlined into the kernel (3 blocks per SM;
                                      path estimator), 0 = one out-of-line copy */
+    int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
+                                     1 = a turn is one node or one leaf (same steps, same results) */
+    int32_t reserved;
     double best_ms;               /* the kept shape's time on the tuning work */
     double default_ms;            /* the default shape's time on the same work */
 } albedo_tuning;
@@ -288,8 +291,8 @@ typedef struct albedo_tuning {
  * some scenes and slower on others). */
 int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
 /* Tunes the wavefront engine on a batch (coordinate descent over traversal
- * blocks per SM, fetch batch, queue-kernel blocks per SM, iterations per graph
- * and slot count) and keeps the result for the process. */
+ * blocks per SM, fetch batch, traversal turn shape, queue-kernel blocks per SM,
+ * iterations per graph and slot count) and keeps the result for the process. */
 int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_tuning* out);
 /* The shape renders use now: the scene's megakernel shape (scene not NULL) or
  * the process's wavefront shape (scene NULL); timing fields are zero. */
@@ -298,8 +301,9 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
  * (scene not NULL: tile_width 8, 16 or 32, blocks_per_sm 3 or 4, and
  * inline_traversal 0 or 1, the latter with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
- * fetch_batch, iterations_per_graph and slot_count, all positive). Timing fields
- * are ignored. Images do not depend on the shape. */
+ * fetch_batch, iterations_per_graph and slot_count, all positive, and
+ * trace_loop 0 or 1). Timing fields are ignored. Images do not depend on the
+ * shape. */
 int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */
 int albedo_wavefront_last_iterations(int64_t* out);
@@ -344,8 +348,9 @@ int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, fl
 int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film,
                              int32_t count, float* out_rays);
 /* Closest-hit (any = 0) or any-hit queries of given rays, traced as the
- * wavefront's persistent kernels trace them (persistent = 1) or one query per
- * thread through the shared traversal (persistent = 0): raw hit flag, FP32 t
+ * wavefront's persistent kernels trace them (persistent = 1: a turn descends
+ * nodes then handles a leaf; 2: a turn is one step) or one query per thread
+ * through the shared traversal (persistent = 0): raw hit flag, FP32 t
  * bits, object leaf position and triangle table position (0xFFFFFFFF if none),
  * so that tests can compare the two ways bit for bit. */
 int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,

@@ -342,9 +342,9 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
     wave_job = ab.RenderJob(160, 90, samples_per_axis=3, seed=4, max_depth=10, method=ab.WAVEFRONT)
     wave = render(scene, wave_job)
     for shape in (dict(blocks_per_sm=4, trace_blocks_per_sm=2, fetch_batch=16, iterations_per_graph=2,
-                       slot_count=1 << 14),
+                       slot_count=1 << 14, trace_loop=1),
                   dict(blocks_per_sm=16, trace_blocks_per_sm=4, fetch_batch=128, iterations_per_graph=8,
-                       slot_count=1 << 20)):
+                       slot_count=1 << 20, trace_loop=0)):
         ab.set_tuning(**shape)
         np.testing.assert_array_equal(render(scene, wave_job), wave)
     ab.wavefront_configure()

@@ -269,16 +269,18 @@ def trace_modes(scene, rays, any_hit, persistent, t_max=float("inf")):
 
 @pytest.mark.parametrize("which", ["room", "trefoil"])
 @pytest.mark.parametrize("any_hit", [False, True])
-def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, room_path, trefoil_path):
-    """The wavefront's persistent kernels (warp fetch, node-then-leaf steps) trace
-    every query with the same steps as the per-thread traversal the ray-query
-    tests compare with the reference: hit flags, FP32 t, object and triangle are
-    identical bit for bit, for closest-hit and any-hit queries."""
+@pytest.mark.parametrize("mode", [1, 2])
+def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, mode, room_path, trefoil_path):
+    """The wavefront's persistent kernels (warp fetch; a turn descends nodes then
+    handles a leaf, mode 1, or takes one step, mode 2) trace every query with the
+    same steps as the per-thread traversal the ray-query tests compare with the
+    reference: hit flags, FP32 t, object and triangle are identical bit for bit,
+    for closest-hit and any-hit queries."""
     scene = ab.Scene.load(room_path if which == "room" else trefoil_path)
     rays = random_rays(100_000, 12, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
     t_max = 3.0 if any_hit else float("inf")
-    per_thread = trace_modes(scene, rays, any_hit, False, t_max)
-    persistent = trace_modes(scene, rays, any_hit, True, t_max)
+    per_thread = trace_modes(scene, rays, any_hit, 0, t_max)
+    persistent = trace_modes(scene, rays, any_hit, mode, t_max)
     assert 0.05 < per_thread["hit"].mean() < 1.0
     for key in ("hit", "t", "object", "triangle"):
         np.testing.assert_array_equal(persistent[key], per_thread[key], err_msg=key)

@@ -73,9 +73,10 @@ def test_batch_tuning_leaves_accumulators_untouched_and_images_unchanged(room_pa
     assert shape["blocks_per_sm"] in (4, 8, 16)
     assert shape["iterations_per_graph"] in (2, 4, 8)
     assert shape["slot_count"] in (1 << 19, 1 << 20, 1 << 21)
-    assert shape["evaluations"] >= 12 and shape["best_ms"] <= shape["default_ms"]
+    assert shape["trace_loop"] in (0, 1)
+    assert shape["evaluations"] >= 13 and shape["best_ms"] <= shape["default_ms"]
     kept = ab.tuning()
-    assert all(kept[k] == shape[k] for k in ("trace_blocks_per_sm", "fetch_batch", "blocks_per_sm",
+    assert all(kept[k] == shape[k] for k in ("trace_blocks_per_sm", "fetch_batch", "trace_loop", "blocks_per_sm",
                                              "iterations_per_graph", "slot_count"))
     for a in accs:
         a.zero_()
