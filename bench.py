@@ -550,9 +550,10 @@ def run_reference(args, rank: int, world: int) -> None:
 
 def main():
     args = parse_args()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    from albedo_b200.replicas import max_over_ranks, ranks_from_env, whole_job_throughput
+
+    ranks = ranks_from_env()
+    rank, world, local_rank = ranks.rank, ranks.world, ranks.local_rank
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -621,11 +622,8 @@ def main():
     barrier()
     scene.check()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = torch.tensor([sum(step_ms)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(total_ms, op=dist.ReduceOp.MAX)
-    total_s = float(total_ms.item()) / 1e3
-    value = world * PATHS_PER_STEP * args.steps / total_s / 1e6
+    total_s = max_over_ranks(sum(step_ms), dist, "cuda") / 1e3
+    value = whole_job_throughput(PATHS_PER_STEP / 1e6, args.steps, world, total_s)
 
     # End to end through the host-buffer entry point, pinned accumulators.
     host_accum = torch.zeros((WIDTH * HEIGHT, 4), dtype=torch.float64).pin_memory()
@@ -643,10 +641,8 @@ def main():
             e.synchronize()
             e2e_ms.append(s.elapsed_time(e))
     barrier()
-    e2e_total = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(e2e_total, op=dist.ReduceOp.MAX)
-    e2e_value = world * PATHS_PER_STEP * args.steps / (float(e2e_total.item()) / 1e3) / 1e6
+    e2e_value = whole_job_throughput(PATHS_PER_STEP / 1e6, args.steps, world,
+                                     max_over_ranks(sum(e2e_ms), dist, "cuda") / 1e3)
     frame_bytes = WIDTH * HEIGHT * 32
 
     if rank == 0:
