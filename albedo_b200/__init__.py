@@ -401,10 +401,13 @@ def tuning(scene: Scene | None = None) -> dict:
 class Server:
     """Continuous-batching render server (albedo_server_* in the C ABI)."""
 
-    def __init__(self, memory_budget_bytes: int = 150 << 30, slots: int = 1 << 20):
+    def __init__(self, memory_budget_bytes: int = 150 << 30, slots: int = 1 << 20, express_pixels: int = 65536):
+        """`express_pixels`: requests of at most this many pixels may be rendered by the
+        megakernel beside a lightly loaded batch (0: every request joins the batch)."""
         handle = c_void_p()
         _raise(library().albedo_server_create(memory_budget_bytes, slots, byref(handle)))
         self._handle = handle
+        _raise(library().albedo_server_set_express(self._handle, express_pixels))
 
     def submit(self, scene: Scene, job: RenderJob, accumulators_ptr: int, camera: Camera | None = None) -> int:
         c = job.to_c()
@@ -418,6 +421,12 @@ class Server:
         count = c_int32()
         _raise(library().albedo_server_step(self._handle, out, capacity, byref(count)))
         return [out[i] for i in range(count.value)]
+
+    def routes(self) -> tuple[int, int]:
+        """Requests admitted so far (to the batch, to the express route)."""
+        batched, express = ctypes.c_int64(), ctypes.c_int64()
+        _raise(library().albedo_server_routes(self._handle, byref(batched), byref(express)))
+        return batched.value, express.value
 
     def release_scene(self, scene: Scene) -> None:
         """Stops counting `scene` against the budget; it must have no requests left in the server."""

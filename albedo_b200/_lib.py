@@ -92,6 +92,8 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_server_step": (c_int32, [c_void_p, POINTER(c_int64), c_int32, POINTER(c_int32)]),
     "albedo_server_pending": (c_int32, [c_void_p, POINTER(c_int32), POINTER(c_int32)]),
     "albedo_server_release_scene": (c_int32, [c_void_p, c_void_p]),
+    "albedo_server_set_express": (c_int32, [c_void_p, c_int64]),
+    "albedo_server_routes": (c_int32, [c_void_p, POINTER(c_int64), POINTER(c_int64)]),
     "albedo_server_destroy": (None, [c_void_p]),
     "albedo_autotune_megakernel": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(TuningC)]),
     "albedo_autotune_batch": (c_int32, [c_void_p, c_int32, POINTER(TuningC)]),

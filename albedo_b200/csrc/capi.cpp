@@ -454,8 +454,20 @@ struct albedo_server {
         std::int64_t ticket{};
         const albedo_scene* scene{};
         WfJob job{};
+        RenderArgs megakernel_args{}; // the same render as a megakernel launch (express route)
         std::int64_t bytes{};
     };
+    // A request on the express route: rendered by the megakernel on the
+    // server's own stream, done when its event completes.
+    struct Express {
+        std::int64_t ticket{};
+        const albedo_scene* scene{};
+        std::int64_t bytes{};
+        cudaEvent_t done{nullptr};
+    };
+    static constexpr std::size_t kMaxExpress{8};
+    // The wavefront batch counts as lightly loaded below this many pixels in flight.
+    static constexpr std::int64_t kLightPixels{std::int64_t{1} << 18};
 
     std::unique_ptr<WavefrontEngine> engine;
     // The engine's traversal error flag: the server's own, since requests of
@@ -469,6 +481,64 @@ struct albedo_server {
     std::map<int, Request> running; // engine job index -> request
     std::set<const albedo_scene*> resident;
     std::deque<std::int64_t> finished; // tickets not yet handed to the caller
+    std::vector<Express> express;      // in launch order
+    cudaStream_t express_stream{nullptr};
+    std::int64_t express_max_pixels{65536};
+    std::int64_t routed_batch{0};   // requests admitted to the batch so far
+    std::int64_t routed_express{0}; // requests admitted to the express route so far
+
+    albedo_server() = default;
+    albedo_server(const albedo_server&) = delete;
+    albedo_server& operator=(const albedo_server&) = delete;
+    ~albedo_server()
+    {
+        if (express_stream != nullptr) {
+            cudaStreamSynchronize(express_stream);
+            for (const Express& e : express) {
+                cudaEventDestroy(e.done);
+            }
+            cudaStreamDestroy(express_stream);
+        }
+    }
+
+    std::int64_t wavefrontPixels() const
+    {
+        std::int64_t pixels{0};
+        for (const auto& [index, request] : running) {
+            pixels += request.bytes / static_cast<std::int64_t>(sizeof(PixelAccum));
+        }
+        return pixels;
+    }
+
+    // A small request arriving while the batch is lightly loaded goes to the
+    // megakernel: its pixels' samples run in sequence either way, and the
+    // megakernel runs them in one launch where the wavefront needs an
+    // iteration per bounce.
+    bool takesExpress(const Request& r) const
+    {
+        const std::int64_t pixels{r.bytes / static_cast<std::int64_t>(sizeof(PixelAccum))};
+        return express_max_pixels > 0 && pixels <= express_max_pixels && express.size() < kMaxExpress &&
+               wavefrontPixels() < kLightPixels;
+    }
+
+    // Collects finished express renders in order; with `wait_oldest` it first
+    // waits for the oldest.
+    void pollExpress(bool wait_oldest)
+    {
+        for (auto it{express.begin()}; it != express.end();) {
+            const cudaError_t e{wait_oldest && it == express.begin() ? cudaEventSynchronize(it->done)
+                                                                     : cudaEventQuery(it->done)};
+            if (e == cudaErrorNotReady) {
+                ++it;
+                continue;
+            }
+            check(e, "express render");
+            finished.push_back(it->ticket);
+            used -= it->bytes;
+            cudaEventDestroy(it->done);
+            it = express.erase(it);
+        }
+    }
 
     std::int64_t sceneBytes(const albedo_scene* scene) const
     {
@@ -483,6 +553,24 @@ struct albedo_server {
             const std::int64_t need{head.bytes + sceneBytes(head.scene)};
             if (used + need > budget) {
                 return;
+            }
+            if (takesExpress(head)) {
+                check(launchMegakernel(head.scene->dev, head.job.camera, head.megakernel_args, head.job.accum,
+                                       error_flag.as<unsigned int>(), head.scene->stack_capacity, express_stream),
+                      "express render");
+                cudaEvent_t done{nullptr};
+                check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "express event");
+                const cudaError_t recorded{cudaEventRecord(done, express_stream)};
+                if (recorded != cudaSuccess) {
+                    cudaEventDestroy(done);
+                    check(recorded, "express event");
+                }
+                express.push_back({head.ticket, head.scene, head.bytes, done});
+                ++routed_express;
+                used += need;
+                resident.insert(head.scene);
+                waiting.pop_front();
+                continue;
             }
             const int head_stack{head.scene->stack_capacity};
             const bool table_full{submitted_in_batch >= engine->jobCapacity()};
@@ -501,6 +589,7 @@ struct albedo_server {
             resident.insert(head.scene);
             const int index{engine->submit(head.job)};
             ++submitted_in_batch;
+            ++routed_batch;
             running.emplace(index, head);
             waiting.pop_front();
         }
@@ -1106,6 +1195,7 @@ int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo
             server->engine->setShape(engineShape());
             server->error_flag = DeviceBuffer{sizeof(unsigned int)};
             check(cudaMemset(server->error_flag.ptr, 0, sizeof(unsigned int)), "cudaMemset");
+            check(cudaStreamCreateWithFlags(&server->express_stream, cudaStreamNonBlocking), "express stream");
         } catch (const std::bad_alloc&) {
             throw;
         } catch (const std::exception& e) {
@@ -1133,6 +1223,10 @@ int albedo_server_submit_view(albedo_server* server, const albedo_scene* scene, 
     return guarded([&] {
         albedo_server::Request request;
         request.job = wavefrontJob(*scene, *job, reinterpret_cast<PixelAccum*>(accumulators), camera);
+        albedo_render_job as_megakernel{*job};
+        as_megakernel.method = ALBEDO_MEGAKERNEL;
+        as_megakernel.accumulation = ALBEDO_ACCUMULATE_FP64;
+        request.megakernel_args = renderArgsFor(*scene, as_megakernel);
         request.ticket = server->next_ticket++;
         request.scene = scene;
         request.bytes = static_cast<std::int64_t>(job->width) * job->height * static_cast<std::int64_t>(sizeof(PixelAccum));
@@ -1166,7 +1260,11 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
         };
         try {
             server->admit();
-            if (!server->engine->isOpen() || server->running.empty()) {
+            const bool batch_busy{server->engine->isOpen() && !server->running.empty()};
+            // With no batch to advance, wait for the oldest express render.
+            server->pollExpress(!batch_busy && !server->express.empty());
+            if (!batch_busy) {
+                server->admit();
                 report();
                 return;
             }
@@ -1180,6 +1278,7 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
                 server->used -= found->second.bytes;
                 server->running.erase(found);
             }
+            server->pollExpress(false);
             server->admit();
             report();
         } catch (const std::invalid_argument&) {
@@ -1200,13 +1299,33 @@ int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacit
     });
 }
 
+int albedo_server_routes(const albedo_server* server, int64_t* out_batched, int64_t* out_express)
+{
+    return guarded([&] {
+        *out_batched = server->routed_batch;
+        *out_express = server->routed_express;
+    });
+}
+
+int albedo_server_set_express(albedo_server* server, int64_t max_pixels)
+{
+    return guarded([&] {
+        if (max_pixels < 0) {
+            throw std::invalid_argument{"the express route's pixel limit must not be negative"};
+        }
+        server->express_max_pixels = max_pixels;
+    });
+}
+
 int albedo_server_release_scene(albedo_server* server, const albedo_scene* scene)
 {
     return guarded([&] {
         const auto uses = [&](const albedo_server::Request& r) { return r.scene == scene; };
         if (std::any_of(server->waiting.begin(), server->waiting.end(), uses) ||
             std::any_of(server->running.begin(), server->running.end(),
-                        [&](const auto& entry) { return uses(entry.second); })) {
+                        [&](const auto& entry) { return uses(entry.second); }) ||
+            std::any_of(server->express.begin(), server->express.end(),
+                        [&](const albedo_server::Express& e) { return e.scene == scene; })) {
             throw std::invalid_argument{"the scene still has requests waiting or running in the server"};
         }
         if (server->resident.erase(scene) > 0) {
@@ -1220,7 +1339,7 @@ int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int
 {
     return guarded([&] {
         *out_waiting = static_cast<int32_t>(server->waiting.size());
-        *out_running = static_cast<int32_t>(server->running.size());
+        *out_running = static_cast<int32_t>(server->running.size() + server->express.size());
     });
 }
 

@@ -106,7 +106,8 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
     against the plain megakernel serving one request at a time in arrival order.
     Both use autotuned shapes (tuned before the streams start). Latency is
     completion minus arrival (wall clock); throughput is paths over the time from
-    the first arrival to the last completion."""
+    the first arrival to the last completion. The server's batch_mrays_per_s
+    counts the rays its wavefront batch traced (not the express route's)."""
     import torch
 
     import albedo_b200 as ab
@@ -173,6 +174,7 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
             waiting, running = server.pending()
             if waiting == 0 and running == 0 and submitted < len(reqs):
                 time.sleep(max(0.0, arrivals[submitted] - (time.perf_counter() - start)))
+        routes = server.routes()
         server.close()
         lat_server = np.array([done_at[k] - arrivals[k] for k in range(len(reqs))])
         span_server = max(done_at.values()) - arrivals[0]
@@ -192,7 +194,8 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
         span_mega = finish[-1] - arrivals[0]
         results.append({
             "rate_per_s": rate, "requests": len(reqs), "paths": paths,
-            "server": {"mpaths_per_s": paths / span_server / 1e6, "mrays_per_s": rays / span_server / 1e6,
+            "server": {"mpaths_per_s": paths / span_server / 1e6, "batch_mrays_per_s": rays / span_server / 1e6,
+                       "routed_batch": routes[0], "routed_express": routes[1],
                        "p50_ms": float(np.percentile(lat_server, 50) * 1e3),
                        "p99_ms": float(np.percentile(lat_server, 99) * 1e3)},
             "megakernel_one_at_a_time": {"mpaths_per_s": paths / span_mega / 1e6,

@@ -234,9 +234,13 @@ int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* jo
  * the budget: the engine's path slots and queues, each scene's tables (counted
  * once; scenes stay resident) and each running request's accumulators. Admitted
  * requests join the batch already on the device between graph launches, so
- * their work overlaps the work of requests admitted before them; each result
- * is the image the same request would get alone. No counterpart in the
- * reference, which renders one image per process. */
+ * their work overlaps the work of requests admitted before them. A small
+ * request admitted while the batch is lightly loaded takes the express route
+ * instead: the megakernel renders it on the server's own stream, beside the
+ * batch (a pixel's samples run in sequence either way, and the megakernel runs
+ * them in one launch). Each result is the image the same request would get
+ * alone: the same paths, equal within the tolerance between the two forms. No
+ * counterpart in the reference, which renders one image per process. */
 typedef struct albedo_server albedo_server;
 int albedo_server_create(int64_t memory_budget_bytes, int32_t slot_count, albedo_server** out);
 /* Queues a request (committed scene, job, device accumulators) and admits what
@@ -251,6 +255,11 @@ int albedo_server_submit_view(albedo_server* server, const albedo_scene* scene, 
  * reported by later calls. */
 int albedo_server_step(albedo_server* server, int64_t* finished, int32_t capacity, int32_t* out_finished);
 int albedo_server_pending(const albedo_server* server, int32_t* out_waiting, int32_t* out_running);
+/* The express route's limit: requests of at most `max_pixels` pixels may take
+ * it (default 65,536); 0 sends every request to the batch. */
+int albedo_server_set_express(albedo_server* server, int64_t max_pixels);
+/* Requests admitted so far to the batch and to the express route. */
+int albedo_server_routes(const albedo_server* server, int64_t* out_batched, int64_t* out_express);
 /* Stops counting a scene's tables against the server's budget (and admits what
  * then fits). The server counts each scene once, from its first admitted
  * request until this call; call it before destroying a scene the server has

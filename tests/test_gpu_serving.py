@@ -1,5 +1,5 @@
-"""The render server: continuous batching gives each request the image it gets
-alone (GPU).
+"""The render server: continuous batching (and the express route beside it)
+gives each request the image it gets alone (GPU).
 
 Requests are submitted while others are already running on the device; each
 finished result is compared with the same job rendered alone, with the wavefront
@@ -64,12 +64,17 @@ def serve(server, items, stagger=True):
     return [a.cpu().numpy() for a in accs]
 
 
-def test_each_request_is_the_same_alone_and_in_the_mix(room_path, trefoil_path):
+@pytest.mark.parametrize("express_pixels", [0, 65536])
+def test_each_request_is_the_same_alone_and_in_the_mix(room_path, trefoil_path, express_pixels):
+    """express_pixels 0: every request joins the batch on the device; 65536: small
+    requests arriving while the batch is light take the megakernel route beside it."""
     room, trefoil = ab.Scene.load(room_path), ab.Scene.load(trefoil_path)
     items = requests(room, trefoil)
-    server = ab.Server(memory_budget_bytes=8 << 30, slots=1 << 16)
+    server = ab.Server(memory_budget_bytes=8 << 30, slots=1 << 16, express_pixels=express_pixels)
     results = serve(server, items)
     assert server.pending() == (0, 0)
+    batched, express = server.routes()
+    assert batched + express == len(items) and (express == 0) == (express_pixels == 0)
     for (scene, job), result in zip(items, results):
         assert_same_image(result, alone(scene, job))
     server.close()
@@ -84,7 +89,7 @@ def test_requests_wait_for_memory_and_still_match(room_path, trefoil_path):
     slot_bytes = slots * 232 + (1 << 20)
     scene_bytes = room.info()["device_bytes"] + trefoil.info()["device_bytes"]
     budget = slot_bytes + scene_bytes + 160 * 90 * 32 + 64 * 36 * 32 + (4 << 20)
-    server = ab.Server(memory_budget_bytes=budget, slots=slots)
+    server = ab.Server(memory_budget_bytes=budget, slots=slots, express_pixels=0)
     accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in items]
     for (scene, job), acc in zip(items, accs):
         server.submit(scene, job, acc.data_ptr())
@@ -141,3 +146,29 @@ def test_releasing_a_scene_frees_its_share_of_the_budget(trefoil_path, tmp_path)
     assert_same_image(a.cpu().numpy(), alone(first_scene, job))
     assert_same_image(b.cpu().numpy(), alone(second_scene, job))
     server.close()
+
+
+def test_express_route_runs_beside_a_busy_batch(room_path, trefoil_path):
+    """A large request fills the batch; a small one that arrives then still joins
+    the batch (the batch is not light). Once the batch drains, a small request
+    takes the express route. Every result equals its render alone."""
+    room, trefoil = ab.Scene.load(room_path), ab.Scene.load(trefoil_path)
+    big = ab.RenderJob(640, 480, samples_per_axis=2, seed=3, max_depth=8, method=ab.WAVEFRONT)  # 307,200 pixels
+    small = ab.RenderJob(96, 54, samples_per_axis=3, seed=4, max_depth=10, method=ab.WAVEFRONT)
+    server = ab.Server(memory_budget_bytes=8 << 30, slots=1 << 19, express_pixels=65536)
+    jobs = [(room, big), (trefoil, small), (trefoil, small)]
+    accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in jobs]
+    t0 = server.submit(room, big, accs[0].data_ptr())
+    t1 = server.submit(trefoil, small, accs[1].data_ptr())
+    done = []
+    while t0 not in done or t1 not in done:
+        done += server.step()
+    assert server.routes() == (2, 0)
+    t2 = server.submit(trefoil, small, accs[2].data_ptr())
+    assert server.routes() == (2, 1)
+    while t2 not in done:
+        done += server.step()
+    torch.cuda.synchronize()
+    server.close()
+    for (scene, job), acc in zip(jobs, accs):
+        assert_same_image(acc.cpu().numpy(), alone(scene, job))
