@@ -510,15 +510,20 @@ struct albedo_server {
         return pixels;
     }
 
-    // A small request arriving while the batch is lightly loaded goes to the
-    // megakernel: its pixels' samples run in sequence either way, and the
-    // megakernel runs them in one launch where the wavefront needs an
-    // iteration per bounce.
+    // A small request goes to the megakernel when the batch is lightly loaded,
+    // or when it cannot join the batch now (it needs a deeper traversal stack
+    // or the job table is full, so it would wait for the batch to drain): its
+    // pixels' samples run in sequence either way, and the megakernel runs them
+    // in one launch where the wavefront needs an iteration per bounce.
     bool takesExpress(const Request& r) const
     {
         const std::int64_t pixels{r.bytes / static_cast<std::int64_t>(sizeof(PixelAccum))};
-        return express_max_pixels > 0 && pixels <= express_max_pixels && express.size() < kMaxExpress &&
-               wavefrontPixels() < kLightPixels;
+        if (express_max_pixels <= 0 || pixels > express_max_pixels || express.size() >= kMaxExpress) {
+            return false;
+        }
+        const bool batch_blocked{engine->isOpen() && !running.empty() &&
+                                 (r.scene->stack_capacity > stack || submitted_in_batch >= engine->jobCapacity())};
+        return batch_blocked || wavefrontPixels() < kLightPixels;
     }
 
     // Collects finished express renders in order; with `wait_oldest` it first

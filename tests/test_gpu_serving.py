@@ -149,24 +149,28 @@ def test_releasing_a_scene_frees_its_share_of_the_budget(trefoil_path, tmp_path)
 
 
 def test_express_route_runs_beside_a_busy_batch(room_path, trefoil_path):
-    """A large request fills the batch; a small one that arrives then still joins
-    the batch (the batch is not light). Once the batch drains, a small request
+    """A large request fills the batch; a small one of the same scene that arrives
+    then joins the batch (the batch is not light), and a small one needing a
+    deeper traversal stack than the open batch takes the express route rather
+    than wait for the batch to drain. Once the batch drains, a small request
     takes the express route. Every result equals its render alone."""
     room, trefoil = ab.Scene.load(room_path), ab.Scene.load(trefoil_path)
+    assert trefoil.info()["stack_capacity"] > room.info()["stack_capacity"]
     big = ab.RenderJob(640, 480, samples_per_axis=2, seed=3, max_depth=8, method=ab.WAVEFRONT)  # 307,200 pixels
     small = ab.RenderJob(96, 54, samples_per_axis=3, seed=4, max_depth=10, method=ab.WAVEFRONT)
     server = ab.Server(memory_budget_bytes=8 << 30, slots=1 << 19, express_pixels=65536)
-    jobs = [(room, big), (trefoil, small), (trefoil, small)]
+    jobs = [(room, big), (room, small), (trefoil, small), (room, small)]
     accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in jobs]
-    t0 = server.submit(room, big, accs[0].data_ptr())
-    t1 = server.submit(trefoil, small, accs[1].data_ptr())
-    done = []
-    while t0 not in done or t1 not in done:
-        done += server.step()
+    tickets = [server.submit(room, big, accs[0].data_ptr()), server.submit(room, small, accs[1].data_ptr())]
     assert server.routes() == (2, 0)
-    t2 = server.submit(trefoil, small, accs[2].data_ptr())
+    tickets.append(server.submit(trefoil, small, accs[2].data_ptr()))
     assert server.routes() == (2, 1)
-    while t2 not in done:
+    done = []
+    while not all(t in done for t in tickets):
+        done += server.step()
+    tickets.append(server.submit(room, small, accs[3].data_ptr()))
+    assert server.routes() == (2, 2)
+    while tickets[-1] not in done:
         done += server.step()
     torch.cuda.synchronize()
     server.close()
