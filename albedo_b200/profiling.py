@@ -4,8 +4,10 @@
                                    [--accumulation fp64|kahan]
     python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16 [--autotune]
 
-Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene), max
-depth 10, seed 0. With --autotune the launch shape is tuned first (as bench.py
+Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
+--scene icosphere6 (a displaced icosphere of 6 levels, 81,920 triangles), max
+depth 10, seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
+nodes then leaf, 1: one step). With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
 for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel).
@@ -31,6 +33,8 @@ def main() -> None:
     parser.add_argument("--spp", type=int, default=16)
     parser.add_argument("--no-warmup", action="store_true")
     parser.add_argument("--autotune", action="store_true")
+    parser.add_argument("--scene", choices=["trefoil", "icosphere6"], default="trefoil")
+    parser.add_argument("--trace-loop", type=int, choices=[0, 1], default=None)
     parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
                         help="megakernel per-pixel sums: FP64 or Kahan-compensated FP32")
     args = parser.parse_args()
@@ -42,7 +46,15 @@ def main() -> None:
 
     n = int(round(math.sqrt(args.spp)))
     with tempfile.TemporaryDirectory() as tmp:
-        scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
+        if args.scene == "icosphere6":
+            scene = ab.Scene.load(scenes.icosphere_scene(Path(tmp), levels=6))
+        else:
+            scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
+        if args.trace_loop is not None:
+            shape = ab.tuning()
+            ab.set_tuning(blocks_per_sm=shape["blocks_per_sm"], trace_blocks_per_sm=4,
+                          fetch_batch=shape["fetch_batch"], iterations_per_graph=shape["iterations_per_graph"],
+                          slot_count=shape["slot_count"], trace_loop=args.trace_loop)
         method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
         accumulation = ab.ACCUMULATE_KAHAN_FP32 if args.accumulation == "kahan" else ab.ACCUMULATE_FP64
         job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=10, method=method,
