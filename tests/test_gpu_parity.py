@@ -284,3 +284,72 @@ def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, mo
     assert 0.05 < per_thread["hit"].mean() < 1.0
     for key in ("hit", "t", "object", "triangle"):
         np.testing.assert_array_equal(persistent[key], per_thread[key], err_msg=key)
+
+
+TEXTURES = """\
+camera from 0 2.2 6.5  at 0 0.7 0  up 0 1 0  fov 45
+material marble perlin low 0.2 0.15 0.1  high 0.9 0.85 0.8  scale 3  veins 5
+material smoke perlin low 0.05 0.05 0.08  high 0.6 0.6 0.7  scale 8
+material tiles checker even 0.8 0.8 0.8  odd 0.1 0.1 0.1  frequency 2
+material gold conductor eta 0.156 0.424 1.383  k 3.602 2.472 1.915  roughness 0.25
+material frosted dielectric ior 1.5 roughness 0.3
+material veined mix first gold second marble scale 2 veins 6 threshold 0.45
+material cloudy mix first frosted second smoke scale 4 threshold 0.6
+sphere 0 -1000 0 radius 1000 material tiles
+sphere -1.6 0.7 0 radius 0.7 material marble
+sphere 0 0.7 -0.4 radius 0.7 material veined
+sphere 1.6 0.7 0 radius 0.7 material cloudy
+sphere 0.8 0.3 1.2 radius 0.3 material smoke
+area_light 0 4 1 radius 0.8 radiance 6 6 5
+point_light -2 3 3 intensity 2 2 2
+sky nadir 0.1 0.12 0.15 zenith 0.3 0.35 0.45
+"""
+
+
+def test_textured_and_mixed_materials_match_reference_images(tmp_path):
+    """Perlin textures (with and without veins), checker, and mix materials of a
+    conductor or a rough dielectric with a Perlin-textured diffuse: the same
+    per-pixel two-sample test against the reference at equal spp as the other
+    image tests."""
+    path = tmp_path / "textures.scene"
+    path.write_text(TEXTURES)
+    scene = ab.Scene.load(path)
+    width, height, n, depth = 320, 180, 4, 8
+    pixels = _pixel_grid(width, height, 1500, 21)
+    acc, squares = ab.render_pixels(scene, ab.RenderJob(width, height, samples_per_axis=n, max_depth=depth), pixels,
+                                    with_squares=True)
+    rsum, rsq = ref.RefScene(path).render_pixels(width, height, n, pixels, max_depth=depth)
+    samples = n * n
+    ours = np.stack([acc["r"], acc["g"], acc["b"]], axis=1) / samples
+    theirs = rsum / samples
+    var_o = np.maximum(squares / samples - ours**2, 0)
+    var_t = np.maximum(rsq / samples - theirs**2, 0)
+    z = (ours - theirs) / np.sqrt((var_o + var_t) / samples + 1e-12)
+    assert np.mean(np.abs(z) > 4) < 0.005, np.mean(np.abs(z) > 4)
+    assert abs(ours.mean() - theirs.mean()) / theirs.mean() < 0.01
+
+
+def test_textured_and_mixed_materials_same_in_both_forms(tmp_path):
+    """The wavefront's per-class shade kernels (the mix class included) against
+    the megakernel on the textured scene: identical sample counts, image sums
+    within 1e-4, at most 0.5% of pixels beyond 1e-3 relative (the wavefront
+    tests' tolerance)."""
+    import torch
+
+    path = tmp_path / "textures.scene"
+    path.write_text(TEXTURES)
+    scene = ab.Scene.load(path)
+    images = []
+    for method in (ab.MEGAKERNEL, ab.WAVEFRONT):
+        job = ab.RenderJob(160, 90, samples_per_axis=4, seed=3, max_depth=8, method=method)
+        acc = torch.zeros((160 * 90, 4), dtype=torch.float64, device="cuda")
+        ab.render_device(scene, job, acc.data_ptr())
+        torch.cuda.synchronize()
+        scene.check()
+        images.append(acc.cpu().numpy())
+    mega, wave = images
+    np.testing.assert_array_equal(np.ascontiguousarray(wave[:, 3]).view(np.int64),
+                                  np.ascontiguousarray(mega[:, 3]).view(np.int64))
+    assert abs(wave[:, :3].sum() - mega[:, :3].sum()) / mega[:, :3].sum() < 1e-4
+    rel = np.abs(wave[:, :3] - mega[:, :3]) / np.maximum(np.abs(mega[:, :3]), 1e-3)
+    assert np.mean(rel.max(axis=1) > 1e-3) < 0.005
