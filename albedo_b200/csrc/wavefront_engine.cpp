@@ -264,8 +264,22 @@ void WavefrontEngine::render(const std::vector<WfJob>& jobs, int stack, unsigned
     cudaCheck(cudaStreamWaitEvent(stream_, ordering_, 0), "ordering wait");
     open(stack, error_flag);
     try {
-        for (const WfJob& job : jobs) {
-            submit(job);
+        // Longest pixels first: a pixel's samples run in sequence on one slot,
+        // so the jobs with the most samples per pixel are handed out first and
+        // the batch does not end on a tail of their pixels alone. Each job's
+        // image does not depend on the order.
+        std::vector<std::size_t> order(jobs.size());
+        for (std::size_t i{0}; i < order.size(); ++i) {
+            order[i] = i;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) {
+            const auto work = [&](const WfJob& j) {
+                return static_cast<long long>(j.samples_per_axis) * j.samples_per_axis * (j.max_depth + 1);
+            };
+            return work(jobs[a]) > work(jobs[b]);
+        });
+        for (const std::size_t i : order) {
+            submit(jobs[i]);
         }
         while (!in_flight_.empty()) {
             step();
