@@ -1077,7 +1077,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
                                           {"trace_loop", {0, 1}},
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
-                                          {"slot_count", {1 << 19, 1 << 20, 1 << 21}}};
+                                          {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}}};
         const WfShape kept_shape{engineShape()};
         int kept_slots{0};
         {
