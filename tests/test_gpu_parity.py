@@ -174,12 +174,15 @@ def random_rays(count, seed, low, high):
 def test_ray_queries_match(which, room_path, trefoil_path):
     path = room_path if which == "room" else trefoil_path
     scene = ab.Scene.load(path)
-    rays = random_rays(100_000, 5, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    # 10^6 seeded random rays; FP32 traversal against the reference's FP64 may
+    # split a near-tie (two surfaces within rounding of each other, or a ray
+    # grazing a silhouette) the other way: at most 0.02% of rays.
+    rays = random_rays(1_000_000, 5, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
     ours = scene.intersect(rays, geometry=True)
     theirs = ref.RefScene(path).intersect(rays.astype(np.float64))
     same = (ours["hit"] == theirs["hit"]) & ((ours["hit"] == 0) | (ours["object"] == theirs["object"]))
     mismatches = int((~same).sum())
-    assert mismatches <= 20, mismatches
+    assert mismatches <= 200, mismatches
     both = same & (ours["hit"] == 1)
     ulps = ulp_distance(ours["t"][both], theirs["t"][both])
     assert np.mean(ulps <= 2) > 0.999, np.quantile(ulps, [0.5, 0.999, 1.0])
