@@ -594,7 +594,7 @@ cudaError_t wfAppend(const WfBuffers& b, int first, int count, unsigned long lon
 }
 
 cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
-                        cudaStream_t stream)
+                        cudaStream_t stream, const WfSide* side)
 {
     const int g = launch.blocks;
     const int tg = launch.trace_blocks > 0 ? launch.trace_blocks : launch.blocks;
@@ -610,10 +610,33 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         }
         return 0;
     });
-    shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
-    shadeKernel<kClassConductor><<<g, 128, 0, stream>>>(jobs, b);
-    shadeKernel<kClassDielectric><<<g, 128, 0, stream>>>(jobs, b);
-    shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
+    if (side != nullptr) {
+        cudaError_t e = cudaEventRecord(side->fork, stream);
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+            e = cudaStreamWaitEvent(side->stream[k], side->fork, 0);
+        }
+        if (e != cudaSuccess) {
+            return e;
+        }
+        shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
+        shadeKernel<kClassConductor><<<g, 128, 0, side->stream[0]>>>(jobs, b);
+        shadeKernel<kClassDielectric><<<g, 128, 0, side->stream[1]>>>(jobs, b);
+        shadeKernel<kClassMix><<<g, 128, 0, side->stream[2]>>>(jobs, b);
+        for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+            e = cudaEventRecord(side->join[k], side->stream[k]);
+            if (e == cudaSuccess) {
+                e = cudaStreamWaitEvent(stream, side->join[k], 0);
+            }
+        }
+        if (e != cudaSuccess) {
+            return e;
+        }
+    } else {
+        shadeKernel<kClassDiffuse><<<g, 128, 0, stream>>>(jobs, b);
+        shadeKernel<kClassConductor><<<g, 128, 0, stream>>>(jobs, b);
+        shadeKernel<kClassDielectric><<<g, 128, 0, stream>>>(jobs, b);
+        shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
+    }
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
         if (launch.trace_loop == kLoopOneStep) {

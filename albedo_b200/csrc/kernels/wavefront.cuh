@@ -117,8 +117,16 @@ cudaError_t wfTraceBlocksPerSm(int stack, int* out);
 cudaError_t launchTraceModes(const DevScene& scene, const float* rays, int count, float t_min, float t_max, bool any,
                              int mode, int stack, int* counter, unsigned int* error_flag, int* out_hit,
                              unsigned int* out_t, unsigned int* out_obj, unsigned int* out_tri, cudaStream_t stream);
+// Side streams and events for running the per-class shade kernels of an
+// iteration as parallel branches (they touch disjoint slots and push through
+// atomics); without them the kernels run one after another.
+struct WfSide {
+    cudaStream_t stream[3];
+    cudaEvent_t fork;
+    cudaEvent_t join[3];
+};
 cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& launch, unsigned int* error_flag,
-                        cudaStream_t stream);
+                        cudaStream_t stream, const WfSide* side = nullptr);
 // Appends jobs [first, first + count) of the (already uploaded) job table to a
 // running batch: zeroes their completion counters and grows the batch's size.
 cudaError_t wfAppend(const WfBuffers& b, int first, int count, unsigned long long new_total_items,

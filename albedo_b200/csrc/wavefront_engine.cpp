@@ -79,6 +79,11 @@ WavefrontEngine::WavefrontEngine(int slot_count, int job_capacity)
     cudaCheck(cudaGetDevice(&device), "cudaGetDevice");
     cudaCheck(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SM count");
     cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "engine stream");
+    for (int k{0}; k < 3; ++k) {
+        cudaCheck(cudaStreamCreateWithFlags(&side_.stream[k], cudaStreamNonBlocking), "engine side stream");
+        cudaCheck(cudaEventCreateWithFlags(&side_.join[k], cudaEventDisableTiming), "engine event");
+    }
+    cudaCheck(cudaEventCreateWithFlags(&side_.fork, cudaEventDisableTiming), "engine event");
     cudaCheck(cudaEventCreateWithFlags(&ordering_, cudaEventDisableTiming), "engine event");
     cudaCheck(cudaEventCreateWithFlags(&step_done_[0], cudaEventDisableTiming), "engine event");
     cudaCheck(cudaEventCreateWithFlags(&step_done_[1], cudaEventDisableTiming), "engine event");
@@ -93,6 +98,11 @@ WavefrontEngine::~WavefrontEngine()
     cudaEventDestroy(step_done_[0]);
     cudaEventDestroy(step_done_[1]);
     cudaEventDestroy(ordering_);
+    for (int k{0}; k < 3; ++k) {
+        cudaEventDestroy(side_.join[k]);
+        cudaStreamDestroy(side_.stream[k]);
+    }
+    cudaEventDestroy(side_.fork);
     cudaStreamDestroy(stream_);
     cudaFree(slab_);
     cudaFreeHost(staging_jobs_);
@@ -137,7 +147,8 @@ void WavefrontEngine::open(int stack, unsigned int* error_flag)
     cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};
     for (int i{0}; i < shape_.iterations_per_graph && captured == cudaSuccess; ++i) {
-        captured = wfIteration(device_jobs_, buffers_, launch, error_flag, stream_);
+        captured = wfIteration(device_jobs_, buffers_, launch, error_flag, stream_,
+                               parallel_shade_ ? &side_ : nullptr);
     }
     const cudaError_t ended{cudaStreamEndCapture(stream_, &graph)};
     cudaCheck(captured, "wavefront iteration");

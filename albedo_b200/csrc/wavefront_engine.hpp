@@ -68,6 +68,8 @@ public:
 
 private:
     cudaStream_t stream_{nullptr};
+    WfSide side_{};     // branches for the shade kernels
+    bool parallel_shade_{true};
     cudaEvent_t ordering_{nullptr};
     cudaEvent_t step_done_[2]{nullptr, nullptr};
     WfBuffers buffers_{};
