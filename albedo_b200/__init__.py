@@ -8,6 +8,8 @@ of include/albedo_b200.h:
     RenderJob                 RenderJob            (src/albedo/render/render_image.hpp:17-32)
     PixelBuffer               PixelBuffer          (src/albedo/image/pixel_buffer.hpp:17-65)
     render_image              renderImage          (src/albedo/render/render_image.hpp:36-49)
+    resolve_srgb / write_ppm  encodeSrgb, toByte, writePpm (src/albedo/color/srgb.cpp:18-36,
+                              src/albedo/image/ppm.cpp:22-85)
     Scene.intersect/occluded  Scene::intersect / occluded (src/albedo/scene/scene.hpp:69-88)
 
 Errors raise the Python counterpart of the reference's exception: ValueError for
@@ -164,6 +166,11 @@ class PixelBuffer:
         with np.errstate(invalid="ignore", divide="ignore"):
             avg = np.where(count[:, None] > 0, rgb / count[:, None], 0.0)
         return avg.reshape(self.height, self.width, 3)
+
+    def write_ppm(self, path) -> None:
+        """writePpm(path, image): resolved to sRGB bytes on the device."""
+        _raise(library().albedo_save_ppm_host(str(path).encode(), self.pixels.ctypes.data_as(c_void_p),
+                                              self.width, self.height))
 
 
 class Scene:
@@ -336,6 +343,36 @@ def render_device(scene: Scene, job: RenderJob, accumulators_ptr: int, stream: i
     else:
         _raise(library().albedo_render_view(scene.handle, byref(c), _camera_ref(camera), c_void_p(accumulators_ptr),
                                             c_void_p(stream)))
+
+
+def resolve_srgb(accumulators_ptr: int, width: int, height: int, out_ptr: int, stream: int = 0) -> None:
+    """Stream-ordered resolve of width*height device accumulators into
+    width*height*3 device bytes: the sRGB bytes writePpm writes for each pixel's
+    average, rows from the top (image/ppm.cpp:22-33)."""
+    _raise(library().albedo_resolve_srgb(c_void_p(accumulators_ptr), width, height, c_void_p(out_ptr),
+                                         c_void_p(stream)))
+
+
+def srgb_thresholds() -> np.ndarray:
+    """The resolve's table: [b] is the smallest positive double whose byte is at
+    least b (b = 1..255); [0] is -inf."""
+    out = np.empty(256, dtype=np.float64)
+    _raise(library().albedo_srgb_thresholds(out.ctypes.data_as(POINTER(c_double))))
+    return out
+
+
+def write_ppm(path, rgb: np.ndarray) -> None:
+    """writePpm from host sRGB bytes of shape (height, width, 3)."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    if rgb.ndim != 3 or rgb.shape[2] != 3:
+        raise ValueError("rgb must have shape (height, width, 3)")
+    _raise(library().albedo_write_ppm(str(path).encode(), rgb.ctypes.data_as(c_void_p), rgb.shape[1], rgb.shape[0]))
+
+
+def save_ppm(path, accumulators_ptr: int, width: int, height: int, stream: int = 0) -> None:
+    """writePpm for device accumulators: resolved on `stream`, then written."""
+    _raise(library().albedo_save_ppm(str(path).encode(), c_void_p(accumulators_ptr), width, height,
+                                     c_void_p(stream)))
 
 
 def _batch_array(items):
@@ -519,5 +556,6 @@ __all__ = [
     "ACCUMULATE_FP64", "ACCUMULATE_KAHAN_FP32", "ACCUMULATOR_DTYPE", "BasicMaterial", "Camera", "DeviceError",
     "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
     "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
-    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "set_tuning", "trace_work_counts", "tuning", "wavefront_last_rays",
+    "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "resolve_srgb", "save_ppm",
+    "set_tuning", "srgb_thresholds", "trace_work_counts", "tuning", "wavefront_last_rays", "write_ppm",
 ]

@@ -84,6 +84,11 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_trace_counts_host": (c_int32, [c_void_p, _F, c_int64, c_float, c_float, POINTER(c_int64)]),
     "albedo_render_batch": (c_int32, [c_void_p, c_int32, c_void_p]),
     "albedo_render_noalloc": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
+    "albedo_resolve_srgb": (c_int32, [c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
+    "albedo_srgb_thresholds": (c_int32, [_D3]),
+    "albedo_write_ppm": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
+    "albedo_save_ppm": (c_int32, [c_char_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "albedo_save_ppm_host": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "albedo_wavefront_configure": (c_int32, [c_int32, c_int32, c_int32]),
     "albedo_server_create": (c_int32, [c_int64, c_int32, POINTER(c_void_p)]),
     "albedo_server_submit": (c_int32, [c_void_p, c_void_p, POINTER(RenderJobC), c_void_p, POINTER(c_int64)]),

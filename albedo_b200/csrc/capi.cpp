@@ -6,6 +6,7 @@
 #include "autotune.hpp"
 #include "host/flatten.hpp"
 #include "host/scene_file.hpp"
+#include "host/srgb.hpp"
 #include "kernels/launch.hpp"
 #include "wavefront_engine.hpp"
 
@@ -993,6 +994,117 @@ int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* jo
             throw DeviceError{"albedo_render_noalloc made no progress within its iteration bound"};
         }
         check(e, "albedo_render_noalloc");
+    });
+}
+
+namespace {
+
+// PixelBuffer's size check (image/pixel_buffer.hpp:30-38) for the film output calls.
+std::size_t filmPixels(int32_t width, int32_t height)
+{
+    if (width <= 0 || height <= 0 ||
+        static_cast<std::uint64_t>(width) > (std::uint64_t{1} << 28) / static_cast<std::uint64_t>(height)) {
+        throw std::invalid_argument{
+            std::format("invalid image size {}x{}: dimensions must be positive and the image at most {} pixels",
+                        width, height, std::uint64_t{1} << 28)};
+    }
+    return static_cast<std::size_t>(width) * static_cast<std::size_t>(height);
+}
+
+const SrgbThresholds& deviceSrgbTable()
+{
+    static const SrgbThresholds table{[] {
+        SrgbThresholds t{};
+        std::copy(srgbTable().lower.begin(), srgbTable().lower.end(), t.lower);
+        return t;
+    }()};
+    return table;
+}
+
+void resolveOnDevice(const albedo_accumulator* accumulators, std::size_t pixels, uint8_t* out_rgb,
+                     cudaStream_t stream)
+{
+    if (accumulators == nullptr || out_rgb == nullptr) {
+        throw std::invalid_argument{"null accumulator or output pointer"};
+    }
+    if ((reinterpret_cast<std::uintptr_t>(accumulators) & 7) != 0) {
+        throw std::invalid_argument{"accumulators must be 8-byte aligned"};
+    }
+    check(launchResolveSrgb(reinterpret_cast<const PixelAccum*>(accumulators), static_cast<long long>(pixels),
+                            out_rgb, deviceSrgbTable(), stream),
+          "albedo_resolve_srgb");
+}
+
+// Resolves device accumulators into a temporary device buffer, reads the bytes
+// back and writes the file.
+void savePpm(const char* path, const albedo_accumulator* device_accumulators, int32_t width, int32_t height,
+             cudaStream_t stream)
+{
+    if (path == nullptr) {
+        throw std::invalid_argument{"null path"};
+    }
+    const std::size_t pixels{filmPixels(width, height)};
+    DeviceBuffer bytes{3 * pixels};
+    resolveOnDevice(device_accumulators, pixels, bytes.as<uint8_t>(), stream);
+    std::vector<uint8_t> rgb(3 * pixels);
+    check(cudaMemcpyAsync(rgb.data(), bytes.ptr, rgb.size(), cudaMemcpyDeviceToHost, stream), "download");
+    check(cudaStreamSynchronize(stream), "albedo_resolve_srgb");
+    writePpm(path, rgb.data(), width, height);
+}
+
+} // namespace
+
+int albedo_resolve_srgb(const albedo_accumulator* accumulators, int32_t width, int32_t height, uint8_t* out_rgb,
+                        void* stream)
+{
+    return guarded([&] {
+        resolveOnDevice(accumulators, filmPixels(width, height), out_rgb, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int albedo_srgb_thresholds(double* out_lower)
+{
+    return guarded([&] {
+        if (out_lower == nullptr) {
+            throw std::invalid_argument{"null output pointer"};
+        }
+        std::copy(srgbTable().lower.begin(), srgbTable().lower.end(), out_lower);
+    });
+}
+
+int albedo_write_ppm(const char* path, const uint8_t* rgb, int32_t width, int32_t height)
+{
+    return guarded([&] {
+        if (path == nullptr || rgb == nullptr) {
+            throw std::invalid_argument{"null path or pixel pointer"};
+        }
+        writePpm(path, rgb, width, height);
+    });
+}
+
+int albedo_save_ppm(const char* path, const albedo_accumulator* accumulators, int32_t width, int32_t height,
+                    void* stream)
+{
+    return guarded([&] { savePpm(path, accumulators, width, height, static_cast<cudaStream_t>(stream)); });
+}
+
+int albedo_save_ppm_host(const char* path, const albedo_accumulator* accumulators, int32_t width, int32_t height)
+{
+    return guarded([&] {
+        const std::size_t bytes{filmPixels(width, height) * sizeof(PixelAccum)};
+        if (accumulators == nullptr) {
+            throw std::invalid_argument{"null accumulator pointer"};
+        }
+        int device{0};
+        check(cudaGetDevice(&device), "cudaGetDevice");
+        HostStaging& staging{hostStaging(device)};
+        const std::lock_guard lock{staging.mutex};
+        if (staging.buffer.bytes < bytes) {
+            staging.buffer = DeviceBuffer{};
+            staging.buffer = DeviceBuffer{bytes};
+        }
+        check(cudaMemcpyAsync(staging.buffer.ptr, accumulators, bytes, cudaMemcpyHostToDevice, nullptr), "upload");
+        savePpm(path, staging.buffer.as<albedo_accumulator>(), width, height, nullptr);
     });
 }
 

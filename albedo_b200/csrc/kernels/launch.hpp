@@ -115,6 +115,15 @@ cudaError_t launchTrace(const DevScene& scene, const float* rays, int count, flo
 cudaError_t launchOccluded(const DevScene& scene, const float* rays, const float* t_max, int count, int* occluded,
                            unsigned int* error_flag, int stack_capacity, cudaStream_t stream);
 
+// The film's resolve to 8-bit sRGB (3 bytes a pixel) from per-pixel averages,
+// by comparison against a table of the smallest double of each byte (lower[b],
+// b = 1..255; lower[0] is unused).
+struct SrgbThresholds {
+    double lower[256];
+};
+cudaError_t launchResolveSrgb(const PixelAccum* accum, long long pixels, unsigned char* out,
+                              const SrgbThresholds& table, cudaStream_t stream);
+
 // Probe kernels for parity tests of device arithmetic.
 cudaError_t launchPixelStream(unsigned long long seed, int x, int y, int width, int count, unsigned int* out_u32,
                               float* out_real, cudaStream_t stream);

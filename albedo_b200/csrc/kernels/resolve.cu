@@ -1,0 +1,150 @@
+// The film's resolve: per-pixel FP64 accumulators to 8-bit sRGB, 3 bytes a pixel,
+// rows from the top — the bytes the reference's writePpm writes for
+// PixelBuffer::average (image/ppm.cpp:22-33, image/pixel_buffer.cpp:37-45,
+// color/srgb.cpp:18-36).
+//
+// The average is sum / count in FP64 (correctly rounded, as on the host). Its
+// byte comes from a table of 255 thresholds (the smallest double of each byte,
+// computed on the host with the reference's own transfer function): an FP32
+// estimate picks a starting byte and comparisons against the table correct it,
+// so the result is the reference's byte exactly and the kernel evaluates no
+// FP64 power function. A pure stream: 32 bytes read and 3 written per pixel.
+#include "launch.hpp"
+
+#include <algorithm>
+#include <cstdint>
+
+namespace albedo_b200 {
+
+namespace {
+
+constexpr int kResolveThreads{256};
+// Pixels per thread: 4 pixels are 12 output bytes, three aligned 32-bit words.
+constexpr int kResolveGroup{4};
+
+__device__ __forceinline__ unsigned int srgbByteOf(double v, const double* lower)
+{
+    // NaN, zero and negative averages fail the first test; 1.0 and above pass
+    // the second.
+    if (!(v >= lower[1])) {
+        return 0u;
+    }
+    if (v >= lower[255]) {
+        return 255u;
+    }
+    const float f{static_cast<float>(v)};
+    const float e{f <= 0.0031308f ? 12.92f * f : 1.055f * __powf(f, 1.0f / 2.4f) - 0.055f};
+    int b{min(max(__float2int_rn(e * 255.0f), 1), 254)};
+    // lower[1] <= v < lower[255], so both loops end inside [1, 254].
+    while (v < lower[b]) {
+        --b;
+    }
+    while (v >= lower[b + 1]) {
+        ++b;
+    }
+    return static_cast<unsigned int>(b);
+}
+
+__device__ __forceinline__ double averageOf(double sum, long long count)
+{
+    return count == 0 ? 0.0 : sum / static_cast<double>(count);
+}
+
+// ALIGNED: accumulators 16-byte aligned (two 16-byte loads a pixel) and the
+// output 4-byte aligned (word stores); otherwise 8-byte loads and byte stores.
+template <bool ALIGNED>
+__global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const PixelAccum* __restrict__ accum,
+                                                                      long long pixels,
+                                                                      unsigned char* __restrict__ out,
+                                                                      SrgbThresholds table)
+{
+    __shared__ double lower[256];
+    for (int i{static_cast<int>(threadIdx.x)}; i < 256; i += blockDim.x) {
+        lower[i] = table.lower[i];
+    }
+    __syncthreads();
+
+    const long long groups{(pixels + kResolveGroup - 1) / kResolveGroup};
+    const long long stride{static_cast<long long>(gridDim.x) * blockDim.x};
+    for (long long g{static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x}; g < groups; g += stride) {
+        const long long first{g * kResolveGroup};
+        const int n{static_cast<int>(min(static_cast<long long>(kResolveGroup), pixels - first))};
+        unsigned int bytes[3 * kResolveGroup];
+#pragma unroll
+        for (int p{0}; p < kResolveGroup; ++p) {
+            double r{0.0}, gr{0.0}, bl{0.0};
+            long long count{0};
+            if (p < n) {
+                const PixelAccum* a{accum + first + p};
+                if constexpr (ALIGNED) {
+                    const double2 rg{__ldcs(reinterpret_cast<const double2*>(a))};
+                    const double2 bc{__ldcs(reinterpret_cast<const double2*>(a) + 1)};
+                    r = rg.x;
+                    gr = rg.y;
+                    bl = bc.x;
+                    count = __double_as_longlong(bc.y);
+                } else {
+                    r = __ldcs(&a->r);
+                    gr = __ldcs(&a->g);
+                    bl = __ldcs(&a->b);
+                    count = __ldcs(&a->count);
+                }
+            }
+            bytes[3 * p + 0] = srgbByteOf(averageOf(r, count), lower);
+            bytes[3 * p + 1] = srgbByteOf(averageOf(gr, count), lower);
+            bytes[3 * p + 2] = srgbByteOf(averageOf(bl, count), lower);
+        }
+        unsigned char* dst{out + 3 * first};
+        if (ALIGNED && n == kResolveGroup) {
+            unsigned int* words{reinterpret_cast<unsigned int*>(dst)};
+#pragma unroll
+            for (int w{0}; w < 3; ++w) {
+                __stcs(words + w, bytes[4 * w] | bytes[4 * w + 1] << 8 | bytes[4 * w + 2] << 16 |
+                                      bytes[4 * w + 3] << 24);
+            }
+        } else {
+#pragma unroll
+            for (int i{0}; i < 3 * kResolveGroup; ++i) {
+                if (i < 3 * n) {
+                    dst[i] = static_cast<unsigned char>(bytes[i]);
+                }
+            }
+        }
+    }
+}
+
+} // namespace
+
+cudaError_t launchResolveSrgb(const PixelAccum* accum, long long pixels, unsigned char* out,
+                              const SrgbThresholds& table, cudaStream_t stream)
+{
+    if (pixels <= 0) {
+        return cudaSuccess;
+    }
+    int device{0};
+    int sms{0};
+    cudaError_t e{cudaGetDevice(&device)};
+    if (e == cudaSuccess) {
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    }
+    if (e != cudaSuccess) {
+        return e;
+    }
+    // A grid-stride stream, one wave of resident blocks: all of them keep
+    // loads in flight, enough to saturate HBM.
+    const bool aligned{(reinterpret_cast<std::uintptr_t>(accum) & 15) == 0 &&
+                       (reinterpret_cast<std::uintptr_t>(out) & 3) == 0};
+    const auto kernel{aligned ? resolveSrgbKernel<true> : resolveSrgbKernel<false>};
+    int per_sm{0};
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kResolveThreads, 0);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    const long long groups{(pixels + kResolveGroup - 1) / kResolveGroup};
+    const long long wanted{(groups + kResolveThreads - 1) / kResolveThreads};
+    const int blocks{static_cast<int>(std::min(wanted, static_cast<long long>(std::max(per_sm, 1)) * sms))};
+    kernel<<<blocks, kResolveThreads, 0, stream>>>(accum, pixels, out, table);
+    return cudaGetLastError();
+}
+
+} // namespace albedo_b200

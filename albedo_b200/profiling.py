@@ -3,6 +3,7 @@
     python -m albedo_b200.profiling megakernel --width 480 --height 270 --spp 64 [--autotune]
                                    [--accumulation fp64|kahan]
     python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16 [--autotune]
+    python -m albedo_b200.profiling resolve --width 3840 --height 2160
 
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
 --scene icosphere6 (a displaced icosphere of 6 levels, 81,920 triangles), max
@@ -10,7 +11,9 @@ depth 10, seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
 nodes then leaf, 1: one step). With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
-for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel).
+for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel). `resolve` resolves
+seeded accumulators (64 samples a pixel) of the given size to sRGB bytes: one
+warm-up launch, then the profiled one.
 """
 
 from __future__ import annotations
@@ -27,7 +30,7 @@ MEGAKERNEL_TUNING_LAUNCHES = 9 * 3
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("method", choices=["megakernel", "wavefront"])
+    parser.add_argument("method", choices=["megakernel", "wavefront", "resolve"])
     parser.add_argument("--width", type=int, default=480)
     parser.add_argument("--height", type=int, default=270)
     parser.add_argument("--spp", type=int, default=16)
@@ -44,6 +47,9 @@ def main() -> None:
     import albedo_b200 as ab
     from albedo_b200 import scenes
 
+    if args.method == "resolve":
+        resolve_case(args.width, args.height, warmups=0 if args.no_warmup else 1)
+        return
     n = int(round(math.sqrt(args.spp)))
     with tempfile.TemporaryDirectory() as tmp:
         if args.scene == "icosphere6":
@@ -82,6 +88,21 @@ def main() -> None:
             print(f"rendered {args.width}x{args.height} at {n * n} spp (wavefront, {ab.wavefront_last_iterations()} "
                   f"iterations, {ab.wavefront_last_rays()} rays per render); tuned shape {shape or ab.tuning()}")
         scene.close()
+
+
+def resolve_case(width: int, height: int, warmups: int) -> None:
+    import torch
+
+    import albedo_b200 as ab
+
+    generator = torch.Generator(device="cuda").manual_seed(5)
+    acc = torch.rand((width * height, 4), dtype=torch.float64, device="cuda", generator=generator) * 64.0
+    acc.view(torch.int64)[:, 3] = 64
+    out = torch.empty(3 * width * height, dtype=torch.uint8, device="cuda")
+    for _ in range(warmups + 1):
+        ab.resolve_srgb(acc.data_ptr(), width, height, out.data_ptr())
+    torch.cuda.synchronize()
+    print(f"resolved {width}x{height} accumulators to sRGB; resolve launches before the profiled one: {warmups}")
 
 
 if __name__ == "__main__":

@@ -99,6 +99,46 @@ def wavefront_frame(scene, flush, steps: int = 3) -> dict:
             "ms_per_step": s * 1e3, "steps": steps, "iterations": ab.wavefront_last_iterations(), "autotune": shape}
 
 
+RESOLVE_WIDTH, RESOLVE_HEIGHT = 3840, 2160
+RESOLVE_BYTES_PER_PIXEL = 32 + 3  # one accumulator read, three sRGB bytes written
+
+
+def film_resolve_figures(flush, launches: int = 20) -> dict:
+    """The film's device resolve (accumulators to sRGB bytes, bit-exact with the
+    reference's writePpm bytes) on a 3840 x 2160 frame: 265 MB of accumulators,
+    more than L2, and L2 flushed between launches; each launch timed with CUDA
+    events. Algorithmic bytes: 32 read and 3 written per pixel."""
+    import torch
+
+    import albedo_b200 as ab
+
+    pixels = RESOLVE_WIDTH * RESOLVE_HEIGHT
+    generator = torch.Generator(device="cuda").manual_seed(5)
+    acc = torch.rand((pixels, 4), dtype=torch.float64, device="cuda", generator=generator) * 64.0
+    acc.view(torch.int64)[:, 3] = 64
+    out = torch.empty(3 * pixels, dtype=torch.uint8, device="cuda")
+    for _ in range(3):
+        ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
+    torch.cuda.synchronize()
+    ms = []
+    for i in range(launches):
+        flush.fill_(i & 0xFF)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
+        end.record()
+        end.synchronize()
+        ms.append(start.elapsed_time(end))
+    launch_s = statistics.median(ms) / 1e3
+    achieved = RESOLVE_BYTES_PER_PIXEL * pixels / launch_s / 1e9
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    return {"workload": f"{RESOLVE_WIDTH}x{RESOLVE_HEIGHT} accumulators to sRGB bytes", "launches": launches,
+            "us_per_launch": launch_s * 1e6, "gpixels_per_s": pixels / launch_s / 1e9,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "algorithmic_bytes_per_launch": RESOLVE_BYTES_PER_PIXEL * pixels},
+            "d2h_bytes_per_frame": {"accumulators": 32 * pixels, "srgb": 3 * pixels}}
+
+
 def served_figures(rates: list[float], requests: int) -> list[dict]:
     """Poisson request streams (seeded) drawn from the batched-job distribution
     over 16 resident scenes, each request with its own seeded camera around its
@@ -106,7 +146,9 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
     against the plain megakernel serving one request at a time in arrival order.
     Both use autotuned shapes (tuned before the streams start). Latency is
     completion minus arrival (wall clock); throughput is paths over the time from
-    the first arrival to the last completion. The server's batch_mrays_per_s
+    the first arrival to the last completion, where a request completes when its
+    image is on the host as sRGB bytes (device resolve, then a copy of 3 bytes a
+    pixel to pinned memory). The server's batch_mrays_per_s
     counts the rays its wavefront batch traced (not the express route's)."""
     import torch
 
@@ -143,6 +185,18 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
             reqs.append((sid, w, h, n, k, view))
         paths = sum(w * h * n * n for _, w, h, n, _, _ in reqs)
         accs = [torch.zeros((w * h, 4), dtype=torch.float64, device="cuda") for _, w, h, _, _, _ in reqs]
+        srgb_dev = [torch.empty(3 * w * h, dtype=torch.uint8, device="cuda") for _, w, h, _, _, _ in reqs]
+        srgb_host = [torch.empty(3 * w * h, dtype=torch.uint8).pin_memory() for _, w, h, _, _, _ in reqs]
+        delivery = torch.cuda.Stream()
+
+        def deliver(k):
+            # The finished image reaches the host as sRGB bytes: resolved on the
+            # device, 3 bytes a pixel copied instead of 32 of accumulators.
+            _, w, h, _, _, _ = reqs[k]
+            with torch.cuda.stream(delivery):
+                ab.resolve_srgb(accs[k].data_ptr(), w, h, srgb_dev[k].data_ptr(), stream=delivery.cuda_stream)
+                srgb_host[k].copy_(srgb_dev[k], non_blocking=True)
+            delivery.synchronize()
 
         def job(r, method):
             _, w, h, n, seed, _ = r
@@ -167,7 +221,8 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
             finished = server.step()
             now = time.perf_counter() - start
             for t in finished:
-                done_at[ticket_of[t]] = now
+                deliver(ticket_of[t])
+                done_at[ticket_of[t]] = time.perf_counter() - start
             count = server.rays()
             rays += count - last_rays if count >= last_rays else count
             last_rays = count
@@ -189,6 +244,7 @@ def served_figures(rates: list[float], requests: int) -> list[dict]:
                 time.sleep(arrivals[k] - now)
             ab.render_device(loaded[r[0]], job(r, ab.MEGAKERNEL), accs[k].data_ptr(), camera=r[5])
             torch.cuda.synchronize()
+            deliver(k)
             finish.append(time.perf_counter() - start)
         lat_mega = np.array(finish) - arrivals
         span_mega = finish[-1] - arrivals[0]
@@ -684,7 +740,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline_sample(scene_path)
             if not args.no_forms:
                 line["forms"] = {"wavefront_frame": wavefront_frame(scene, flush),
-                                 "batched_64_jobs": batched_figures(1, 1)}
+                                 "batched_64_jobs": batched_figures(1, 1),
+                                 "film_resolve": film_resolve_figures(flush)}
         print(json.dumps(line), flush=True)
     scene.close()
     if dist is not None:

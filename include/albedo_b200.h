@@ -229,6 +229,34 @@ int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* str
  * height entries; the call returns after the render is complete on `stream`. */
 int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
                           void* stream);
+/* Film output (image/ppm.cpp:22-85, color/srgb.cpp:18-36). albedo_resolve_srgb
+ * turns width*height device accumulators into width*height*3 device bytes, the
+ * R G B bytes writePpm writes for each pixel's average (rows from the top): the
+ * average is sum / count (0 without samples), its byte toByte(encodeSrgb(.)).
+ * The bytes equal the reference's exactly. It is asynchronous on `stream`;
+ * accumulators must be 8-byte aligned. It replaces the reference's per-pixel
+ * encodeRow loop (image/ppm.cpp:22-33) and, for a served image, the copy of 32
+ * bytes a pixel to the host by one of 3. */
+int albedo_resolve_srgb(const albedo_accumulator* accumulators, int32_t width, int32_t height, uint8_t* out_rgb,
+                        void* stream);
+/* The 256 thresholds the resolve compares against: out_lower[b] (b = 1..255) is
+ * the smallest positive double whose byte is at least b; out_lower[0] is
+ * -infinity. Computed on the host from the reference's transfer function. */
+int albedo_srgb_thresholds(double* out_lower);
+/* writePpm(path, image) (image/ppm.cpp:61-85) from host bytes already encoded:
+ * a binary P6 file with maxval 255. The file is truncated on open; on a failed
+ * write the partial file is removed (when it is a regular file). Errors carry the
+ * reference's messages: "cannot open '<path>' for writing", "failed to write
+ * '<path>': failed to write PPM image" (a failure while writing) and "failed to
+ * write '<path>'" (a failure on close); all are ALBEDO_IO_ERROR. */
+int albedo_write_ppm(const char* path, const uint8_t* rgb, int32_t width, int32_t height);
+/* writePpm(path, image) for device accumulators: resolves them on `stream`,
+ * copies the bytes back, synchronizes the stream and writes the file. */
+int albedo_save_ppm(const char* path, const albedo_accumulator* accumulators, int32_t width, int32_t height,
+                    void* stream);
+/* albedo_save_ppm for host accumulators, uploaded through the per-device staging
+ * buffer that albedo_render_host uses. */
+int albedo_save_ppm_host(const char* path, const albedo_accumulator* accumulators, int32_t width, int32_t height);
 /* A render server: continuous batching of requests on one wavefront engine. A
  * request is admitted, in arrival order, once the device memory it needs fits
  * the budget: the engine's path slots and queues, each scene's tables (counted

@@ -24,7 +24,9 @@
 #include "albedo/geometry/sphere.hpp"
 #include "albedo/geometry/triangle.hpp"
 #include "albedo/geometry/triangle_mesh.hpp"
+#include "albedo/color/srgb.hpp"
 #include "albedo/image/pixel_buffer.hpp"
+#include "albedo/image/ppm.hpp"
 #include "albedo/light/area_light.hpp"
 #include "albedo/render/render_image.hpp"
 #include "albedo/sampling/pcg32.hpp"
@@ -44,6 +46,7 @@
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <filesystem>
 #include <memory>
 #include <string>
 #include <thread>
@@ -461,6 +464,31 @@ void ref_warps(const double* u, std::int64_t count, double* out_cosine, double* 
         out_sphere[3 * i + 1] = s.y;
         out_sphere[3 * i + 2] = s.z;
     }
+}
+
+// toByte(encodeSrgb(x)) for each value (color/srgb.cpp:18-36).
+void ref_srgb_bytes(const double* linear, std::int64_t count, std::uint8_t* out)
+{
+    for (std::int64_t i{0}; i < count; ++i) {
+        out[i] = toByte(encodeSrgb(linear[i]));
+    }
+}
+
+// writePpm(path, image) (image/ppm.cpp:61-85) of a PixelBuffer whose pixels hold
+// the given averages (W*H*3 doubles, rows from the top): one sample each, so
+// each pixel's average is the value itself.
+int ref_write_ppm(const char* path, int width, int height, const double* averages)
+{
+    return guarded([&] {
+        PixelBuffer image{width, height};
+        for (int y{0}; y < height; ++y) {
+            for (int x{0}; x < width; ++x) {
+                const double* v{averages + 3 * (static_cast<std::int64_t>(y) * width + x)};
+                image.addSample({.x = x, .y = y}, Rgb{v[0], v[1], v[2]});
+            }
+        }
+        writePpm(std::filesystem::path{path}, image);
+    });
 }
 
 } // extern "C"

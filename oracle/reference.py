@@ -43,6 +43,8 @@ _PROTOTYPES = {
     "ref_sphere_intersect": (None, [_D, _D, c_int64, c_double, c_double, _I32, _D]),
     "ref_triangle_intersect": (None, [_D, _D, c_int64, c_double, c_double, _I32, _D]),
     "ref_warps": (None, [_D, c_int64, _D, _D]),
+    "ref_srgb_bytes": (None, [_D, c_int64, POINTER(ctypes.c_uint8)]),
+    "ref_write_ppm": (c_int, [c_char_p, c_int, c_int, _D]),
 }
 
 _lib = None
@@ -182,3 +184,19 @@ def lobe_sample(kind: int, params, inputs: np.ndarray):
     _check(lib().ref_lobe_sample(kind, _d(params), _d(inputs), n, valid.ctypes.data_as(_I32), _d(direction),
                                  _d(weight), _d(pdf), specular.ctypes.data_as(_I32)))
     return valid, direction, weight, pdf, specular
+
+
+def srgb_bytes(linear: np.ndarray) -> np.ndarray:
+    """The reference's toByte(encodeSrgb(x)) per value (color/srgb.cpp:18-36)."""
+    linear = np.ascontiguousarray(linear, dtype=np.float64)
+    out = np.empty(linear.shape, dtype=np.uint8)
+    lib().ref_srgb_bytes(_d(linear), linear.size, out.ctypes.data_as(POINTER(ctypes.c_uint8)))
+    return out
+
+
+def write_ppm(path, averages: np.ndarray) -> None:
+    """The reference's writePpm of an image whose pixel averages are `averages`
+    (shape (H, W, 3)); raises RuntimeError with its message on failure."""
+    averages = np.ascontiguousarray(averages, dtype=np.float64)
+    h, w, _ = averages.shape
+    _check(lib().ref_write_ppm(str(path).encode(), w, h, _d(averages)))

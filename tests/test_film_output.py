@@ -1,0 +1,151 @@
+"""The film's output encoding and PPM writer against the reference, on the host.
+
+The device resolve compares each pixel's average against a table of the
+smallest double of every byte, built with the reference's transfer function
+(color/srgb.cpp:18-36). Here the table is checked against the reference's own
+toByte(encodeSrgb(x)) on the golden values of its tests
+(tests/color/srgb_test.cpp, tests/image/ppm_test.cpp), on millions of seeded
+values and on every value within 2,000 ulps of each threshold, where a rounding
+difference could show. The PPM writer (image/ppm.cpp:47-85) is compared byte
+for byte with the reference's, including its failures.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import albedo_b200 as ab
+from oracle import reference as ref
+
+needs_ref = pytest.mark.skipif(not ref.available(), reason="reference library not built")
+
+
+def table_bytes(values: np.ndarray) -> np.ndarray:
+    """The byte the table gives: the largest b >= 1 with value >= lower[b], else 0."""
+    lower = ab.srgb_thresholds()[1:]
+    values = np.asarray(values, dtype=np.float64)
+    b = np.searchsorted(lower, values, side="right")
+    return np.where(np.isnan(values), 0, b).astype(np.uint8)
+
+
+def test_thresholds_are_increasing_and_bracket_the_byte_range():
+    lower = ab.srgb_thresholds()
+    assert lower[0] == -np.inf
+    assert np.all(np.diff(lower[1:]) > 0)
+    assert 0 < lower[1] < 1e-3 and 0.99 < lower[255] <= 1.0
+
+
+# (linear value, byte) pairs from the reference's tests: black, white, 50% linear
+# is 188 (srgb_test.cpp:56-58), clamping above one and below zero
+# (ppm_test.cpp:60-67), NaN and infinities (srgb_test.cpp:52-76).
+GOLDEN = [(0.0, 0), (1.0, 255), (0.5, 188), (4.0, 255), (-2.0, 0), (-0.5, 0), (7.0, 255),
+          (np.nan, 0), (np.inf, 255), (-np.inf, 0), (0.001, 3), (-0.0, 0)]
+
+
+@needs_ref
+def test_golden_values_from_the_reference_tests():
+    values = np.array([v for v, _ in GOLDEN])
+    expected = np.array([b for _, b in GOLDEN], dtype=np.uint8)
+    assert np.array_equal(ref.srgb_bytes(values), expected)
+    assert np.array_equal(table_bytes(values), expected)
+
+
+@needs_ref
+def test_table_equals_the_reference_on_seeded_values():
+    rng = np.random.default_rng(7)
+    values = np.concatenate([
+        rng.uniform(-0.1, 1.2, 2_000_000),
+        np.exp(rng.uniform(np.log(1e-7), np.log(2.0), 2_000_000)),
+        rng.uniform(0.0031, 0.00316, 200_000),  # around the segment switch
+    ])
+    assert np.array_equal(table_bytes(values), ref.srgb_bytes(values))
+
+
+@needs_ref
+def test_table_equals_the_reference_within_2000_ulps_of_every_threshold():
+    lower = ab.srgb_thresholds()[1:]
+    bits = lower.view(np.int64)[:, None] + np.arange(-2000, 2001, dtype=np.int64)[None, :]
+    values = bits.reshape(-1).view(np.float64)
+    ours = table_bytes(values)
+    theirs = ref.srgb_bytes(values)
+    assert np.array_equal(ours, theirs)
+    # Each threshold is where the reference's byte steps up.
+    assert np.array_equal(ref.srgb_bytes(lower), np.arange(1, 256, dtype=np.uint8))
+    below = np.nextafter(lower, -np.inf)
+    assert np.array_equal(ref.srgb_bytes(below), np.arange(0, 255, dtype=np.uint8))
+
+
+TWO_PIXEL_PPM = b"P6\n2 1\n255\n\xFF\x00\x00\xBC\xBC\xBC"
+
+
+def test_two_pixel_image_writes_the_reference_test_bytes(tmp_path):
+    # ppm_test.cpp:22-33: a red pixel beside a 50%-gray one.
+    rgb = np.array([[[255, 0, 0], [188, 188, 188]]], dtype=np.uint8)
+    path = tmp_path / "two.ppm"
+    ab.write_ppm(path, rgb)
+    assert path.read_bytes() == TWO_PIXEL_PPM
+
+
+def test_overwrites_a_longer_existing_file(tmp_path):
+    path = tmp_path / "old.ppm"
+    path.write_bytes(b"x" * 64)
+    ab.write_ppm(path, np.array([[[255, 0, 0], [188, 188, 188]]], dtype=np.uint8))
+    assert path.read_bytes() == TWO_PIXEL_PPM
+
+
+@needs_ref
+@pytest.mark.parametrize("shape", [(1, 1), (2, 3), (37, 53), (270, 480)])
+def test_files_equal_the_reference_writer(tmp_path, shape):
+    h, w = shape
+    rng = np.random.default_rng(h * 1000 + w)
+    averages = rng.uniform(-0.2, 1.4, size=(h, w, 3))
+    averages.reshape(-1)[rng.choice(averages.size, size=max(1, averages.size // 50))] = np.nan
+    ours, theirs = tmp_path / "ours.ppm", tmp_path / "theirs.ppm"
+    ab.write_ppm(ours, ref.srgb_bytes(averages))
+    ref.write_ppm(theirs, averages)
+    assert ours.read_bytes() == theirs.read_bytes()
+
+
+@needs_ref
+def test_unopenable_path_fails_with_the_reference_message(tmp_path):
+    path = tmp_path / "missing_dir" / "image.ppm"
+    with pytest.raises(OSError) as ours:
+        ab.write_ppm(path, np.zeros((1, 2, 3), dtype=np.uint8))
+    with pytest.raises(RuntimeError) as theirs:
+        ref.write_ppm(path, np.zeros((1, 2, 3)))
+    assert str(ours.value) == str(theirs.value) == f"cannot open '{path}' for writing"
+
+
+@needs_ref
+@pytest.mark.skipif(not os.path.exists("/dev/full"), reason="needs /dev/full")
+@pytest.mark.parametrize("shape", [(1, 2), (256, 256)])
+def test_failed_writes_report_like_the_reference(shape):
+    # /dev/full accepts the open and fails every write: a small image fails on
+    # close, a large one while its rows are written (ppm_test.cpp:135-172).
+    h, w = shape
+    with pytest.raises(OSError) as ours:
+        ab.write_ppm("/dev/full", np.zeros((h, w, 3), dtype=np.uint8))
+    with pytest.raises(RuntimeError) as theirs:
+        ref.write_ppm("/dev/full", np.zeros((h, w, 3)))
+    assert str(ours.value) == str(theirs.value)
+    stream_message = "failed to write PPM image"
+    assert (stream_message in str(ours.value)) == (h * w > 2)
+
+
+def test_refused_writes_leave_the_target_alone(tmp_path):
+    # A size the writer refuses fails before anything is opened; a directory in
+    # the way of the file fails the open and is left as it was.
+    path = tmp_path / "image.ppm"
+    with pytest.raises(ValueError, match="invalid image size 0x1"):
+        ab.write_ppm(path, np.zeros((1, 0, 3), dtype=np.uint8))
+    assert not path.exists()
+    (tmp_path / "dir.ppm").mkdir()
+    with pytest.raises(OSError, match="cannot open"):
+        ab.write_ppm(tmp_path / "dir.ppm", np.zeros((1, 1, 3), dtype=np.uint8))
+    assert (tmp_path / "dir.ppm").is_dir()
+
+
+def test_invalid_shapes_are_refused():
+    with pytest.raises(ValueError):
+        ab.write_ppm("unused.ppm", np.zeros((2, 2), dtype=np.uint8))
