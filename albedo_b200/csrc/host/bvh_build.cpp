@@ -4,9 +4,13 @@
 #include <algorithm>
 #include <array>
 #include <cstddef>
+#include <exception>
 #include <format>
+#include <memory>
 #include <optional>
 #include <stdexcept>
+#include <thread>
+#include <utility>
 
 namespace albedo_b200 {
 
@@ -162,29 +166,121 @@ Partition partitionForSplit(std::span<Prim> prims, const Extents& extents, std::
 }
 
 // buildSubtree, accel/bvh.cpp:224-244 (recursion depth is bounded by 32 + log2 n).
-std::size_t buildSubtree(BuiltBvh& bvh, std::span<Prim> prims, std::size_t first, std::size_t depth)
+// Appends the subtree to `nodes`; interior offsets index `nodes` itself.
+std::size_t buildSubtree(std::vector<BuildNode>& nodes, std::uint32_t& max_depth, std::span<Prim> prims,
+                         std::size_t first, std::size_t depth)
 {
-    const std::size_t index{bvh.nodes.size()};
+    const std::size_t index{nodes.size()};
     const Extents extents{extentsOf(prims)};
-    bvh.nodes.push_back({.bounds = extents.bounds});
-    bvh.max_depth = std::max<std::uint32_t>(bvh.max_depth, static_cast<std::uint32_t>(depth));
+    nodes.push_back({.bounds = extents.bounds});
+    max_depth = std::max<std::uint32_t>(max_depth, static_cast<std::uint32_t>(depth));
     const Partition partition{prims.size() == 1 ? Partition{} : partitionForSplit(prims, extents, depth)};
     if (partition.left_count == 0) {
-        bvh.nodes[index].offset = first;
-        bvh.nodes[index].count = static_cast<std::uint32_t>(prims.size());
+        nodes[index].offset = first;
+        nodes[index].count = static_cast<std::uint32_t>(prims.size());
         return index;
     }
-    buildSubtree(bvh, prims.first(partition.left_count), first, depth + 1);
-    const std::size_t second{
-        buildSubtree(bvh, prims.subspan(partition.left_count), first + partition.left_count, depth + 1)};
-    bvh.nodes[index].offset = second;
-    bvh.nodes[index].axis = static_cast<std::uint8_t>(partition.axis);
+    buildSubtree(nodes, max_depth, prims.first(partition.left_count), first, depth + 1);
+    const std::size_t second{buildSubtree(nodes, max_depth, prims.subspan(partition.left_count),
+                                          first + partition.left_count, depth + 1)};
+    nodes[index].offset = second;
+    nodes[index].axis = static_cast<std::uint8_t>(partition.axis);
     return index;
+}
+
+// Ranges below this many primitives are built on one thread.
+constexpr std::size_t kParallelMinimum{8192};
+
+// A subtree built in parallel: either nodes built on one thread (interior
+// offsets relative to the piece's first node) or one node whose two children
+// were built concurrently. Every node makes the same decision from the same
+// primitive range as in the one-thread build, because a node's range is
+// partitioned before its children start, so the tree is the same.
+struct Piece {
+    std::vector<BuildNode> nodes;
+    BuildNode self{};
+    std::unique_ptr<Piece> left;
+    std::unique_ptr<Piece> right;
+    std::size_t total{0};
+    std::uint32_t max_depth{0};
+};
+
+std::unique_ptr<Piece> buildPiece(std::span<Prim> prims, std::size_t first, std::size_t depth, unsigned threads)
+{
+    auto piece{std::make_unique<Piece>()};
+    if (threads <= 1 || prims.size() < kParallelMinimum) {
+        piece->nodes.reserve(2 * prims.size() - 1);
+        buildSubtree(piece->nodes, piece->max_depth, prims, first, depth);
+        piece->total = piece->nodes.size();
+        return piece;
+    }
+    const Extents extents{extentsOf(prims)};
+    const Partition partition{partitionForSplit(prims, extents, depth)};
+    if (partition.left_count == 0) {
+        piece->nodes.push_back({.bounds = extents.bounds, .offset = first,
+                                .count = static_cast<std::uint32_t>(prims.size())});
+        piece->total = 1;
+        piece->max_depth = static_cast<std::uint32_t>(depth);
+        return piece;
+    }
+    piece->self = {.bounds = extents.bounds, .axis = static_cast<std::uint8_t>(partition.axis)};
+    // Threads split in proportion to the primitives on each side.
+    const double share{static_cast<double>(partition.left_count) / static_cast<double>(prims.size())};
+    const unsigned left_threads{std::clamp(static_cast<unsigned>(share * threads + 0.5), 1u, threads - 1)};
+    std::exception_ptr failure;
+    std::thread worker{[&] {
+        try {
+            piece->left = buildPiece(prims.first(partition.left_count), first, depth + 1, left_threads);
+        } catch (...) {
+            failure = std::current_exception();
+        }
+    }};
+    try {
+        piece->right = buildPiece(prims.subspan(partition.left_count), first + partition.left_count, depth + 1,
+                                  threads - left_threads);
+    } catch (...) {
+        worker.join();
+        throw;
+    }
+    worker.join();
+    if (failure) {
+        std::rethrow_exception(failure);
+    }
+    piece->total = 1 + piece->left->total + piece->right->total;
+    piece->max_depth = std::max(piece->left->max_depth, piece->right->max_depth);
+    return piece;
+}
+
+// Lays a piece out in depth-first order from node `at`, collecting the
+// one-thread pieces (with their positions) for a parallel copy.
+void layOut(const Piece& piece, std::vector<BuildNode>& out, std::size_t at,
+            std::vector<std::pair<const Piece*, std::size_t>>& copies)
+{
+    if (!piece.left) {
+        copies.emplace_back(&piece, at);
+        return;
+    }
+    BuildNode self{piece.self};
+    self.offset = at + 1 + piece.left->total;
+    out[at] = self;
+    layOut(*piece.left, out, at + 1, copies);
+    layOut(*piece.right, out, at + 1 + piece.left->total, copies);
+}
+
+void copyPiece(const Piece& piece, std::vector<BuildNode>& out, std::size_t at)
+{
+    for (std::size_t i{0}; i < piece.nodes.size(); ++i) {
+        BuildNode node{piece.nodes[i]};
+        if (node.count == 0) {
+            node.offset += at;
+        }
+        out[at + i] = node;
+    }
 }
 
 } // namespace
 
-BuiltBvh buildBvh(std::span<const Box3> primitive_bounds)
+BuiltBvh buildBvh(std::span<const Box3> primitive_bounds, unsigned threads)
 {
     BuiltBvh bvh;
     if (primitive_bounds.empty()) {
@@ -199,8 +295,26 @@ BuiltBvh buildBvh(std::span<const Box3> primitive_bounds)
         }
         prims.push_back({box, centroidOf(box), index});
     }
-    bvh.nodes.reserve(2 * prims.size() - 1);
-    buildSubtree(bvh, prims, 0, 0);
+    if (threads == 0) {
+        threads = std::max(1u, std::thread::hardware_concurrency());
+    }
+    std::unique_ptr<Piece> root{buildPiece(prims, 0, 0, threads)};
+    bvh.max_depth = root->max_depth;
+    if (!root->left) {
+        bvh.nodes = std::move(root->nodes);
+    } else {
+        bvh.nodes.resize(root->total);
+        std::vector<std::pair<const Piece*, std::size_t>> copies;
+        layOut(*root, bvh.nodes, 0, copies);
+        std::vector<std::thread> workers;
+        for (std::size_t t{1}; t < copies.size(); ++t) {
+            workers.emplace_back([&, t] { copyPiece(*copies[t].first, bvh.nodes, copies[t].second); });
+        }
+        copyPiece(*copies[0].first, bvh.nodes, copies[0].second);
+        for (std::thread& worker : workers) {
+            worker.join();
+        }
+    }
     bvh.order.reserve(prims.size());
     for (const Prim& p : prims) {
         bvh.order.push_back(static_cast<std::uint32_t>(p.index));

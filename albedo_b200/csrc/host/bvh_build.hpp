@@ -37,7 +37,9 @@ struct BuiltBvh {
 };
 
 // Builds over boxes 0..n-1. Throws std::invalid_argument for an empty or
-// non-finite box, as accel/bvh.cpp:253-261 does.
-BuiltBvh buildBvh(std::span<const Box3> primitive_bounds);
+// non-finite box, as accel/bvh.cpp:253-261 does. Subtrees of large ranges are
+// built on up to `threads` threads (0: one per hardware thread); the tree is
+// the same for every thread count.
+BuiltBvh buildBvh(std::span<const Box3> primitive_bounds, unsigned threads = 0);
 
 } // namespace albedo_b200
