@@ -3,9 +3,12 @@
 // (camera/perspective_camera.cpp:24-110).
 #include "host_scene.hpp"
 
+#include <algorithm>
 #include <format>
 #include <numbers>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 namespace albedo_b200 {
 
@@ -116,6 +119,64 @@ void HostScene::setSky(Rgb nadir, Rgb zenith)
 
 namespace {
 
+// Meshes of at least this many faces are processed on several threads.
+constexpr std::size_t kParallelFaces{8192};
+
+std::size_t chunkCount(std::size_t faces)
+{
+    if (faces < kParallelFaces) {
+        return 1;
+    }
+    return std::max<std::size_t>(1, std::min<std::size_t>(std::thread::hardware_concurrency(), faces / 4096));
+}
+
+// Runs body(chunk, begin, end) over `chunks` contiguous ranges of [0, n), each
+// on its own thread (the first on the calling one).
+template <typename F>
+void forEachChunk(std::size_t n, std::size_t chunks, F&& body)
+{
+    const auto range = [&](std::size_t chunk) { return n * chunk / chunks; };
+    std::vector<std::thread> workers;
+    for (std::size_t chunk{1}; chunk < chunks; ++chunk) {
+        workers.emplace_back([&, chunk] { body(chunk, range(chunk), range(chunk + 1)); });
+    }
+    body(0, range(0), range(1));
+    for (std::thread& worker : workers) {
+        worker.join();
+    }
+}
+
+// Area-weighted vertex normals (geometry/triangle_mesh.cpp:92-107): the
+// unnormalized edge cross product of every face that forms a triangle, summed
+// per position in face order. Each thread owns a range of positions and scans
+// all faces in order, adding only to the positions it owns, so every sum adds
+// the same terms in the same order as one thread would.
+std::vector<Vec3> smoothNormalSums(const std::vector<Vec3>& positions,
+                                   const std::vector<std::array<std::uint32_t, 3>>& faces,
+                                   const std::vector<std::uint8_t>& forms, std::size_t chunks)
+{
+    std::vector<Vec3> sums(positions.size());
+    forEachChunk(positions.size(), chunks, [&](std::size_t, std::size_t begin, std::size_t end) {
+        const auto owned = [&](std::uint32_t index) { return index >= begin && index < end; };
+        for (std::size_t face{0}; face < faces.size(); ++face) {
+            const auto& f{faces[face]};
+            if (!forms[face] || !(owned(f[0]) || owned(f[1]) || owned(f[2]))) {
+                continue;
+            }
+            const Vec3 p0{positions[f[0]]};
+            const Vec3 p1{positions[f[1]]};
+            const Vec3 p2{positions[f[2]]};
+            const Vec3 area_normal{cross(p1 - p0, p2 - p0)};
+            for (const std::uint32_t index : f) {
+                if (owned(index)) {
+                    sums[index] = sums[index] + area_normal;
+                }
+            }
+        }
+    });
+    return sums;
+}
+
 // TriangleMesh validation (geometry/triangle_mesh.cpp:57-74) and its triangles()
 // and smoothNormals() (geometry/triangle_mesh.cpp:76-125).
 struct MeshTriangles {
@@ -158,52 +219,63 @@ MeshTriangles meshTriangles(const std::vector<Vec3>& positions, const std::vecto
             }
         }
     }
-    MeshTriangles result;
-    result.triangles.reserve(faces.size());
-    for (std::size_t face{0}; face < faces.size(); ++face) {
-        const Vec3 p0{positions[faces[face][0]]};
-        const Vec3 p1{positions[faces[face][1]]};
-        const Vec3 p2{positions[faces[face][2]]};
-        if (!formsTriangle(p0, p1, p2)) {
-            continue;
+    // Faces are independent except for the vertex-normal sums, so large meshes
+    // are processed in chunks on several threads; the results are the
+    // one-thread results (see smoothNormalSums for the sums).
+    const std::size_t chunks{chunkCount(faces.size())};
+    std::vector<std::uint8_t> forms(faces.size());
+    std::vector<std::size_t> kept_before(chunks + 1, 0);
+    forEachChunk(faces.size(), chunks, [&](std::size_t chunk, std::size_t begin, std::size_t end) {
+        std::size_t kept{0};
+        for (std::size_t face{begin}; face < end; ++face) {
+            forms[face] = formsTriangle(positions[faces[face][0]], positions[faces[face][1]],
+                                        positions[faces[face][2]]);
+            kept += forms[face];
         }
-        std::array<std::array<double, 2>, 3> uv{kDefaultUv};
-        if (!texture_faces.empty()) {
-            uv = {uvs[texture_faces[face][0]], uvs[texture_faces[face][1]], uvs[texture_faces[face][2]]};
-        }
-        result.triangles.push_back(makeTriangle(p0, p1, p2, uv));
+        kept_before[chunk + 1] = kept;
+    });
+    for (std::size_t chunk{0}; chunk < chunks; ++chunk) {
+        kept_before[chunk + 1] += kept_before[chunk];
     }
+    MeshTriangles result;
+    result.triangles.resize(kept_before[chunks]);
+    forEachChunk(faces.size(), chunks, [&](std::size_t chunk, std::size_t begin, std::size_t end) {
+        std::size_t out{kept_before[chunk]};
+        for (std::size_t face{begin}; face < end; ++face) {
+            if (!forms[face]) {
+                continue;
+            }
+            std::array<std::array<double, 2>, 3> uv{kDefaultUv};
+            if (!texture_faces.empty()) {
+                uv = {uvs[texture_faces[face][0]], uvs[texture_faces[face][1]], uvs[texture_faces[face][2]]};
+            }
+            result.triangles[out++] =
+                makeTriangle(positions[faces[face][0]], positions[faces[face][1]], positions[faces[face][2]], uv);
+        }
+    });
     if (!smooth) {
         return result;
     }
-    // Area-weighted vertex normals: unnormalized edge cross products summed per position.
-    std::vector<Vec3> sums(positions.size());
-    for (const auto& f : faces) {
-        const Vec3 p0{positions[f[0]]};
-        const Vec3 p1{positions[f[1]]};
-        const Vec3 p2{positions[f[2]]};
-        if (formsTriangle(p0, p1, p2)) {
-            const Vec3 area_normal{cross(p1 - p0, p2 - p0)};
-            sums[f[0]] = sums[f[0]] + area_normal;
-            sums[f[1]] = sums[f[1]] + area_normal;
-            sums[f[2]] = sums[f[2]] + area_normal;
+    const std::vector<Vec3> sums{smoothNormalSums(positions, faces, forms, chunks)};
+    result.corner_normals.resize(result.triangles.size());
+    forEachChunk(faces.size(), chunks, [&](std::size_t chunk, std::size_t begin, std::size_t end) {
+        std::size_t out{kept_before[chunk]};
+        for (std::size_t face{begin}; face < end; ++face) {
+            if (!forms[face]) {
+                continue;
+            }
+            const auto& f{faces[face]};
+            const Vec3 p0{positions[f[0]]};
+            const Vec3 p1{positions[f[1]]};
+            const Vec3 p2{positions[f[2]]};
+            const Vec3 face_normal{normalized(cross(p1 - p0, p2 - p0))};
+            const auto corner = [&](std::uint32_t index) {
+                const Vec3 sum{sums[index]};
+                return std::isnormal(lengthSquared(sum)) ? normalized(sum) : face_normal;
+            };
+            result.corner_normals[out++] = {corner(f[0]), corner(f[1]), corner(f[2])};
         }
-    }
-    result.corner_normals.reserve(result.triangles.size());
-    for (const auto& f : faces) {
-        const Vec3 p0{positions[f[0]]};
-        const Vec3 p1{positions[f[1]]};
-        const Vec3 p2{positions[f[2]]};
-        if (!formsTriangle(p0, p1, p2)) {
-            continue;
-        }
-        const Vec3 face_normal{normalized(cross(p1 - p0, p2 - p0))};
-        const auto corner = [&](std::uint32_t index) {
-            const Vec3 sum{sums[index]};
-            return std::isnormal(lengthSquared(sum)) ? normalized(sum) : face_normal;
-        };
-        result.corner_normals.push_back({corner(f[0]), corner(f[1]), corner(f[2])});
-    }
+    });
     return result;
 }
 
