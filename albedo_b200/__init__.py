@@ -353,12 +353,22 @@ def resolve_srgb(accumulators_ptr: int, width: int, height: int, out_ptr: int, s
                                          c_void_p(stream)))
 
 
+SRGB_BUCKET_SHIFT, SRGB_BUCKET_BASE, SRGB_BUCKETS = 45, (1023 - 13) * 128, 13 * 128
+
+
+def srgb_tables() -> tuple[np.ndarray, np.ndarray]:
+    """The resolve's tables: lower[b] is the smallest positive double whose byte
+    is at least b (b = 1..255; lower[0] is -inf), and start[k] the byte at the
+    smallest double of bucket k (bits >> SRGB_BUCKET_SHIFT == SRGB_BUCKET_BASE + k)."""
+    lower = np.empty(256, dtype=np.float64)
+    start = np.empty(SRGB_BUCKETS, dtype=np.uint8)
+    _raise(library().albedo_srgb_tables(lower.ctypes.data_as(POINTER(c_double)), start.ctypes.data_as(c_void_p)))
+    return lower, start
+
+
 def srgb_thresholds() -> np.ndarray:
-    """The resolve's table: [b] is the smallest positive double whose byte is at
-    least b (b = 1..255); [0] is -inf."""
-    out = np.empty(256, dtype=np.float64)
-    _raise(library().albedo_srgb_thresholds(out.ctypes.data_as(POINTER(c_double))))
-    return out
+    """lower of srgb_tables()."""
+    return srgb_tables()[0]
 
 
 def write_ppm(path, rgb: np.ndarray) -> None:
@@ -557,5 +567,5 @@ __all__ = [
     "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
     "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
     "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "resolve_srgb", "save_ppm",
-    "set_tuning", "srgb_thresholds", "trace_work_counts", "tuning", "wavefront_last_rays", "write_ppm",
+    "set_tuning", "srgb_tables", "srgb_thresholds", "trace_work_counts", "tuning", "wavefront_last_rays", "write_ppm",
 ]

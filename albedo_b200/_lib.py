@@ -85,7 +85,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render_batch": (c_int32, [c_void_p, c_int32, c_void_p]),
     "albedo_render_noalloc": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
     "albedo_resolve_srgb": (c_int32, [c_void_p, c_int32, c_int32, c_void_p, c_void_p]),
-    "albedo_srgb_thresholds": (c_int32, [_D3]),
+    "albedo_srgb_tables": (c_int32, [_D3, c_void_p]),
     "albedo_write_ppm": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "albedo_save_ppm": (c_int32, [c_char_p, c_void_p, c_int32, c_int32, c_void_p]),
     "albedo_save_ppm_host": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),

@@ -1013,9 +1013,12 @@ std::size_t filmPixels(int32_t width, int32_t height)
 
 const SrgbThresholds& deviceSrgbTable()
 {
+    static_assert(kResolveBucketBase == kSrgbBucketBase && kResolveBuckets == kSrgbBuckets &&
+                  kResolveBucketShift == 52 - kSrgbBucketBits);
     static const SrgbThresholds table{[] {
         SrgbThresholds t{};
         std::copy(srgbTable().lower.begin(), srgbTable().lower.end(), t.lower);
+        std::copy(srgbTable().start.begin(), srgbTable().start.end(), t.start);
         return t;
     }()};
     return table;
@@ -1062,13 +1065,16 @@ int albedo_resolve_srgb(const albedo_accumulator* accumulators, int32_t width, i
     });
 }
 
-int albedo_srgb_thresholds(double* out_lower)
+int albedo_srgb_tables(double* out_lower, uint8_t* out_start)
 {
     return guarded([&] {
         if (out_lower == nullptr) {
             throw std::invalid_argument{"null output pointer"};
         }
         std::copy(srgbTable().lower.begin(), srgbTable().lower.end(), out_lower);
+        if (out_start != nullptr) {
+            std::copy(srgbTable().start.begin(), srgbTable().start.end(), out_start);
+        }
     });
 }
 

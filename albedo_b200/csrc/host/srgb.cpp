@@ -1,5 +1,6 @@
 #include "srgb.hpp"
 
+#include <algorithm>
 #include <bit>
 #include <cmath>
 #include <format>
@@ -40,6 +41,24 @@ SrgbTable buildTable()
             }
         }
         table.lower[static_cast<std::size_t>(b)] = std::bit_cast<double>(hi);
+    }
+    if (!(table.lower[1] > 0x1p-13) || !(table.lower[255] <= 1.0)) {
+        throw std::logic_error{"sRGB thresholds outside the bucketed range"};
+    }
+    // The byte at a value: the number of thresholds at or below it.
+    const auto byteAt = [&](double v) {
+        return static_cast<int>(std::upper_bound(table.lower.begin() + 1, table.lower.end(), v) -
+                                (table.lower.begin() + 1));
+    };
+    for (int k{0}; k < kSrgbBuckets; ++k) {
+        const std::int64_t first_bits{(kSrgbBucketBase + k) << (52 - kSrgbBucketBits)};
+        const double first{std::bit_cast<double>(first_bits)};
+        const double last{std::bit_cast<double>(first_bits + (std::int64_t{1} << (52 - kSrgbBucketBits)) - 1)};
+        const int low{byteAt(first)};
+        if (byteAt(last) > low + 1) {
+            throw std::logic_error{"an sRGB bucket holds more than one threshold"};
+        }
+        table.start[static_cast<std::size_t>(k)] = static_cast<std::uint8_t>(low);
     }
     return table;
 }

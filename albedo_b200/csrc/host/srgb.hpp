@@ -24,8 +24,20 @@ std::uint8_t srgbByte(double linear) noexcept;
 // qualifies (NaN included), which equals srgbByte because srgbByte never
 // decreases as its argument grows. The device resolve compares against this
 // table, so it needs no transcendental function of its own.
+//
+// start[k] speeds the search up: it is the byte of the smallest double in bucket
+// k, where the buckets split [2^-13, 1) by the double's exponent and the top 7
+// bits of its mantissa (bucket k holds the doubles whose bits shifted right by
+// 45 equal kSrgbBucketBase + k). No bucket holds more than one threshold (the
+// build checks this), so a value's byte is start[k] or start[k] + 1, and one
+// comparison with lower[start[k] + 1] decides. Every value with a byte from 1
+// to 254 lies in some bucket: lower[1] > 2^-13 and lower[255] <= 1.
+inline constexpr int kSrgbBucketBits{7};
+inline constexpr std::int64_t kSrgbBucketBase{(1023 - 13) << kSrgbBucketBits};
+inline constexpr int kSrgbBuckets{13 << kSrgbBucketBits};
 struct SrgbTable {
     std::array<double, 256> lower;
+    std::array<std::uint8_t, kSrgbBuckets> start;
 };
 const SrgbTable& srgbTable();
 

@@ -117,9 +117,15 @@ cudaError_t launchOccluded(const DevScene& scene, const float* rays, const float
 
 // The film's resolve to 8-bit sRGB (3 bytes a pixel) from per-pixel averages,
 // by comparison against a table of the smallest double of each byte (lower[b],
-// b = 1..255; lower[0] is unused).
+// b = 1..255; lower[0] is unused). start[k] is the byte at the smallest double of
+// bucket k: the doubles whose bits shifted right by 45 equal kResolveBucketBase +
+// k, each holding at most one threshold (the host builds and checks both tables).
+constexpr int kResolveBucketShift{45};
+constexpr long long kResolveBucketBase{(1023 - 13) << 7};
+constexpr int kResolveBuckets{13 << 7};
 struct SrgbThresholds {
     double lower[256];
+    unsigned char start[kResolveBuckets];
 };
 cudaError_t launchResolveSrgb(const PixelAccum* accum, long long pixels, unsigned char* out,
                               const SrgbThresholds& table, cudaStream_t stream);

@@ -3,12 +3,15 @@
 // PixelBuffer::average (image/ppm.cpp:22-33, image/pixel_buffer.cpp:37-45,
 // color/srgb.cpp:18-36).
 //
-// The average is sum / count in FP64 (correctly rounded, as on the host). Its
-// byte comes from a table of 255 thresholds (the smallest double of each byte,
-// computed on the host with the reference's own transfer function): an FP32
-// estimate picks a starting byte and comparisons against the table correct it,
-// so the result is the reference's byte exactly and the kernel evaluates no
-// FP64 power function. A pure stream: 32 bytes read and 3 written per pixel.
+// The average is sum / count in FP64, correctly rounded as on the host; a count
+// that is a power of two multiplies by its exact reciprocal instead, which rounds
+// the same real number the same way. The byte comes from the host's tables: 255
+// thresholds (the smallest double of each byte, found with the reference's own
+// transfer function) and a start byte per bucket of doubles (exponent and top 7
+// mantissa bits) that holds at most one threshold. One table read and one
+// comparison settle a channel, so the result is the reference's byte exactly and
+// the kernel evaluates no power function. A pure stream: 32 bytes read and 3
+// written per pixel.
 #include "launch.hpp"
 
 #include <algorithm>
@@ -22,32 +25,42 @@ constexpr int kResolveThreads{256};
 // Pixels per thread: 4 pixels are 12 output bytes, three aligned 32-bit words.
 constexpr int kResolveGroup{4};
 
-__device__ __forceinline__ unsigned int srgbByteOf(double v, const double* lower)
+__device__ __forceinline__ unsigned int srgbByteOf(double v, double lowest, double highest, const double* lower,
+                                                   const unsigned char* start)
 {
-    // NaN, zero and negative averages fail the first test; 1.0 and above pass
-    // the second.
-    if (!(v >= lower[1])) {
+    // NaN, zero and negative averages fail the first test (byte 0); 1.0 and
+    // above pass the second (byte 255). Between them v lies in a bucket:
+    // lower[1] > 2^-13 and lower[255] <= 1.
+    if (!(v >= lowest)) {
         return 0u;
     }
-    if (v >= lower[255]) {
+    if (v >= highest) {
         return 255u;
     }
-    const float f{static_cast<float>(v)};
-    const float e{f <= 0.0031308f ? 12.92f * f : 1.055f * __powf(f, 1.0f / 2.4f) - 0.055f};
-    int b{min(max(__float2int_rn(e * 255.0f), 1), 254)};
-    // lower[1] <= v < lower[255], so both loops end inside [1, 254].
-    while (v < lower[b]) {
-        --b;
-    }
-    while (v >= lower[b + 1]) {
-        ++b;
-    }
-    return static_cast<unsigned int>(b);
+    const int bucket{static_cast<int>((__double_as_longlong(v) >> kResolveBucketShift) - kResolveBucketBase)};
+    const unsigned int b{start[bucket]};
+    return b + (v >= lower[b + 1] ? 1u : 0u);
 }
 
-__device__ __forceinline__ double averageOf(double sum, long long count)
+// PixelBuffer::average (image/pixel_buffer.cpp:37-45): the count is unsigned.
+struct Divisor {
+    unsigned long long count;
+    double reciprocal;  // 2^-k when count = 2^k, else 0
+};
+
+__device__ __forceinline__ Divisor divisorOf(unsigned long long count)
 {
-    return count == 0 ? 0.0 : sum / static_cast<double>(count);
+    const bool power_of_two{count != 0 && (count & (count - 1)) == 0};
+    const long long k{63 - __clzll(static_cast<long long>(count))};
+    return {count, power_of_two ? __longlong_as_double((1023 - k) << 52) : 0.0};
+}
+
+__device__ __forceinline__ double averageOf(double sum, const Divisor& d)
+{
+    if (d.count == 0) {
+        return 0.0;
+    }
+    return d.reciprocal != 0.0 ? sum * d.reciprocal : sum / static_cast<double>(d.count);
 }
 
 // ALIGNED: accumulators 16-byte aligned (two 16-byte loads a pixel) and the
@@ -59,10 +72,16 @@ __global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const Pixel
                                                                       SrgbThresholds table)
 {
     __shared__ double lower[256];
+    __shared__ unsigned char start[kResolveBuckets];
     for (int i{static_cast<int>(threadIdx.x)}; i < 256; i += blockDim.x) {
         lower[i] = table.lower[i];
     }
+    for (int i{static_cast<int>(threadIdx.x)}; i < kResolveBuckets; i += blockDim.x) {
+        start[i] = table.start[i];
+    }
     __syncthreads();
+    const double lowest{lower[1]};
+    const double highest{lower[255]};
 
     const long long groups{(pixels + kResolveGroup - 1) / kResolveGroup};
     const long long stride{static_cast<long long>(gridDim.x) * blockDim.x};
@@ -73,7 +92,7 @@ __global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const Pixel
 #pragma unroll
         for (int p{0}; p < kResolveGroup; ++p) {
             double r{0.0}, gr{0.0}, bl{0.0};
-            long long count{0};
+            unsigned long long count{0};
             if (p < n) {
                 const PixelAccum* a{accum + first + p};
                 if constexpr (ALIGNED) {
@@ -82,17 +101,18 @@ __global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const Pixel
                     r = rg.x;
                     gr = rg.y;
                     bl = bc.x;
-                    count = __double_as_longlong(bc.y);
+                    count = static_cast<unsigned long long>(__double_as_longlong(bc.y));
                 } else {
                     r = __ldcs(&a->r);
                     gr = __ldcs(&a->g);
                     bl = __ldcs(&a->b);
-                    count = __ldcs(&a->count);
+                    count = static_cast<unsigned long long>(__ldcs(&a->count));
                 }
             }
-            bytes[3 * p + 0] = srgbByteOf(averageOf(r, count), lower);
-            bytes[3 * p + 1] = srgbByteOf(averageOf(gr, count), lower);
-            bytes[3 * p + 2] = srgbByteOf(averageOf(bl, count), lower);
+            const Divisor d{divisorOf(count)};
+            bytes[3 * p + 0] = srgbByteOf(averageOf(r, d), lowest, highest, lower, start);
+            bytes[3 * p + 1] = srgbByteOf(averageOf(gr, d), lowest, highest, lower, start);
+            bytes[3 * p + 2] = srgbByteOf(averageOf(bl, d), lowest, highest, lower, start);
         }
         unsigned char* dst{out + 3 * first};
         if (ALIGNED && n == kResolveGroup) {

@@ -239,10 +239,14 @@ int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* jo
  * bytes a pixel to the host by one of 3. */
 int albedo_resolve_srgb(const albedo_accumulator* accumulators, int32_t width, int32_t height, uint8_t* out_rgb,
                         void* stream);
-/* The 256 thresholds the resolve compares against: out_lower[b] (b = 1..255) is
- * the smallest positive double whose byte is at least b; out_lower[0] is
- * -infinity. Computed on the host from the reference's transfer function. */
-int albedo_srgb_thresholds(double* out_lower);
+/* The resolve's tables, computed on the host from the reference's transfer
+ * function. out_lower (256 doubles): [b] (b = 1..255) is the smallest positive
+ * double whose byte is at least b; [0] is -infinity. out_start (1664 bytes, or
+ * NULL): the byte at the smallest double of each bucket, where bucket k holds the
+ * doubles whose bit pattern shifted right by 45 is (1023 - 13) * 128 + k (an
+ * exponent and the top 7 mantissa bits, covering [2^-13, 1)); no bucket holds
+ * more than one threshold, so a value's byte is start or start + 1. */
+int albedo_srgb_tables(double* out_lower, uint8_t* out_start);
 /* writePpm(path, image) (image/ppm.cpp:61-85) from host bytes already encoded:
  * a binary P6 file with maxval 255. The file is truncated on open; on a failed
  * write the partial file is removed (when it is a regular file). Errors carry the

@@ -2,7 +2,9 @@
 
 The device resolve compares each pixel's average against a table of the
 smallest double of every byte, built with the reference's transfer function
-(color/srgb.cpp:18-36). Here the table is checked against the reference's own
+(color/srgb.cpp:18-36), starting from a per-bucket byte (buckets of doubles by
+exponent and top mantissa bits). Here both tables, and the kernel's steps
+restated in numpy, are checked against the reference's own
 toByte(encodeSrgb(x)) on the golden values of its tests
 (tests/color/srgb_test.cpp, tests/image/ppm_test.cpp), on millions of seeded
 values and on every value within 2,000 ulps of each threshold, where a rounding
@@ -29,6 +31,22 @@ def table_bytes(values: np.ndarray) -> np.ndarray:
     return np.where(np.isnan(values), 0, b).astype(np.uint8)
 
 
+def bucket_bytes(values: np.ndarray) -> np.ndarray:
+    """The device resolve's steps, in numpy: below lower[1] (or NaN) 0, from
+    lower[255] 255, else the bucket's start byte plus one comparison."""
+    lower, start = ab.srgb_tables()
+    v = np.asarray(values, dtype=np.float64)
+    out = np.zeros(v.shape, dtype=np.int64)
+    with np.errstate(invalid="ignore"):
+        mid = (v >= lower[1]) & (v < lower[255])
+        out[v >= lower[255]] = 255
+    bucket = (v[mid].view(np.int64) >> ab.SRGB_BUCKET_SHIFT) - ab.SRGB_BUCKET_BASE
+    assert bucket.min(initial=0) >= 0 and bucket.max(initial=0) < ab.SRGB_BUCKETS
+    b = start[bucket].astype(np.int64)
+    out[mid] = b + (v[mid] >= lower[b + 1])
+    return out.astype(np.uint8)
+
+
 def test_thresholds_are_increasing_and_bracket_the_byte_range():
     lower = ab.srgb_thresholds()
     assert lower[0] == -np.inf
@@ -49,6 +67,7 @@ def test_golden_values_from_the_reference_tests():
     expected = np.array([b for _, b in GOLDEN], dtype=np.uint8)
     assert np.array_equal(ref.srgb_bytes(values), expected)
     assert np.array_equal(table_bytes(values), expected)
+    assert np.array_equal(bucket_bytes(values), expected)
 
 
 @needs_ref
@@ -59,7 +78,9 @@ def test_table_equals_the_reference_on_seeded_values():
         np.exp(rng.uniform(np.log(1e-7), np.log(2.0), 2_000_000)),
         rng.uniform(0.0031, 0.00316, 200_000),  # around the segment switch
     ])
-    assert np.array_equal(table_bytes(values), ref.srgb_bytes(values))
+    theirs = ref.srgb_bytes(values)
+    assert np.array_equal(table_bytes(values), theirs)
+    assert np.array_equal(bucket_bytes(values), theirs)
 
 
 @needs_ref
@@ -67,13 +88,22 @@ def test_table_equals_the_reference_within_2000_ulps_of_every_threshold():
     lower = ab.srgb_thresholds()[1:]
     bits = lower.view(np.int64)[:, None] + np.arange(-2000, 2001, dtype=np.int64)[None, :]
     values = bits.reshape(-1).view(np.float64)
-    ours = table_bytes(values)
     theirs = ref.srgb_bytes(values)
-    assert np.array_equal(ours, theirs)
+    assert np.array_equal(table_bytes(values), theirs)
+    assert np.array_equal(bucket_bytes(values), theirs)
     # Each threshold is where the reference's byte steps up.
     assert np.array_equal(ref.srgb_bytes(lower), np.arange(1, 256, dtype=np.uint8))
     below = np.nextafter(lower, -np.inf)
     assert np.array_equal(ref.srgb_bytes(below), np.arange(0, 255, dtype=np.uint8))
+
+
+def test_every_bucket_holds_at_most_one_threshold():
+    lower, start = ab.srgb_tables()
+    edges = ((ab.SRGB_BUCKET_BASE + np.arange(ab.SRGB_BUCKETS + 1, dtype=np.int64)) << ab.SRGB_BUCKET_SHIFT).view(np.float64)
+    inside = np.searchsorted(lower[1:], edges[1:], side="left") - np.searchsorted(lower[1:], edges[:-1], side="right")
+    assert inside.max() <= 1
+    assert np.array_equal(start, table_bytes(edges[:-1]))
+    assert edges[0] < lower[1] and lower[255] <= edges[-1]
 
 
 TWO_PIXEL_PPM = b"P6\n2 1\n255\n\xFF\x00\x00\xBC\xBC\xBC"
