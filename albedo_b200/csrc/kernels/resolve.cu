@@ -21,9 +21,19 @@ namespace albedo_b200 {
 
 namespace {
 
+// Build-time launch shape: pixels per thread (a multiple of 4, so a thread's
+// output is whole aligned 32-bit words) and the minimum resident blocks per SM
+// the register budget must allow.
+#ifndef ALBEDO_RESOLVE_GROUP
+#define ALBEDO_RESOLVE_GROUP 4
+#endif
+#ifndef ALBEDO_RESOLVE_MIN_BLOCKS
+#define ALBEDO_RESOLVE_MIN_BLOCKS 1
+#endif
+
 constexpr int kResolveThreads{256};
-// Pixels per thread: 4 pixels are 12 output bytes, three aligned 32-bit words.
-constexpr int kResolveGroup{4};
+constexpr int kResolveGroup{ALBEDO_RESOLVE_GROUP};
+static_assert(kResolveGroup % 4 == 0, "a thread's pixels must fill whole 32-bit words");
 
 __device__ __forceinline__ unsigned int srgbByteOf(double v, double lowest, double highest, const double* lower,
                                                    const unsigned char* start)
@@ -65,8 +75,9 @@ __device__ __forceinline__ double averageOf(double sum, const Divisor& d)
 
 // ALIGNED: accumulators 16-byte aligned (two 16-byte loads a pixel) and the
 // output 4-byte aligned (word stores); otherwise 8-byte loads and byte stores.
+// Each thread resolves kResolveGroup consecutive pixels per grid-stride turn.
 template <bool ALIGNED>
-__global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const PixelAccum* __restrict__ accum,
+__global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS) resolveSrgbKernel(const PixelAccum* __restrict__ accum,
                                                                       long long pixels,
                                                                       unsigned char* __restrict__ out,
                                                                       SrgbThresholds table)
@@ -118,7 +129,7 @@ __global__ void __launch_bounds__(kResolveThreads) resolveSrgbKernel(const Pixel
         if (ALIGNED && n == kResolveGroup) {
             unsigned int* words{reinterpret_cast<unsigned int*>(dst)};
 #pragma unroll
-            for (int w{0}; w < 3; ++w) {
+            for (int w{0}; w < 3 * kResolveGroup / 4; ++w) {
                 __stcs(words + w, bytes[4 * w] | bytes[4 * w + 1] << 8 | bytes[4 * w + 2] << 16 |
                                       bytes[4 * w + 3] << 24);
             }
