@@ -16,6 +16,8 @@
  *   albedo_render_host          renderImage with a host PixelBuffer src/albedo/render/render_image.hpp:36-49
  *   albedo_trace_host           Scene::intersect                   src/albedo/scene/scene.hpp:69-75
  *   albedo_occluded_host        Scene::occluded                    src/albedo/scene/scene.hpp:86-88
+ *   albedo_resolve_srgb         writePpm's encodeRow               src/albedo/image/ppm.cpp:22-33
+ *   albedo_write_ppm/save_ppm   writePpm(path, image)              src/albedo/image/ppm.cpp:61-85
  *
  * Exceptions never cross the ABI: every call returns an albedo_status and leaves
  * a message in a thread-local string (albedo_last_error). Status values map to
