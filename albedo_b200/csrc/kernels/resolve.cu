@@ -11,7 +11,7 @@
 // mantissa bits) that holds at most one threshold. One table read and one
 // comparison settle a channel, so the result is the reference's byte exactly and
 // the kernel evaluates no power function. A pure stream: 32 bytes read and 3
-// written per pixel.
+// written per pixel, the reads as one coalesced 256-bit load per pixel.
 #include "launch.hpp"
 
 #include <algorithm>
@@ -21,35 +21,36 @@ namespace albedo_b200 {
 
 namespace {
 
-// Build-time launch shape: pixels per thread (a multiple of 4, so a thread's
-// output is whole aligned 32-bit words) and the minimum resident blocks per SM
-// the register budget must allow.
+// Build-time launch shape: pixels per lane in a warp's tile and the minimum
+// resident blocks per SM the register budget must allow.
 #ifndef ALBEDO_RESOLVE_GROUP
 #define ALBEDO_RESOLVE_GROUP 4
 #endif
 #ifndef ALBEDO_RESOLVE_MIN_BLOCKS
-#define ALBEDO_RESOLVE_MIN_BLOCKS 1
+#define ALBEDO_RESOLVE_MIN_BLOCKS 4
 #endif
 
 constexpr int kResolveThreads{256};
 constexpr int kResolveGroup{ALBEDO_RESOLVE_GROUP};
-static_assert(kResolveGroup % 4 == 0, "a thread's pixels must fill whole 32-bit words");
 
 __device__ __forceinline__ unsigned int srgbByteOf(double v, double lowest, double highest, const double* lower,
                                                    const unsigned char* start)
 {
-    // NaN, zero and negative averages fail the first test (byte 0); 1.0 and
-    // above pass the second (byte 255). Between them v lies in a bucket:
-    // lower[1] > 2^-13 and lower[255] <= 1.
-    if (!(v >= lowest)) {
-        return 0u;
-    }
-    if (v >= highest) {
-        return 255u;
-    }
-    const int bucket{static_cast<int>((__double_as_longlong(v) >> kResolveBucketShift) - kResolveBucketBase)};
-    const unsigned int b{start[bucket]};
-    return b + (v >= lower[b + 1] ? 1u : 0u);
+    // Without branches: NaN, zero and negative averages fail `in_range` (byte
+    // 0); 1.0 and above pass `saturated` (byte 255). Between them v lies in a
+    // bucket, since lower[1] > 2^-13 and lower[255] <= 1; outside, the bucket
+    // and the start byte are clamped so every table read stays in bounds, and
+    // the selects discard what they give. The bucket is the high word of v
+    // shifted right by kResolveBucketShift - 32.
+    const bool in_range{v >= lowest};
+    const bool saturated{v >= highest};
+    const int bucket{min(max((__double2hiint(v) >> (kResolveBucketShift - 32)) -
+                                 static_cast<int>(kResolveBucketBase),
+                             0),
+                         kResolveBuckets - 1)};
+    const unsigned int b{min(static_cast<unsigned int>(start[bucket]), 254u)};
+    const unsigned int byte{b + (v >= lower[b + 1] ? 1u : 0u)};
+    return saturated ? 255u : (in_range ? byte : 0u);
 }
 
 // PixelBuffer::average (image/pixel_buffer.cpp:37-45): the count is unsigned.
@@ -73,17 +74,9 @@ __device__ __forceinline__ double averageOf(double sum, const Divisor& d)
     return d.reciprocal != 0.0 ? sum * d.reciprocal : sum / static_cast<double>(d.count);
 }
 
-// ALIGNED: accumulators 16-byte aligned (two 16-byte loads a pixel) and the
-// output 4-byte aligned (word stores); otherwise 8-byte loads and byte stores.
-// Each thread resolves kResolveGroup consecutive pixels per grid-stride turn.
-template <bool ALIGNED>
-__global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS) resolveSrgbKernel(const PixelAccum* __restrict__ accum,
-                                                                      long long pixels,
-                                                                      unsigned char* __restrict__ out,
-                                                                      SrgbThresholds table)
+// The tables into shared memory; every thread takes part.
+__device__ __forceinline__ void loadTables(const SrgbThresholds& table, double* lower, unsigned char* start)
 {
-    __shared__ double lower[256];
-    __shared__ unsigned char start[kResolveBuckets];
     for (int i{static_cast<int>(threadIdx.x)}; i < 256; i += blockDim.x) {
         lower[i] = table.lower[i];
     }
@@ -91,56 +84,125 @@ __global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS) re
         start[i] = table.start[i];
     }
     __syncthreads();
+}
+
+// One pixel's accumulator in one 256-bit load (sm_100 global vector load), marked
+// streaming: each accumulator is read once. The address is 32-byte aligned.
+__device__ __forceinline__ void loadPixel(const PixelAccum* a, double& r, double& g, double& b,
+                                          unsigned long long& count)
+{
+    double c;
+    asm("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+                 : "=d"(r), "=d"(g), "=d"(b), "=d"(c)
+                 : "l"(a));
+    count = static_cast<unsigned long long>(__double_as_longlong(c));
+}
+
+constexpr int kResolveWarps{kResolveThreads / 32};
+constexpr int kTilePixels{32 * kResolveGroup};
+constexpr int kTileBytes{3 * kTilePixels};  // 96 * kResolveGroup: whole 16-byte units
+
+// One warp tile into the warp's stage: lane l resolves pixels l, l + 32, ...
+// of the tile's n. FULL tiles (n == kTilePixels) need no bounds tests, so the
+// loads and the byte computations run as straight-line code the compiler can
+// interleave.
+template <bool FULL>
+__device__ __forceinline__ void resolveTile(const PixelAccum* tile, int n, int lane, unsigned char* stage,
+                                            double lowest, double highest, const double* lower,
+                                            const unsigned char* start)
+{
+    double r[kResolveGroup], g[kResolveGroup], b[kResolveGroup];
+    unsigned long long count[kResolveGroup];
+#pragma unroll
+    for (int j{0}; j < kResolveGroup; ++j) {
+        const int q{lane + 32 * j};
+        r[j] = g[j] = b[j] = 0.0;
+        count[j] = 0;
+        if (FULL || q < n) {
+            loadPixel(tile + q, r[j], g[j], b[j], count[j]);
+        }
+    }
+#pragma unroll
+    for (int j{0}; j < kResolveGroup; ++j) {
+        const int q{lane + 32 * j};
+        if (FULL || q < n) {
+            const Divisor d{divisorOf(count[j])};
+            stage[3 * q + 0] =
+                static_cast<unsigned char>(srgbByteOf(averageOf(r[j], d), lowest, highest, lower, start));
+            stage[3 * q + 1] =
+                static_cast<unsigned char>(srgbByteOf(averageOf(g[j], d), lowest, highest, lower, start));
+            stage[3 * q + 2] =
+                static_cast<unsigned char>(srgbByteOf(averageOf(b[j], d), lowest, highest, lower, start));
+        }
+    }
+}
+
+// Accumulators 32-byte aligned and output 16-byte aligned. Each warp resolves
+// tiles of kTilePixels pixels: lane l takes pixels l, l + 32, ..., so each of
+// its kResolveGroup loads is one coalesced 1 KB read across the warp. The bytes
+// are transposed through the warp's shared-memory stage and leave as coalesced
+// 16-byte stores.
+__global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS)
+    resolveSrgbTiles(const PixelAccum* __restrict__ accum, long long pixels, unsigned char* __restrict__ out,
+                     SrgbThresholds table)
+{
+    __shared__ double lower[256];
+    __shared__ unsigned char start[kResolveBuckets];
+    __shared__ __align__(16) unsigned char stage[kResolveWarps][kTileBytes];
+    loadTables(table, lower, start);
     const double lowest{lower[1]};
     const double highest{lower[255]};
+    const int lane{static_cast<int>(threadIdx.x) & 31};
+    const int warp{static_cast<int>(threadIdx.x) >> 5};
+    unsigned char* my_stage{stage[warp]};
 
-    const long long groups{(pixels + kResolveGroup - 1) / kResolveGroup};
-    const long long stride{static_cast<long long>(gridDim.x) * blockDim.x};
-    for (long long g{static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x}; g < groups; g += stride) {
-        const long long first{g * kResolveGroup};
-        const int n{static_cast<int>(min(static_cast<long long>(kResolveGroup), pixels - first))};
-        unsigned int bytes[3 * kResolveGroup];
-#pragma unroll
-        for (int p{0}; p < kResolveGroup; ++p) {
-            double r{0.0}, gr{0.0}, bl{0.0};
-            unsigned long long count{0};
-            if (p < n) {
-                const PixelAccum* a{accum + first + p};
-                if constexpr (ALIGNED) {
-                    const double2 rg{__ldcs(reinterpret_cast<const double2*>(a))};
-                    const double2 bc{__ldcs(reinterpret_cast<const double2*>(a) + 1)};
-                    r = rg.x;
-                    gr = rg.y;
-                    bl = bc.x;
-                    count = static_cast<unsigned long long>(__double_as_longlong(bc.y));
-                } else {
-                    r = __ldcs(&a->r);
-                    gr = __ldcs(&a->g);
-                    bl = __ldcs(&a->b);
-                    count = static_cast<unsigned long long>(__ldcs(&a->count));
-                }
-            }
-            const Divisor d{divisorOf(count)};
-            bytes[3 * p + 0] = srgbByteOf(averageOf(r, d), lowest, highest, lower, start);
-            bytes[3 * p + 1] = srgbByteOf(averageOf(gr, d), lowest, highest, lower, start);
-            bytes[3 * p + 2] = srgbByteOf(averageOf(bl, d), lowest, highest, lower, start);
+    const long long tiles{(pixels + kTilePixels - 1) / kTilePixels};
+    const long long warps_total{static_cast<long long>(gridDim.x) * kResolveWarps};
+    for (long long t{static_cast<long long>(blockIdx.x) * kResolveWarps + warp}; t < tiles; t += warps_total) {
+        const long long first{t * kTilePixels};
+        const int n{static_cast<int>(min(static_cast<long long>(kTilePixels), pixels - first))};
+        if (n == kTilePixels) {
+            resolveTile<true>(accum + first, n, lane, my_stage, lowest, highest, lower, start);
+        } else {
+            resolveTile<false>(accum + first, n, lane, my_stage, lowest, highest, lower, start);
         }
+        __syncwarp();
         unsigned char* dst{out + 3 * first};
-        if (ALIGNED && n == kResolveGroup) {
-            unsigned int* words{reinterpret_cast<unsigned int*>(dst)};
-#pragma unroll
-            for (int w{0}; w < 3 * kResolveGroup / 4; ++w) {
-                __stcs(words + w, bytes[4 * w] | bytes[4 * w + 1] << 8 | bytes[4 * w + 2] << 16 |
-                                      bytes[4 * w + 3] << 24);
+        if (n == kTilePixels) {
+            for (int i{lane}; i < kTileBytes / 16; i += 32) {
+                __stcs(reinterpret_cast<uint4*>(dst) + i, reinterpret_cast<const uint4*>(my_stage)[i]);
             }
         } else {
-#pragma unroll
-            for (int i{0}; i < 3 * kResolveGroup; ++i) {
-                if (i < 3 * n) {
-                    dst[i] = static_cast<unsigned char>(bytes[i]);
-                }
+            for (int i{lane}; i < 3 * n; i += 32) {
+                dst[i] = my_stage[i];
             }
         }
+        __syncwarp();
+    }
+}
+
+// Any other alignment (accumulators at least 8-byte aligned): one pixel per
+// thread per turn, 8-byte loads and byte stores.
+__global__ void __launch_bounds__(kResolveThreads) resolveSrgbAnyAlignment(const PixelAccum* __restrict__ accum,
+                                                                            long long pixels,
+                                                                            unsigned char* __restrict__ out,
+                                                                            SrgbThresholds table)
+{
+    __shared__ double lower[256];
+    __shared__ unsigned char start[kResolveBuckets];
+    loadTables(table, lower, start);
+    const double lowest{lower[1]};
+    const double highest{lower[255]};
+    const long long stride{static_cast<long long>(gridDim.x) * blockDim.x};
+    for (long long p{static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x}; p < pixels; p += stride) {
+        const PixelAccum* a{accum + p};
+        const Divisor d{divisorOf(static_cast<unsigned long long>(__ldcs(&a->count)))};
+        out[3 * p + 0] = static_cast<unsigned char>(srgbByteOf(averageOf(__ldcs(&a->r), d), lowest, highest, lower,
+                                                               start));
+        out[3 * p + 1] = static_cast<unsigned char>(srgbByteOf(averageOf(__ldcs(&a->g), d), lowest, highest, lower,
+                                                               start));
+        out[3 * p + 2] = static_cast<unsigned char>(srgbByteOf(averageOf(__ldcs(&a->b), d), lowest, highest, lower,
+                                                               start));
     }
 }
 
@@ -163,16 +225,16 @@ cudaError_t launchResolveSrgb(const PixelAccum* accum, long long pixels, unsigne
     }
     // A grid-stride stream, one wave of resident blocks: all of them keep
     // loads in flight, enough to saturate HBM.
-    const bool aligned{(reinterpret_cast<std::uintptr_t>(accum) & 15) == 0 &&
-                       (reinterpret_cast<std::uintptr_t>(out) & 3) == 0};
-    const auto kernel{aligned ? resolveSrgbKernel<true> : resolveSrgbKernel<false>};
+    const bool tiled{(reinterpret_cast<std::uintptr_t>(accum) & 31) == 0 &&
+                     (reinterpret_cast<std::uintptr_t>(out) & 15) == 0};
+    const auto kernel{tiled ? resolveSrgbTiles : resolveSrgbAnyAlignment};
     int per_sm{0};
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kResolveThreads, 0);
     if (e != cudaSuccess) {
         return e;
     }
-    const long long groups{(pixels + kResolveGroup - 1) / kResolveGroup};
-    const long long wanted{(groups + kResolveThreads - 1) / kResolveThreads};
+    const long long per_block{tiled ? static_cast<long long>(kTilePixels) * kResolveWarps : kResolveThreads};
+    const long long wanted{(pixels + per_block - 1) / per_block};
     const int blocks{static_cast<int>(std::min(wanted, static_cast<long long>(std::max(per_sm, 1)) * sms))};
     kernel<<<blocks, kResolveThreads, 0, stream>>>(accum, pixels, out, table);
     return cudaGetLastError();

@@ -54,7 +54,7 @@ def to_device(acc: np.ndarray, byte_offset: int = 0):
 
 
 @pytest.mark.parametrize("shape", [(1, 1), (1, 3), (5, 7), (13, 1), (270, 480), (1080, 1920)])
-@pytest.mark.parametrize("offsets", [(0, 0), (8, 0), (0, 1), (8, 3)])
+@pytest.mark.parametrize("offsets", [(0, 0), (32, 16), (16, 0), (0, 4), (8, 0), (0, 1), (8, 3)])
 def test_resolve_is_bit_exact_with_the_reference(shape, offsets):
     import torch
 
