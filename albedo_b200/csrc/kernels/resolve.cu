@@ -9,7 +9,8 @@
 // thresholds (the smallest double of each byte, found with the reference's own
 // transfer function) and a start byte per bucket of doubles (exponent and top 7
 // mantissa bits) that holds at most one threshold. One table read and one
-// comparison settle a channel, so the result is the reference's byte exactly and
+// comparison settle a channel (the tiled kernel packs both tables into one
+// 64-bit entry per bucket), so the result is the reference's byte exactly and
 // the kernel evaluates no power function. A pure stream: 32 bytes read and 3
 // written per pixel, the reads as one coalesced 256-bit load per pixel.
 #include "launch.hpp"
@@ -102,14 +103,55 @@ constexpr int kResolveWarps{kResolveThreads / 32};
 constexpr int kTilePixels{32 * kResolveGroup};
 constexpr int kTileBytes{3 * kTilePixels};  // 96 * kResolveGroup: whole 16-byte units
 
+// The tiled kernel's form of the tables: one 64-bit entry per bucket, read
+// with one shared-memory load. Bits 48-55 hold the bucket's start byte s;
+// bits 0-45 hold the low kResolveBucketShift bits of lower[s + 1] when that
+// threshold lies in the bucket, else 2^kResolveBucketShift (above every value's
+// low bits). Doubles of one bucket share their high bits, so comparing low bits
+// compares the values.
+constexpr unsigned long long kLowBits{(1ull << kResolveBucketShift) - 1};
+constexpr unsigned long long kNoThreshold{1ull << kResolveBucketShift};
+
+__device__ __forceinline__ void packBuckets(const SrgbThresholds& table, unsigned long long* packed)
+{
+    for (int k{static_cast<int>(threadIdx.x)}; k < kResolveBuckets; k += blockDim.x) {
+        const unsigned int s{table.start[k]};
+        unsigned long long low{kNoThreshold};
+        if (s < 255) {
+            const long long t{__double_as_longlong(table.lower[s + 1])};
+            if ((t >> kResolveBucketShift) == kResolveBucketBase + k) {
+                low = static_cast<unsigned long long>(t) & kLowBits;
+            }
+        }
+        packed[k] = static_cast<unsigned long long>(s) << 48 | low;
+    }
+    __syncthreads();
+}
+
+// srgbByteOf with the packed table: one table read per channel.
+__device__ __forceinline__ unsigned int srgbBytePacked(double v, double lowest, double highest,
+                                                       const unsigned long long* packed)
+{
+    const bool in_range{v >= lowest};
+    const bool saturated{v >= highest};
+    const int bucket{min(max((__double2hiint(v) >> (kResolveBucketShift - 32)) -
+                                 static_cast<int>(kResolveBucketBase),
+                             0),
+                         kResolveBuckets - 1)};
+    const unsigned long long entry{packed[bucket]};
+    const unsigned long long low{static_cast<unsigned long long>(__double_as_longlong(v)) & kLowBits};
+    const unsigned int byte{static_cast<unsigned int>(entry >> 48) +
+                            (low >= (entry & (kNoThreshold | kLowBits)) ? 1u : 0u)};
+    return saturated ? 255u : (in_range ? byte : 0u);
+}
+
 // One warp tile into the warp's stage: lane l resolves pixels l, l + 32, ...
 // of the tile's n. FULL tiles (n == kTilePixels) need no bounds tests, so the
 // loads and the byte computations run as straight-line code the compiler can
 // interleave.
 template <bool FULL>
 __device__ __forceinline__ void resolveTile(const PixelAccum* tile, int n, int lane, unsigned char* stage,
-                                            double lowest, double highest, const double* lower,
-                                            const unsigned char* start)
+                                            double lowest, double highest, const unsigned long long* packed)
 {
     double r[kResolveGroup], g[kResolveGroup], b[kResolveGroup];
     unsigned long long count[kResolveGroup];
@@ -128,11 +170,11 @@ __device__ __forceinline__ void resolveTile(const PixelAccum* tile, int n, int l
         if (FULL || q < n) {
             const Divisor d{divisorOf(count[j])};
             stage[3 * q + 0] =
-                static_cast<unsigned char>(srgbByteOf(averageOf(r[j], d), lowest, highest, lower, start));
+                static_cast<unsigned char>(srgbBytePacked(averageOf(r[j], d), lowest, highest, packed));
             stage[3 * q + 1] =
-                static_cast<unsigned char>(srgbByteOf(averageOf(g[j], d), lowest, highest, lower, start));
+                static_cast<unsigned char>(srgbBytePacked(averageOf(g[j], d), lowest, highest, packed));
             stage[3 * q + 2] =
-                static_cast<unsigned char>(srgbByteOf(averageOf(b[j], d), lowest, highest, lower, start));
+                static_cast<unsigned char>(srgbBytePacked(averageOf(b[j], d), lowest, highest, packed));
         }
     }
 }
@@ -146,12 +188,11 @@ __global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS)
     resolveSrgbTiles(const PixelAccum* __restrict__ accum, long long pixels, unsigned char* __restrict__ out,
                      SrgbThresholds table)
 {
-    __shared__ double lower[256];
-    __shared__ unsigned char start[kResolveBuckets];
+    __shared__ unsigned long long packed[kResolveBuckets];
     __shared__ __align__(16) unsigned char stage[kResolveWarps][kTileBytes];
-    loadTables(table, lower, start);
-    const double lowest{lower[1]};
-    const double highest{lower[255]};
+    packBuckets(table, packed);
+    const double lowest{table.lower[1]};
+    const double highest{table.lower[255]};
     const int lane{static_cast<int>(threadIdx.x) & 31};
     const int warp{static_cast<int>(threadIdx.x) >> 5};
     unsigned char* my_stage{stage[warp]};
@@ -162,9 +203,9 @@ __global__ void __launch_bounds__(kResolveThreads, ALBEDO_RESOLVE_MIN_BLOCKS)
         const long long first{t * kTilePixels};
         const int n{static_cast<int>(min(static_cast<long long>(kTilePixels), pixels - first))};
         if (n == kTilePixels) {
-            resolveTile<true>(accum + first, n, lane, my_stage, lowest, highest, lower, start);
+            resolveTile<true>(accum + first, n, lane, my_stage, lowest, highest, packed);
         } else {
-            resolveTile<false>(accum + first, n, lane, my_stage, lowest, highest, lower, start);
+            resolveTile<false>(accum + first, n, lane, my_stage, lowest, highest, packed);
         }
         __syncwarp();
         unsigned char* dst{out + 3 * first};

@@ -3,8 +3,8 @@
 The device resolve compares each pixel's average against a table of the
 smallest double of every byte, built with the reference's transfer function
 (color/srgb.cpp:18-36), starting from a per-bucket byte (buckets of doubles by
-exponent and top mantissa bits). Here both tables, and the kernel's steps
-restated in numpy, are checked against the reference's own
+exponent and top mantissa bits). Here both tables, and the kernels' steps
+restated in numpy (two table reads, or one read of a packed entry), are checked against the reference's own
 toByte(encodeSrgb(x)) on the golden values of its tests
 (tests/color/srgb_test.cpp, tests/image/ppm_test.cpp), on millions of seeded
 values and on every value within 2,000 ulps of each threshold, where a rounding
@@ -47,6 +47,32 @@ def bucket_bytes(values: np.ndarray) -> np.ndarray:
     return out.astype(np.uint8)
 
 
+def packed_bytes(values: np.ndarray) -> np.ndarray:
+    """The tiled device kernel's steps, in numpy: one 64-bit entry per bucket
+    holding the start byte (bits 48-55) and the low bits of the bucket's
+    threshold (2^shift when it holds none), compared with the value's low bits."""
+    lower, start = ab.srgb_tables()
+    shift = ab.SRGB_BUCKET_SHIFT
+    low_mask, none = (1 << shift) - 1, 1 << shift
+    packed = np.empty(ab.SRGB_BUCKETS, dtype=np.uint64)
+    for k, st in enumerate(start.tolist()):
+        low = none
+        if st < 255:
+            t = int(lower[st + 1:st + 2].view(np.int64)[0])
+            if t >> shift == ab.SRGB_BUCKET_BASE + k:
+                low = t & low_mask
+        packed[k] = (int(st) << 48) | low
+    v = np.asarray(values, dtype=np.float64).reshape(-1)
+    bits = v.view(np.int64)
+    bucket = np.clip((bits >> shift) - ab.SRGB_BUCKET_BASE, 0, ab.SRGB_BUCKETS - 1)
+    entry = packed[bucket]
+    byte = (entry >> np.uint64(48)).astype(np.int64) + (
+        (bits.astype(np.uint64) & np.uint64(low_mask)) >= (entry & np.uint64((none | low_mask)))).astype(np.int64)
+    with np.errstate(invalid="ignore"):
+        out = np.where(v >= lower[255], 255, np.where(v >= lower[1], byte, 0))
+    return out.astype(np.uint8).reshape(np.shape(values))
+
+
 def test_thresholds_are_increasing_and_bracket_the_byte_range():
     lower = ab.srgb_thresholds()
     assert lower[0] == -np.inf
@@ -68,6 +94,7 @@ def test_golden_values_from_the_reference_tests():
     assert np.array_equal(ref.srgb_bytes(values), expected)
     assert np.array_equal(table_bytes(values), expected)
     assert np.array_equal(bucket_bytes(values), expected)
+    assert np.array_equal(packed_bytes(values), expected)
 
 
 @needs_ref
@@ -81,6 +108,7 @@ def test_table_equals_the_reference_on_seeded_values():
     theirs = ref.srgb_bytes(values)
     assert np.array_equal(table_bytes(values), theirs)
     assert np.array_equal(bucket_bytes(values), theirs)
+    assert np.array_equal(packed_bytes(values), theirs)
 
 
 @needs_ref
@@ -91,6 +119,7 @@ def test_table_equals_the_reference_within_2000_ulps_of_every_threshold():
     theirs = ref.srgb_bytes(values)
     assert np.array_equal(table_bytes(values), theirs)
     assert np.array_equal(bucket_bytes(values), theirs)
+    assert np.array_equal(packed_bytes(values), theirs)
     # Each threshold is where the reference's byte steps up.
     assert np.array_equal(ref.srgb_bytes(lower), np.arange(1, 256, dtype=np.uint8))
     below = np.nextafter(lower, -np.inf)
