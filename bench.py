@@ -106,36 +106,45 @@ RESOLVE_BYTES_PER_PIXEL = 32 + 3  # one accumulator read, three sRGB bytes writt
 def film_resolve_figures(flush, launches: int = 20) -> dict:
     """The film's device resolve (accumulators to sRGB bytes, bit-exact with the
     reference's writePpm bytes) on a 3840 x 2160 frame: 265 MB of accumulators,
-    more than L2, and L2 flushed between launches; each launch timed with CUDA
-    events. Algorithmic bytes: 32 read and 3 written per pixel."""
+    more than L2. Between launches a 256 MB read evicts them from L2 and leaves
+    it clean (a flush by writing would leave up to 126 MB of dirty lines for the
+    timed launch to write back). Each launch is timed with CUDA events.
+    Algorithmic bytes: 32 read and 3 written per pixel. Two sample counts: 64
+    (the bench frame's; a power of two, so the average is one multiplication) and
+    36 (an FP64 division per channel)."""
     import torch
 
     import albedo_b200 as ab
 
     pixels = RESOLVE_WIDTH * RESOLVE_HEIGHT
-    generator = torch.Generator(device="cuda").manual_seed(5)
-    acc = torch.rand((pixels, 4), dtype=torch.float64, device="cuda", generator=generator) * 64.0
-    acc.view(torch.int64)[:, 3] = 64
     out = torch.empty(3 * pixels, dtype=torch.uint8, device="cuda")
-    for _ in range(3):
-        ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
-    torch.cuda.synchronize()
-    ms = []
-    for i in range(launches):
-        flush.fill_(i & 0xFF)
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record()
-        ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
-        end.record()
-        end.synchronize()
-        ms.append(start.elapsed_time(end))
-    launch_s = statistics.median(ms) / 1e3
-    achieved = RESOLVE_BYTES_PER_PIXEL * pixels / launch_s / 1e9
     peak = measured_peaks().get("hbm_gbs") or 6650.0
-    return {"workload": f"{RESOLVE_WIDTH}x{RESOLVE_HEIGHT} accumulators to sRGB bytes", "launches": launches,
+    figures = {}
+    for count in (64, 36):
+        generator = torch.Generator(device="cuda").manual_seed(5)
+        acc = torch.rand((pixels, 4), dtype=torch.float64, device="cuda", generator=generator) * count
+        acc.view(torch.int64)[:, 3] = count
+        for _ in range(3):
+            ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(launches):
+            flush.max()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            ab.resolve_srgb(acc.data_ptr(), RESOLVE_WIDTH, RESOLVE_HEIGHT, out.data_ptr())
+            end.record()
+            end.synchronize()
+            ms.append(start.elapsed_time(end))
+        del acc
+        launch_s = statistics.median(ms) / 1e3
+        achieved = RESOLVE_BYTES_PER_PIXEL * pixels / launch_s / 1e9
+        figures[f"samples_{count}"] = {
             "us_per_launch": launch_s * 1e6, "gpixels_per_s": pixels / launch_s / 1e9,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "algorithmic_bytes_per_launch": RESOLVE_BYTES_PER_PIXEL * pixels},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_launch": RESOLVE_BYTES_PER_PIXEL * pixels}}
+    return {"workload": f"{RESOLVE_WIDTH}x{RESOLVE_HEIGHT} accumulators to sRGB bytes", "launches": launches,
+            "l2": "256 MB read between launches (clean L2; inputs larger than L2)", **figures,
             "d2h_bytes_per_frame": {"accumulators": 32 * pixels, "srgb": 3 * pixels}}
 
 
