@@ -38,13 +38,52 @@ struct Extents {
     Box3 centroids{};
 };
 
-// extentsOf, accel/bvh.cpp:70-78.
-Extents extentsOf(std::span<const Prim> prims)
+// Ranges of at least this many primitives are scanned on several threads.
+constexpr std::size_t kParallelScanMinimum{1 << 17};
+
+// Runs scan(chunk, range) over `chunks` contiguous pieces of `prims`, each on its
+// own thread (the first on the calling one).
+template <typename F>
+void scanChunks(std::span<const Prim> prims, unsigned chunks, F&& scan)
 {
+    const auto piece = [&](unsigned c) {
+        const std::size_t begin{prims.size() * c / chunks};
+        const std::size_t end{prims.size() * (c + 1) / chunks};
+        return prims.subspan(begin, end - begin);
+    };
+    std::vector<std::thread> workers;
+    for (unsigned c{1}; c < chunks; ++c) {
+        workers.emplace_back([&, c] { scan(c, piece(c)); });
+    }
+    scan(0u, piece(0));
+    for (std::thread& worker : workers) {
+        worker.join();
+    }
+}
+
+unsigned scanThreads(std::size_t count, unsigned threads)
+{
+    return count < kParallelScanMinimum ? 1u : threads;
+}
+
+// extentsOf, accel/bvh.cpp:70-78. Boxes merge by minimum and maximum, which
+// give the same result in any order, so large ranges merge per thread first.
+Extents extentsOf(std::span<const Prim> prims, unsigned threads = 1)
+{
+    const unsigned chunks{scanThreads(prims.size(), threads)};
+    std::vector<Extents> parts(chunks);
+    scanChunks(prims, chunks, [&](unsigned c, std::span<const Prim> range) {
+        Extents e;
+        for (const Prim& p : range) {
+            e.bounds = merged(e.bounds, p.bounds);
+            e.centroids = merged(e.centroids, p.centroid);
+        }
+        parts[c] = e;
+    });
     Extents e;
-    for (const Prim& p : prims) {
-        e.bounds = merged(e.bounds, p.bounds);
-        e.centroids = merged(e.centroids, p.centroid);
+    for (const Extents& part : parts) {
+        e.bounds = merged(e.bounds, part.bounds);
+        e.centroids = merged(e.centroids, part.centroids);
     }
     return e;
 }
@@ -87,14 +126,27 @@ struct Split {
     double cost{std::numeric_limits<double>::infinity()};
 };
 
-// bestSplitAlong, accel/bvh.cpp:134-160: bin, sweep from the right, then scan left.
-Split bestSplitAlong(std::span<const Prim> prims, const Extents& extents, std::size_t axis)
+// bestSplitAlong, accel/bvh.cpp:134-160: bin, sweep from the right, then scan
+// left. A bin is a box merge and a count, so large ranges bin per thread and
+// the per-thread bins merge into the same bins.
+Split bestSplitAlong(std::span<const Prim> prims, const Extents& extents, std::size_t axis, unsigned threads)
 {
+    const unsigned chunks{scanThreads(prims.size(), threads)};
+    std::vector<std::array<Bin, kBins>> parts(chunks);
+    scanChunks(prims, chunks, [&](unsigned c, std::span<const Prim> range) {
+        std::array<Bin, kBins> part{};
+        for (const Prim& p : range) {
+            Bin& bin{part[binOf(p.centroid, extents.centroids, axis)]};
+            bin.bounds = merged(bin.bounds, p.bounds);
+            ++bin.count;
+        }
+        parts[c] = part;
+    });
     std::array<Bin, kBins> bins{};
-    for (const Prim& p : prims) {
-        Bin& bin{bins[binOf(p.centroid, extents.centroids, axis)]};
-        bin.bounds = merged(bin.bounds, p.bounds);
-        ++bin.count;
+    for (const auto& part : parts) {
+        for (std::size_t k{0}; k < kBins; ++k) {
+            bins[k] = {merged(bins[k].bounds, part[k].bounds), bins[k].count + part[k].count};
+        }
     }
     std::array<Bin, kBins> right_of{};
     for (std::size_t bin{kBins - 1}; bin > 0; --bin) {
@@ -116,14 +168,14 @@ Split bestSplitAlong(std::span<const Prim> prims, const Extents& extents, std::s
 }
 
 // bestSplit, accel/bvh.cpp:163-176.
-std::optional<Split> bestSplit(std::span<const Prim> prims, const Extents& extents)
+std::optional<Split> bestSplit(std::span<const Prim> prims, const Extents& extents, unsigned threads)
 {
     std::optional<Split> best;
     for (std::size_t axis{0}; axis < 3; ++axis) {
         if (!(halfSpread(extents.centroids, axis) > 0)) {
             continue;
         }
-        const Split split{bestSplitAlong(prims, extents, axis)};
+        const Split split{bestSplitAlong(prims, extents, axis, threads)};
         if (!best || split.cost < best->cost) {
             best = split;
         }
@@ -137,11 +189,11 @@ struct Partition {
 };
 
 // partitionForSplit, accel/bvh.cpp:186-220.
-Partition partitionForSplit(std::span<Prim> prims, const Extents& extents, std::size_t depth)
+Partition partitionForSplit(std::span<Prim> prims, const Extents& extents, std::size_t depth, unsigned threads = 1)
 {
     const std::size_t count{prims.size()};
     if (depth < kSahDepthLimit) {
-        if (const auto split{bestSplit(prims, extents)}) {
+        if (const auto split{bestSplit(prims, extents, threads)}) {
             const double area{extents.bounds.surfaceArea()};
             const bool leaf_is_cheaper{static_cast<double>(count) * area <= kTraversalCost * area + split->cost};
             if (count <= kMaxLeaf && leaf_is_cheaper) {
@@ -214,8 +266,8 @@ std::unique_ptr<Piece> buildPiece(std::span<Prim> prims, std::size_t first, std:
         piece->total = piece->nodes.size();
         return piece;
     }
-    const Extents extents{extentsOf(prims)};
-    const Partition partition{partitionForSplit(prims, extents, depth)};
+    const Extents extents{extentsOf(prims, threads)};
+    const Partition partition{partitionForSplit(prims, extents, depth, threads)};
     if (partition.left_count == 0) {
         piece->nodes.push_back({.bounds = extents.bounds, .offset = first,
                                 .count = static_cast<std::uint32_t>(prims.size())});
