@@ -104,6 +104,8 @@ def test_table_equals_the_reference_on_seeded_values():
         rng.uniform(-0.1, 1.2, 2_000_000),
         np.exp(rng.uniform(np.log(1e-7), np.log(2.0), 2_000_000)),
         rng.uniform(0.0031, 0.00316, 200_000),  # around the segment switch
+        # Arbitrary bit patterns: every sign, exponent and NaN payload.
+        rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, 1_000_000, dtype=np.int64).view(np.float64),
     ])
     theirs = ref.srgb_bytes(values)
     assert np.array_equal(table_bytes(values), theirs)
