@@ -13,6 +13,7 @@
 #include <optional>
 #include <sstream>
 #include <string_view>
+#include <thread>
 #include <vector>
 
 namespace albedo_b200 {
@@ -162,16 +163,81 @@ public:
         : std::runtime_error{std::format("OBJ line {}: {}", line, problem)}
     {
     }
+    // The same error again, from its full message.
+    static ObjError fromMessage(const std::string& message) { return ObjError{message}; }
+
+private:
+    explicit ObjError(const std::string& message) : std::runtime_error{message} {}
 };
 
-ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
+// Calls on_line(line, index) for every line of `text` as std::getline splits
+// it: at each '\n', plus a last line when the text does not end with one.
+template <typename OnLine>
+void forEachTextLine(std::string_view text, OnLine&& on_line)
 {
-    std::ifstream file{path, std::ios::binary};
-    if (!file) {
-        throw std::runtime_error{"cannot open OBJ file"};
+    std::size_t index{0};
+    std::size_t begin{0};
+    while (begin < text.size()) {
+        const std::size_t end{text.find('\n', begin)};
+        if (end == std::string_view::npos) {
+            on_line(text.substr(begin), index);
+            return;
+        }
+        on_line(text.substr(begin, end - begin), index++);
+        begin = end + 1;
     }
+}
+
+// A piece of an OBJ text made of whole lines, with what its lines define. The
+// pieces of a large file are read on separate threads: a first pass counts each
+// piece's lines, vertices, texture coordinates and triangles, which gives every
+// piece the counts of all lines before it, and a second pass reads each piece
+// with those counts as if the lines before it had just been read. The pieces'
+// results are joined in order, and the error of the earliest failing line is the
+// one reported, so the result is the one-thread reader's, error messages
+// included.
+struct ObjPiece {
+    std::string_view text;
+    std::size_t lines{0};
+    std::size_t positions{0};
+    std::size_t uvs{0};
+    std::size_t triangles{0};
+};
+
+struct ObjPieceResult {
     ObjMesh mesh;
     bool every_face_textured{true};
+    std::size_t error_line{0};  // 0: no error
+    std::string error;
+};
+
+void countObjPiece(ObjPiece& piece)
+{
+    forEachTextLine(piece.text, [&](std::string_view line, std::size_t) {
+        ++piece.lines;
+        Words words{line.substr(0, line.find('#'))};
+        const auto keyword{words.next()};
+        if (keyword == "v") {
+            ++piece.positions;
+        } else if (keyword == "vt") {
+            ++piece.uvs;
+        } else if (keyword == "f") {
+            std::size_t corners{0};
+            while (words.next()) {
+                ++corners;
+            }
+            piece.triangles += corners >= 3 ? corners - 2 : 0;
+        }
+    });
+}
+
+// Reads one piece (geometry/obj.cpp's per-line rules) whose first line has
+// number `first_line` and follows `before` (the counts of all earlier lines).
+// Stops at the piece's first error and records it.
+void readObjPiece(std::string_view text, std::size_t first_line, const ObjPiece& before, const ObjBudget& budget,
+                  ObjPieceResult& out)
+{
+    ObjMesh& mesh{out.mesh};
     struct Corner {
         std::uint32_t position{};
         std::optional<std::uint32_t> texture;
@@ -213,14 +279,16 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
         }
         return index;
     };
-    forEachLine(
-        file, kMaxObjLine,
-        [&](std::string_view line, std::size_t number_of_line) {
-            line_number = number_of_line;
+    try {
+        forEachTextLine(text, [&](std::string_view line, std::size_t index) {
+            line_number = first_line + index;
+            if (line.size() > kMaxObjLine) {
+                fail(std::format("line longer than {} bytes", kMaxObjLine));
+            }
             Words words{line.substr(0, line.find('#'))};
             const auto keyword{words.next()};
             if (keyword == "v") {
-                if (mesh.positions.size() >= budget.vertices) {
+                if (before.positions + mesh.positions.size() >= budget.vertices) {
                     fail(std::format("more than {} vertices", budget.vertices));
                 }
                 std::array<double, 3> xyz{};
@@ -236,7 +304,7 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
                 }
                 mesh.positions.push_back({xyz[0], xyz[1], xyz[2]});
             } else if (keyword == "vt") {
-                if (mesh.uvs.size() >= budget.texture_coordinates) {
+                if (before.uvs + mesh.uvs.size() >= budget.texture_coordinates) {
                     fail(std::format("more than {} texture coordinates", budget.texture_coordinates));
                 }
                 const auto u{words.next()};
@@ -253,18 +321,20 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
                 mesh.uvs.push_back(uv);
             } else if (keyword == "f") {
                 corners.clear();
+                const std::size_t positions{before.positions + mesh.positions.size()};
+                const std::size_t uvs{before.uvs + mesh.uvs.size()};
                 while (const auto token{words.next()}) {
                     const std::size_t slash{token->find('/')};
                     const auto position{parseInteger(token->substr(0, slash))};
                     if (!position) {
                         fail("a face corner is not a valid index");
                     }
-                    Corner corner{resolved(*position, "vertex", mesh.positions.size()), std::nullopt};
+                    Corner corner{resolved(*position, "vertex", positions), std::nullopt};
                     if (slash != std::string_view::npos) {
                         const std::string_view rest{token->substr(slash + 1)};
                         const std::size_t second{rest.find('/')};
                         if (const auto texture{optional_index(rest.substr(0, second))}) {
-                            corner.texture = resolved(*texture, "texture coordinate", mesh.uvs.size());
+                            corner.texture = resolved(*texture, "texture coordinate", uvs);
                         }
                         if (second != std::string_view::npos) {
                             static_cast<void>(optional_index(rest.substr(second + 1)));
@@ -275,7 +345,7 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
                 if (corners.size() < 3) {
                     fail("a face needs at least three corners");
                 }
-                if (corners.size() - 2 > budget.triangles - mesh.faces.size()) {
+                if (corners.size() - 2 > budget.triangles - (before.triangles + mesh.faces.size())) {
                     fail(std::format("more than {} triangles", budget.triangles));
                 }
                 for (std::size_t c{1}; c + 1 < corners.size(); ++c) {
@@ -284,21 +354,139 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
                     const Corner& d{corners[c + 1]};
                     mesh.faces.push_back({a.position, b.position, d.position});
                     if (!a.texture || !b.texture || !d.texture) {
-                        every_face_textured = false;
+                        out.every_face_textured = false;
                         mesh.texture_faces.clear();
-                    } else if (every_face_textured) {
+                    } else if (out.every_face_textured) {
                         mesh.texture_faces.push_back({*a.texture, *b.texture, *d.texture});
                     }
                 }
             }
-        },
-        [&](std::size_t number_of_line) {
-            throw ObjError{number_of_line, std::format("line longer than {} bytes", kMaxObjLine)};
         });
-    if (!every_face_textured) {
-        mesh.texture_faces.clear();
+    } catch (const ObjError& error) {
+        out.error_line = line_number;
+        out.error = error.what();
+    }
+}
+
+// Pieces of at least this many bytes are worth a thread of their own.
+constexpr std::size_t kObjPieceBytes{std::size_t{1} << 20U};
+
+// geometry/obj.cpp's reader over text in memory, in `pieces` pieces (1: one
+// thread); the result does not depend on the number of pieces.
+ObjMesh parseObj(std::string_view text, const ObjBudget& budget, unsigned pieces)
+{
+    // Split at line ends near equal byte offsets.
+    std::vector<ObjPiece> parts;
+    std::size_t begin{0};
+    for (unsigned k{1}; k <= pieces && begin < text.size(); ++k) {
+        std::size_t end{k == pieces ? text.size() : text.size() / pieces * k};
+        if (end < begin) {
+            end = begin;
+        }
+        if (end < text.size()) {
+            const std::size_t newline{text.find('\n', end == 0 ? 0 : end - 1)};
+            end = newline == std::string_view::npos ? text.size() : newline + 1;
+        }
+        if (end > begin) {
+            parts.push_back({.text = text.substr(begin, end - begin)});
+            begin = end;
+        }
+    }
+    const auto onThreads = [&](auto&& work) {
+        std::vector<std::thread> workers;
+        for (std::size_t k{1}; k < parts.size(); ++k) {
+            workers.emplace_back([&, k] { work(k); });
+        }
+        if (!parts.empty()) {
+            work(0);
+        }
+        for (std::thread& worker : workers) {
+            worker.join();
+        }
+    };
+    if (parts.size() > 1) {
+        onThreads([&](std::size_t k) { countObjPiece(parts[k]); });
+    }
+    // The counts of all lines before each piece.
+    std::vector<ObjPiece> before(parts.size());
+    for (std::size_t k{1}; k < parts.size(); ++k) {
+        before[k] = {.lines = before[k - 1].lines + parts[k - 1].lines,
+                     .positions = before[k - 1].positions + parts[k - 1].positions,
+                     .uvs = before[k - 1].uvs + parts[k - 1].uvs,
+                     .triangles = before[k - 1].triangles + parts[k - 1].triangles};
+    }
+    std::vector<ObjPieceResult> results(parts.size());
+    std::vector<std::exception_ptr> failures(parts.size());
+    onThreads([&](std::size_t k) {
+        try {
+            readObjPiece(parts[k].text, before[k].lines + 1, before[k], budget, results[k]);
+        } catch (...) {
+            failures[k] = std::current_exception();
+        }
+    });
+    // The earliest failure in file order is the one the one-thread reader meets.
+    for (std::size_t k{0}; k < parts.size(); ++k) {
+        if (failures[k]) {
+            std::rethrow_exception(failures[k]);
+        }
+        if (results[k].error_line != 0) {
+            throw ObjError::fromMessage(results[k].error);
+        }
+    }
+    if (results.size() == 1) {
+        ObjMesh mesh{std::move(results[0].mesh)};
+        if (!results[0].every_face_textured) {
+            mesh.texture_faces.clear();
+        }
+        return mesh;
+    }
+    ObjMesh mesh;
+    bool every_face_textured{true};
+    std::size_t positions{0}, uvs{0}, faces{0};
+    for (const ObjPieceResult& r : results) {
+        positions += r.mesh.positions.size();
+        uvs += r.mesh.uvs.size();
+        faces += r.mesh.faces.size();
+        every_face_textured = every_face_textured && r.every_face_textured;
+    }
+    mesh.positions.reserve(positions);
+    mesh.uvs.reserve(uvs);
+    mesh.faces.reserve(faces);
+    for (const ObjPieceResult& r : results) {
+        mesh.positions.insert(mesh.positions.end(), r.mesh.positions.begin(), r.mesh.positions.end());
+        mesh.uvs.insert(mesh.uvs.end(), r.mesh.uvs.begin(), r.mesh.uvs.end());
+        mesh.faces.insert(mesh.faces.end(), r.mesh.faces.begin(), r.mesh.faces.end());
+    }
+    if (every_face_textured) {
+        mesh.texture_faces.reserve(faces);
+        for (const ObjPieceResult& r : results) {
+            mesh.texture_faces.insert(mesh.texture_faces.end(), r.mesh.texture_faces.begin(),
+                                      r.mesh.texture_faces.end());
+        }
     }
     return mesh;
+}
+
+ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
+{
+    std::ifstream file{path, std::ios::binary};
+    if (!file) {
+        throw std::runtime_error{"cannot open OBJ file"};
+    }
+    std::string text;
+    std::array<char, 1 << 16> block{};
+    while (file.read(block.data(), static_cast<std::streamsize>(block.size())) || file.gcount() > 0) {
+        text.append(block.data(), static_cast<std::size_t>(file.gcount()));
+        if (file.eof()) {
+            break;
+        }
+    }
+    if (file.bad()) {
+        throw std::runtime_error{"reading failed"};
+    }
+    const unsigned threads{std::max(1u, std::thread::hardware_concurrency())};
+    const auto pieces{static_cast<unsigned>(std::clamp<std::size_t>(text.size() / kObjPieceBytes, 1, threads))};
+    return parseObj(text, budget, pieces);
 }
 
 // ---------------------------------------------------------------- scene reading
