@@ -9,6 +9,8 @@
 #include <cmath>
 #include <format>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 namespace albedo_b200 {
 
@@ -80,20 +82,22 @@ Emitted emitBvh(const BuiltBvh& bvh, std::uint64_t prim_base, std::vector<DevNod
     // Heads are discovered in order; their children are filled afterwards.
     for (std::size_t h{0}; h < heads.size(); ++h) {
         const std::size_t i{heads[h]};
-        std::vector<std::size_t> slots;
+        std::array<std::size_t, 4> slots{};
+        std::size_t used{0};
         if (isLeaf(i)) {
-            slots.push_back(i);
+            slots[used++] = i;
         } else {
             for (const std::size_t x : {i + 1, secondOf(i)}) {
                 if (isLeaf(x)) {
-                    slots.push_back(x);
+                    slots[used++] = x;
                 } else {
-                    slots.push_back(x + 1);
-                    slots.push_back(secondOf(x));
+                    slots[used++] = x + 1;
+                    slots[used++] = secondOf(x);
                 }
             }
         }
-        for (const std::size_t s : slots) {
+        for (std::size_t k{0}; k < used; ++k) {
+            const std::size_t s{slots[k]};
             if (!isLeaf(s) && device_index[s] == kEmptyChild) {
                 device_index[s] = static_cast<std::uint32_t>(out.size());
                 out.emplace_back();
@@ -339,9 +343,29 @@ DeviceImage flattenScene(const HostScene& scene)
         const MeshDesc& mesh{scene.meshes[m]};
         const std::uint64_t base{image.triangles.size()};
         image.mesh_triangle_base.push_back(static_cast<std::uint32_t>(base));
-        for (const std::uint32_t t : mesh.bvh.order) {
-            image.triangles.push_back(deviceTriangle(mesh.triangles[t], t));
-            image.attrs.push_back(deviceAttr(mesh.triangles[t], mesh.corner_normals.empty() ? nullptr : &mesh.corner_normals[t]));
+        // Each triangle converts on its own, so large meshes convert in chunks
+        // on several threads.
+        const std::size_t count{mesh.bvh.order.size()};
+        image.triangles.resize(base + count);
+        image.attrs.resize(base + count);
+        const std::size_t chunks{count < (std::size_t{1} << 16)
+                                     ? 1
+                                     : std::max<std::size_t>(1, std::thread::hardware_concurrency())};
+        std::vector<std::thread> workers;
+        const auto convert = [&](std::size_t chunk) {
+            for (std::size_t pos{count * chunk / chunks}; pos < count * (chunk + 1) / chunks; ++pos) {
+                const std::uint32_t t{mesh.bvh.order[pos]};
+                image.triangles[base + pos] = deviceTriangle(mesh.triangles[t], t);
+                image.attrs[base + pos] =
+                    deviceAttr(mesh.triangles[t], mesh.corner_normals.empty() ? nullptr : &mesh.corner_normals[t]);
+            }
+        };
+        for (std::size_t chunk{1}; chunk < chunks; ++chunk) {
+            workers.emplace_back(convert, chunk);
+        }
+        convert(0);
+        for (std::thread& worker : workers) {
+            worker.join();
         }
         const Emitted blas{emitBvh(mesh.bvh, base, image.nodes)};
         mesh_root[m] = blas.root;
