@@ -148,3 +148,37 @@ def test_mutated_inputs_are_accepted_or_refused_alike(tmp_path, target):
         accepted += ours[0] == "ok"
         refused += ours[0] == "error"
     assert accepted > 10 and refused > 10, (accepted, refused)
+
+
+def large_obj(rng: random.Random, vertices: int) -> str:
+    """A mesh file of several MB: the reader splits files this large into pieces
+    read on separate threads."""
+    lines = []
+    for i in range(vertices):
+        lines.append(f"v {rng.uniform(-1, 1):.9f} {rng.uniform(-1, 1):.9f} {rng.uniform(-1, 1):.9f}")
+        lines.append(f"vt {rng.random():.6f} {rng.random():.6f}")
+        if i >= 2:
+            lines.append(f"f {i - 1}/{i - 1} {i}/{i} -1/-1")
+    return "\n".join(lines) + "\n"
+
+
+def test_large_meshes_with_late_errors_read_alike(tmp_path):
+    # Errors placed anywhere in a file of about 5 MB, so in any of its pieces.
+    rng = random.Random(21)
+    base = large_obj(rng, 60_000).split("\n")
+    scene = "camera from 0 0 5 at 0 0 0 up 0 1 0 fov 40\nmaterial white diffuse color 0.5 0.5 0.5\n" \
+            "mesh big big.obj\ninstance big material white\n"
+    outcomes = []
+    for k in range(12):
+        lines = list(base)
+        if k > 0:
+            i = rng.randrange(len(lines) - 1)
+            lines[i] = rng.choice([lines[i] + " junk", "f 1 2", f"f {10 ** 9} 1 2", "v 1 nan 2", "vt", lines[i]])
+        case = tmp_path / f"case{k}"
+        case.mkdir()
+        (case / "big.obj").write_text("\n".join(lines))
+        (case / "case.scene").write_text(scene)
+        ours, theirs = read_ours(case / "case.scene"), read_theirs(case / "case.scene")
+        assert ours == theirs, (k, ours, theirs)
+        outcomes.append(ours[0])
+    assert "ok" in outcomes and "error" in outcomes
