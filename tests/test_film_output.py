@@ -47,10 +47,10 @@ def bucket_bytes(values: np.ndarray) -> np.ndarray:
     return out.astype(np.uint8)
 
 
-def packed_bytes(values: np.ndarray) -> np.ndarray:
-    """The tiled device kernel's steps, in numpy: one 64-bit entry per bucket
-    holding the start byte (bits 48-55) and the low bits of the bucket's
-    threshold (2^shift when it holds none), compared with the value's low bits."""
+def packed_table() -> np.ndarray:
+    """The tiled kernel's table: one 64-bit entry per bucket holding the start
+    byte (bits 48-55) and the low bits of the bucket's threshold (2^shift when it
+    holds none)."""
     lower, start = ab.srgb_tables()
     shift = ab.SRGB_BUCKET_SHIFT
     low_mask, none = (1 << shift) - 1, 1 << shift
@@ -62,6 +62,16 @@ def packed_bytes(values: np.ndarray) -> np.ndarray:
             if t >> shift == ab.SRGB_BUCKET_BASE + k:
                 low = t & low_mask
         packed[k] = (int(st) << 48) | low
+    return packed
+
+
+def packed_bytes(values: np.ndarray) -> np.ndarray:
+    """The tiled device kernel's byte lookup, in numpy: one packed entry per
+    bucket, its threshold's low bits compared with the value's."""
+    lower = ab.srgb_thresholds()
+    packed = packed_table()
+    shift = ab.SRGB_BUCKET_SHIFT
+    low_mask, none = (1 << shift) - 1, 1 << shift
     v = np.asarray(values, dtype=np.float64).reshape(-1)
     bits = v.view(np.int64)
     bucket = np.clip((bits >> shift) - ab.SRGB_BUCKET_BASE, 0, ab.SRGB_BUCKETS - 1)
@@ -71,6 +81,29 @@ def packed_bytes(values: np.ndarray) -> np.ndarray:
     with np.errstate(invalid="ignore"):
         out = np.where(v >= lower[255], 255, np.where(v >= lower[1], byte, 0))
     return out.astype(np.uint8).reshape(np.shape(values))
+
+
+def adversarial_accumulators():
+    """Sums whose averages fall within 6 ulps of every threshold and bucket edge,
+    for counts that are and are not powers of two."""
+    lower = ab.srgb_thresholds()[1:]
+    edges = ((ab.SRGB_BUCKET_BASE + np.arange(ab.SRGB_BUCKETS + 1, dtype=np.int64)) << ab.SRGB_BUCKET_SHIFT
+             ).view(np.float64)
+    targets = np.concatenate([lower, edges])
+    sums, counts = [], []
+    for c in (3, 7, 36, 49, 64, 255, 1_000_003, 2**40 + 3):
+        s0 = (targets * float(c)).view(np.int64)
+        for d in range(-6, 7):
+            sums.append((s0 + d).view(np.float64))
+            counts.append(np.full(len(targets), c, dtype=np.uint64))
+    return np.concatenate(sums), np.concatenate(counts)
+
+
+def reference_average_bytes(sums, counts):
+    c = np.asarray(counts, dtype=np.uint64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        avg = np.where(c > 0, sums / np.where(c > 0, c.astype(np.float64), 1.0), 0.0)
+    return ref.srgb_bytes(avg)
 
 
 def test_thresholds_are_increasing_and_bracket_the_byte_range():
@@ -126,6 +159,14 @@ def test_table_equals_the_reference_within_2000_ulps_of_every_threshold():
     assert np.array_equal(ref.srgb_bytes(lower), np.arange(1, 256, dtype=np.uint8))
     below = np.nextafter(lower, -np.inf)
     assert np.array_equal(ref.srgb_bytes(below), np.arange(0, 255, dtype=np.uint8))
+
+
+@needs_ref
+def test_averages_next_to_every_decision_give_the_reference_bytes():
+    sums, counts = adversarial_accumulators()
+    with np.errstate(invalid="ignore"):
+        averages = sums / counts.astype(np.float64)
+    np.testing.assert_array_equal(packed_bytes(averages), reference_average_bytes(sums, counts))
 
 
 def test_every_bucket_holds_at_most_one_threshold():

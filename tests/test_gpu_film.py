@@ -9,6 +9,8 @@ the same way. A rendered image saved by save_ppm is byte-identical to the file
 the reference's writePpm writes for the same averages.
 """
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -69,6 +71,28 @@ def test_resolve_is_bit_exact_with_the_reference(shape, offsets):
     assert np.array_equal(got[out_offset:out_offset + 3 * w * h], expected_bytes(acc))
     # Nothing outside the image is written.
     assert np.all(got[:out_offset] == 77) and np.all(got[out_offset + 3 * w * h:] == 77)
+
+
+def test_averages_next_to_every_decision_resolve_exactly():
+    # Averages within 6 ulps of every threshold and bucket edge, for counts that
+    # are and are not powers of two (test_film_output.py builds them): a quotient
+    # rounded the wrong way, or a table read from the wrong bucket, shows here.
+    import sys
+    import torch
+
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from test_film_output import adversarial_accumulators, reference_average_bytes
+
+    sums, counts = adversarial_accumulators()
+    acc = np.zeros(len(sums), dtype=ab.ACCUMULATOR_DTYPE)
+    acc["r"], acc["g"], acc["b"] = sums, np.roll(sums, 1), np.roll(sums, 2)
+    acc["count"] = counts.astype(np.int64)
+    device, ptr = to_device(acc)
+    out = torch.empty(3 * len(sums), dtype=torch.uint8, device="cuda")
+    ab.resolve_srgb(ptr, len(sums), 1, out.data_ptr())
+    got = out.cpu().numpy().reshape(-1, 3)
+    for channel, values in enumerate((acc["r"], acc["g"], acc["b"])):
+        np.testing.assert_array_equal(got[:, channel], reference_average_bytes(values, counts))
 
 
 def test_resolve_at_the_largest_image_size():
