@@ -1,7 +1,10 @@
-// Scene-file and OBJ reading. Restates scene/scene_file.cpp (grammar, value
-// ranges, limits, mesh path rules, instance operations) and geometry/obj.cpp
-// (v / vt / f statements, fan triangulation, negative indices), with numbers
-// parsed by std::from_chars exactly as io/tokens.cpp:25-52 parses them.
+// Scene-file and OBJ reading for the reference's formats: the scene grammar of
+// scene/scene_file.cpp (statements, value ranges, limits, mesh path rules,
+// instance operations, messages) and the OBJ subset of geometry/obj.cpp (v / vt
+// / f statements, fan triangulation, negative indices), with numbers parsed by
+// std::from_chars as io/tokens.cpp:25-52 parses them. The scene grammar is
+// table-driven (see "scene reading" below); large OBJ files are read in pieces
+// on several threads.
 #include "scene_file.hpp"
 
 #include <algorithm>
@@ -11,9 +14,11 @@
 #include <functional>
 #include <map>
 #include <optional>
+#include <span>
 #include <sstream>
 #include <string_view>
 #include <thread>
+#include <variant>
 #include <vector>
 
 namespace albedo_b200 {
@@ -490,683 +495,771 @@ ObjMesh readObj(const std::filesystem::path& path, const ObjBudget& budget)
 }
 
 // ---------------------------------------------------------------- scene reading
+//
+// The scene grammar is held as data. A statement is a keyword, a few positional
+// values and a set of named fields, given in any order, each at most once. Every
+// value has a kind (a number, a positive number, a number in a range, a point, a
+// colour whose channels lie in a range, a material name), the noun its error
+// messages use, and its range. One loop reads the named fields of any statement
+// against its table and one function reads a value of any kind; a short builder
+// per statement then turns the values into scene content and checks what a table
+// cannot say: which fields are required (reported in the builder's order),
+// camera and sphere validity, mesh files and instance placement. The limits,
+// ranges and messages are the reference's (scene/scene_file.cpp:17-77 and its
+// statement readers), so a file is accepted or refused, with the same words, by
+// both readers.
 
-class Statement {
+// One line's words, read front to back; every error names the line.
+class LineWords {
 public:
-    Statement(std::string_view text, std::size_t line) : words{text}, line_number{line} {}
+    LineWords(std::string_view text, std::size_t line) : number{line}
+    {
+        Words split{text};
+        while (const auto word{split.next()}) {
+            words.push_back(*word);
+        }
+    }
 
-    [[noreturn]] void fail(const std::string& problem) const { throw SceneParseError{line_number, problem}; }
-    std::optional<std::string_view> next() { return words.next(); }
+    [[noreturn]] void fail(const std::string& problem) const { throw SceneParseError{number, problem}; }
+
+    bool done() const { return at == words.size(); }
     std::optional<std::string_view> peek() const
     {
-        Words rest{words};
-        return rest.next();
+        return done() ? std::nullopt : std::optional<std::string_view>{words[at]};
     }
-    std::string_view word(std::string_view what)
+    std::optional<std::string_view> take()
     {
-        const auto token{next()};
-        if (!token) {
-            fail(std::format("expected {}", what));
+        return done() ? std::nullopt : std::optional<std::string_view>{words[at++]};
+    }
+    // The next word, which must exist; `noun` names it when it does not.
+    std::string_view expect(std::string_view noun)
+    {
+        if (done()) {
+            fail(std::format("expected {}", noun));
         }
-        return *token;
+        return words[at++];
     }
-    double number(std::string_view what)
+    void end() const
     {
-        const std::string_view token{word(what)};
-        const auto value{parseReal(token)};
-        if (!value) {
-            fail(std::format("{} must be a finite number, got {}", what, quoted(token)));
-        }
-        return *value;
-    }
-    double inRange(std::string_view what, double low, double high)
-    {
-        const double value{number(what)};
-        if (value < low || value > high) {
-            fail(std::format("{} must be between {} and {}, got {}", what, low, high, value));
-        }
-        return value;
-    }
-    double positive(std::string_view what)
-    {
-        const double value{number(what)};
-        if (!(value > 0)) {
-            fail(std::format("{} must be positive, got {}", what, value));
-        }
-        return value;
-    }
-    Vec3 point(std::string_view what)
-    {
-        const double x{number(std::format("the x coordinate of {}", what))};
-        const double y{number(std::format("the y coordinate of {}", what))};
-        return {x, y, number(std::format("the z coordinate of {}", what))};
-    }
-    Rgb color(std::string_view what, double low, double high)
-    {
-        const double r{inRange(std::format("the red channel of {}", what), low, high)};
-        const double g{inRange(std::format("the green channel of {}", what), low, high)};
-        return {r, g, inRange(std::format("the blue channel of {}", what), low, high)};
-    }
-    Rgb reflectance(std::string_view what) { return color(what, 0, kMaxReflectance); }
-    Rgb emission(std::string_view what) { return color(what, 0, kMaxEmission); }
-    std::string_view name(std::string_view what)
-    {
-        const std::string_view token{word(what)};
-        if (!isIdentifier(token)) {
-            fail(std::format("{} is not a valid name", quoted(token)));
-        }
-        return token;
-    }
-    template <typename Read>
-    void readFields(Read read)
-    {
-        std::vector<std::string_view> seen;
-        while (const auto field{next()}) {
-            if (std::ranges::find(seen, *field) != seen.end()) {
-                fail(std::format("{} is given twice", quoted(*field)));
-            }
-            seen.push_back(*field);
-            if (!read(*field)) {
-                fail(std::format("unknown field {}", quoted(*field)));
-            }
-        }
-    }
-    template <typename T>
-    T required(const std::optional<T>& value, std::string_view what) const
-    {
-        if (!value) {
-            fail(std::format("missing '{}'", what));
-        }
-        return *value;
-    }
-    void expectEnd()
-    {
-        if (const auto extra{next()}) {
-            fail(std::format("unexpected {}", quoted(*extra)));
+        if (!done()) {
+            fail(std::format("unexpected {}", quoted(words[at])));
         }
     }
 
 private:
-    Words words;
-    std::size_t line_number;
+    std::vector<std::string_view> words;
+    std::size_t at{0};
+    std::size_t number;
 };
 
-struct LoadedMesh {
-    std::uint32_t id{};
-    std::vector<Vec3> points; // positions used by kept triangles, each once
+enum class Kind : std::uint8_t {
+    Number,   // any finite number
+    Positive, // a number above zero
+    Ranged,   // a number in [low, high]
+    Point,    // three numbers: the x, y and z coordinates of <noun>
+    Color,    // three numbers in [low, high]: the red, green and blue channels of <noun>
+    Material, // the name of a defined material
+    Basic,    // the name of a defined material that is not a mix
 };
 
-bool isInstanceKeyword(std::string_view word)
+struct Field {
+    std::string_view key;
+    Kind kind;
+    std::string_view noun;
+    double low{0};
+    double high{0};
+};
+
+using Value = std::variant<double, Vec3, Rgb, std::uint32_t>;
+
+constexpr double kAnyNumber{0};
+
+// Value ranges (scene/scene_file.cpp:68-77) as the field tables use them.
+constexpr Field reflectance(std::string_view key, std::string_view noun)
 {
-    constexpr std::array<std::string_view, 6> keywords{"material", "translate", "scale", "rotate", "fit", "ground"};
-    return std::ranges::find(keywords, word) != keywords.end();
+    return {key, Kind::Color, noun, 0, kMaxReflectance};
+}
+constexpr Field emission(std::string_view key, std::string_view noun)
+{
+    return {key, Kind::Color, noun, 0, kMaxEmission};
 }
 
-// A relative path without '..', control bytes or a root (scene/scene_file.cpp:368-395),
-// resolved inside `base` (scene/scene_file.cpp:400-430).
-std::filesystem::path meshFile(const Statement& statement, const std::filesystem::path& base, std::string_view text)
+constexpr std::array kCameraFields{
+    Field{"from", Kind::Point, "the camera position"},
+    Field{"at", Kind::Point, "the point the camera looks at"},
+    Field{"up", Kind::Point, "the camera's up direction"},
+    Field{"fov", Kind::Number, "the field of view"},
+};
+constexpr std::array kSkyFields{
+    emission("nadir", "the radiance from below"),
+    emission("zenith", "the radiance from above"),
+};
+constexpr std::array kDiffuseFields{reflectance("color", "the color")};
+constexpr std::array kCheckerFields{
+    reflectance("even", "the even color"),
+    reflectance("odd", "the odd color"),
+    Field{"frequency", Kind::Positive, "the checker frequency"},
+};
+constexpr std::array kPerlinFields{
+    reflectance("low", "the low color"),
+    reflectance("high", "the high color"),
+    Field{"scale", Kind::Positive, "the noise scale"},
+    Field{"veins", Kind::Ranged, "the veins", 0, kMaxPerlinVeins},
+};
+constexpr std::array kConductorFields{
+    Field{"eta", Kind::Color, "the refractive index", kMinConductorEta, kMaxConductorEta},
+    Field{"k", Kind::Color, "the absorption", 0, kMaxConductorK},
+    Field{"roughness", Kind::Ranged, "the roughness", 0, kMaxRoughness},
+};
+constexpr std::array kDielectricFields{
+    Field{"ior", Kind::Ranged, "the index of refraction", kMinIor, kMaxIor},
+    Field{"roughness", Kind::Ranged, "the roughness", 0, kMaxRoughness},
+};
+constexpr std::array kMixFields{
+    Field{"first", Kind::Basic, "a material name"},
+    Field{"second", Kind::Basic, "a material name"},
+    Field{"scale", Kind::Positive, "the noise scale"},
+    Field{"veins", Kind::Ranged, "the veins", 0, kMaxPerlinVeins},
+    Field{"threshold", Kind::Ranged, "the threshold", 0, 1},
+};
+constexpr std::array kSphereFields{
+    Field{"radius", Kind::Number, "a radius"},
+    Field{"material", Kind::Material, "a material name"},
+};
+constexpr std::array kPointLightFields{emission("intensity", "the intensity")};
+constexpr std::array kAreaLightFields{
+    Field{"radius", Kind::Number, "a radius"},
+    emission("radiance", "the radiance"),
+    Field{"material", Kind::Material, "a material name"},
+};
+
+double readNumber(LineWords& line, std::string_view noun)
 {
-    const bool control{std::ranges::any_of(text, [](char c) {
-        const auto byte{static_cast<unsigned char>(c)};
-        return byte < 0x20 || byte == 0x7F;
-    })};
-    if (control) {
-        statement.fail(std::format("mesh path {} must be UTF-8 without control characters", quoted(text)));
+    const std::string_view token{line.expect(noun)};
+    const auto value{parseReal(token)};
+    if (!value) {
+        line.fail(std::format("{} must be a finite number, got {}", noun, quoted(token)));
     }
-    const std::filesystem::path relative{std::string{text}};
-    if (relative.is_absolute() || relative.has_root_name() || relative.has_root_directory() ||
-        std::ranges::find(relative, std::filesystem::path{".."}) != relative.end()) {
-        statement.fail(std::format("mesh path {} must be relative to the scene and not use '..'", quoted(text)));
-    }
-    std::error_code error;
-    const std::filesystem::path real_base{std::filesystem::canonical(base, error)};
-    if (error) {
-        statement.fail("the scene's directory cannot be resolved");
-    }
-    const std::filesystem::path real_file{std::filesystem::weakly_canonical(real_base / relative, error)};
-    if (error) {
-        statement.fail(std::format("cannot resolve mesh path {}", quoted(text)));
-    }
-    const auto [base_end, file_part]{std::ranges::mismatch(real_base, real_file)};
-    if (base_end != real_base.end()) {
-        statement.fail(std::format("mesh path {} leads outside the scene's directory", quoted(text)));
-    }
-    const auto status{std::filesystem::status(real_file, error)};
-    if (status.type() == std::filesystem::file_type::not_found) {
-        statement.fail(std::format("mesh file {} does not exist", quoted(text)));
-    }
-    if (status.type() != std::filesystem::file_type::regular) {
-        statement.fail(std::format("mesh path {} is not a regular file", quoted(text)));
-    }
-    return real_file;
+    return *value;
 }
 
-class SceneReader {
+// One number of kind Number, Positive or Ranged, checked as soon as it is read.
+double readScalar(LineWords& line, Kind kind, std::string_view noun, double low, double high)
+{
+    const double value{readNumber(line, noun)};
+    if (kind == Kind::Positive && !(value > 0)) {
+        line.fail(std::format("{} must be positive, got {}", noun, value));
+    }
+    if (kind == Kind::Ranged && (value < low || value > high)) {
+        line.fail(std::format("{} must be between {} and {}, got {}", noun, low, high, value));
+    }
+    return value;
+}
+
+// A point (three numbers) or a colour (three numbers in [low, high]).
+std::array<double, 3> readTriple(LineWords& line, Kind kind, std::string_view noun, double low = kAnyNumber,
+                                 double high = kAnyNumber)
+{
+    static constexpr std::array<std::string_view, 3> kCoordinates{"x coordinate", "y coordinate", "z coordinate"};
+    static constexpr std::array<std::string_view, 3> kChannels{"red channel", "green channel", "blue channel"};
+    const bool color{kind == Kind::Color};
+    std::array<double, 3> out{};
+    for (std::size_t k{0}; k < 3; ++k) {
+        const std::string part{std::format("the {} of {}", color ? kChannels[k] : kCoordinates[k], noun)};
+        out[k] = readScalar(line, color ? Kind::Ranged : Kind::Number, part, low, high);
+    }
+    return out;
+}
+
+Vec3 readPoint(LineWords& line, std::string_view noun)
+{
+    const auto v{readTriple(line, Kind::Point, noun)};
+    return {v[0], v[1], v[2]};
+}
+
+Rgb readColor(LineWords& line, std::string_view noun, double low, double high)
+{
+    const auto v{readTriple(line, Kind::Color, noun, low, high)};
+    return {v[0], v[1], v[2]};
+}
+
+std::string_view readName(LineWords& line, std::string_view noun)
+{
+    const std::string_view token{line.expect(noun)};
+    if (!isIdentifier(token)) {
+        line.fail(std::format("{} is not a valid name", quoted(token)));
+    }
+    return token;
+}
+
+// Named values read from one statement, in the slots of its field table.
+class FieldValues {
 public:
-    explicit SceneReader(std::filesystem::path directory) : base_directory{std::move(directory)} {}
+    explicit FieldValues(std::span<const Field> fields) : table{fields}, values(fields.size()) {}
 
-    void readLine(std::string_view line, std::size_t line_number)
+    std::optional<std::size_t> slot(std::string_view key) const
     {
-        Statement statement{line.substr(0, line.find('#')), line_number};
-        const auto keyword{statement.next()};
-        if (!keyword) {
-            return;
+        for (std::size_t i{0}; i < table.size(); ++i) {
+            if (table[i].key == key) {
+                return i;
+            }
         }
-        if (*keyword == "camera") {
-            readCamera(statement);
-        } else if (*keyword == "sky") {
-            readSky(statement);
-        } else if (*keyword == "material") {
-            readMaterial(statement);
-        } else if (*keyword == "sphere") {
-            readSphere(statement);
-        } else if (*keyword == "point_light") {
-            readPointLight(statement);
-        } else if (*keyword == "area_light") {
-            readAreaLight(statement);
-        } else if (*keyword == "mesh") {
-            readMesh(statement);
-        } else if (*keyword == "instance") {
-            readInstance(statement);
-        } else {
-            statement.fail(std::format("unknown statement {}", quoted(*keyword)));
-        }
+        return std::nullopt;
     }
+    bool given(std::size_t i) const { return values[i].has_value(); }
+    void set(std::size_t i, Value value) { values[i] = value; }
 
-    HostScene finish() &&
+    template <typename T>
+    std::optional<T> get(std::string_view key) const
     {
-        if (!scene.has_camera) {
-            throw SceneParseError{0, "the scene has no camera"};
+        const auto& value{values[*slot(key)]};
+        return value ? std::optional<T>{std::get<T>(*value)} : std::nullopt;
+    }
+    // A required field: its absence is the statement's error.
+    template <typename T>
+    T need(const LineWords& line, std::string_view key) const
+    {
+        const auto value{get<T>(key)};
+        if (!value) {
+            line.fail(std::format("missing '{}'", key));
         }
-        scene.finalize();
-        return std::move(scene);
+        return *value;
     }
 
 private:
-    void readCamera(Statement& statement)
-    {
-        if (scene.has_camera) {
-            statement.fail("the scene already has a camera");
-        }
-        std::optional<Vec3> from;
-        std::optional<Vec3> at;
-        CameraSettings settings{};
-        statement.readFields([&](std::string_view field) {
-            if (field == "from") {
-                from = statement.point("the camera position");
-            } else if (field == "at") {
-                at = statement.point("the point the camera looks at");
-            } else if (field == "up") {
-                settings.up = statement.point("the camera's up direction");
-            } else if (field == "fov") {
-                settings.vertical_fov_degrees = statement.number("the field of view");
-            } else {
-                return false;
-            }
-            return true;
-        });
-        settings.look_from = statement.required(from, "from");
-        settings.look_at = statement.required(at, "at");
-        try {
-            static_cast<void>(buildCameraFrame(settings, 16.0 / 9.0));
-        } catch (const std::invalid_argument& error) {
-            statement.fail(error.what());
-        }
-        scene.camera = settings;
-        scene.has_camera = true;
-    }
+    std::span<const Field> table;
+    std::vector<std::optional<Value>> values;
+};
 
-    void readSky(Statement& statement)
-    {
-        if (sky_given) {
-            statement.fail("the scene already has a sky");
-        }
-        const auto first{statement.peek()};
-        if (first && (*first == "nadir" || *first == "zenith")) {
-            std::optional<Rgb> nadir;
-            std::optional<Rgb> zenith;
-            statement.readFields([&](std::string_view field) {
-                if (field == "nadir") {
-                    nadir = statement.emission("the radiance from below");
-                } else if (field == "zenith") {
-                    zenith = statement.emission("the radiance from above");
-                } else {
-                    return false;
-                }
-                return true;
-            });
-            scene.setSky(statement.required(nadir, "nadir"), statement.required(zenith, "zenith"));
-        } else {
-            const Rgb radiance{statement.emission("the sky's radiance")};
-            statement.expectEnd();
-            scene.setSky(radiance, radiance);
-        }
-        sky_given = true;
-    }
+struct MeshEntry {
+    std::uint32_t id{};
+    std::vector<Vec3> points; // positions that kept triangles use, each once
+};
 
-    void readMaterial(Statement& statement)
-    {
-        if (material_ids.size() >= kMaxMaterials) {
-            statement.fail(std::format("more than {} materials", kMaxMaterials));
-        }
-        const std::string_view name{statement.name("a material name")};
-        if (material_ids.contains(name)) {
-            statement.fail(std::format("material {} is already defined", quoted(name)));
-        }
-        const std::string_view type{statement.word("a material type")};
-        MaterialDesc material;
-        if (type == "mix") {
-            material = readMix(statement);
-        } else {
-            material.first = basicOfType(statement, type);
-        }
-        material_ids.emplace(std::string{name}, scene.addMaterial(material));
-    }
+// Everything a scene file has defined so far.
+struct SceneState {
+    std::filesystem::path directory;
+    HostScene scene;
+    bool sky_given{false};
+    std::map<std::string, std::uint32_t, std::less<>> material_ids;
+    std::map<std::string, MeshEntry, std::less<>> meshes;
+    ObjBudget budget{};
+    std::size_t ground_points_left{kMaxGroundPoints};
+    std::size_t objects{0};
 
-    static BasicMaterialDesc basicOfType(Statement& statement, std::string_view type)
+    std::uint32_t materialNamed(LineWords& line) const
     {
-        BasicMaterialDesc basic;
-        if (type == "diffuse") {
-            std::optional<Rgb> color;
-            statement.readFields([&](std::string_view field) {
-                if (field != "color") {
-                    return false;
-                }
-                color = statement.reflectance("the color");
-                return true;
-            });
-            basic.texture = {TextureKind::Constant, statement.required(color, "color")};
-        } else if (type == "checker") {
-            std::optional<Rgb> even;
-            std::optional<Rgb> odd;
-            std::optional<double> frequency;
-            statement.readFields([&](std::string_view field) {
-                if (field == "even") {
-                    even = statement.reflectance("the even color");
-                } else if (field == "odd") {
-                    odd = statement.reflectance("the odd color");
-                } else if (field == "frequency") {
-                    frequency = statement.positive("the checker frequency");
-                } else {
-                    return false;
-                }
-                return true;
-            });
-            basic.texture = {TextureKind::Checker, statement.required(even, "even"), statement.required(odd, "odd"),
-                             statement.required(frequency, "frequency")};
-        } else if (type == "perlin") {
-            std::optional<Rgb> low;
-            std::optional<Rgb> high;
-            std::optional<double> scale;
-            double veins{0};
-            statement.readFields([&](std::string_view field) {
-                if (field == "low") {
-                    low = statement.reflectance("the low color");
-                } else if (field == "high") {
-                    high = statement.reflectance("the high color");
-                } else if (field == "scale") {
-                    scale = statement.positive("the noise scale");
-                } else if (field == "veins") {
-                    veins = statement.inRange("the veins", 0, kMaxPerlinVeins);
-                } else {
-                    return false;
-                }
-                return true;
-            });
-            basic.texture = {TextureKind::Perlin, statement.required(low, "low"), statement.required(high, "high"),
-                             statement.required(scale, "scale"), veins};
-        } else if (type == "conductor") {
-            std::optional<Rgb> eta;
-            std::optional<Rgb> k;
-            double roughness{0};
-            statement.readFields([&](std::string_view field) {
-                if (field == "eta") {
-                    eta = statement.color("the refractive index", kMinConductorEta, kMaxConductorEta);
-                } else if (field == "k") {
-                    k = statement.color("the absorption", 0, kMaxConductorK);
-                } else if (field == "roughness") {
-                    roughness = statement.inRange("the roughness", 0, kMaxRoughness);
-                } else {
-                    return false;
-                }
-                return true;
-            });
-            basic.kind = BasicKind::Conductor;
-            basic.eta = statement.required(eta, "eta");
-            basic.k = statement.required(k, "k");
-            basic.roughness = roughness;
-            const std::array<double, 3> e{basic.eta.r, basic.eta.g, basic.eta.b};
-            const std::array<double, 3> a{basic.k.r, basic.k.g, basic.k.b};
-            for (std::size_t c{0}; c < 3; ++c) {
-                if (e[c] == 1 && a[c] == 0) {
-                    statement.fail("a conductor channel cannot have eta 1 and k 0");
-                }
-            }
-        } else if (type == "dielectric") {
-            std::optional<double> ior;
-            double roughness{0};
-            statement.readFields([&](std::string_view field) {
-                if (field == "ior") {
-                    ior = statement.inRange("the index of refraction", kMinIor, kMaxIor);
-                } else if (field == "roughness") {
-                    roughness = statement.inRange("the roughness", 0, kMaxRoughness);
-                } else {
-                    return false;
-                }
-                return true;
-            });
-            basic.kind = BasicKind::Dielectric;
-            basic.ior = statement.required(ior, "ior");
-            basic.roughness = roughness;
-        } else {
-            statement.fail(std::format("unknown material type {}", quoted(type)));
-        }
-        return basic;
-    }
-
-    MaterialDesc readMix(Statement& statement) const
-    {
-        std::optional<BasicMaterialDesc> first;
-        std::optional<BasicMaterialDesc> second;
-        std::optional<double> scale;
-        double veins{0};
-        double threshold{0.5};
-        statement.readFields([&](std::string_view field) {
-            if (field == "first") {
-                first = basicNamed(statement);
-            } else if (field == "second") {
-                second = basicNamed(statement);
-            } else if (field == "scale") {
-                scale = statement.positive("the noise scale");
-            } else if (field == "veins") {
-                veins = statement.inRange("the veins", 0, kMaxPerlinVeins);
-            } else if (field == "threshold") {
-                threshold = statement.inRange("the threshold", 0, 1);
-            } else {
-                return false;
-            }
-            return true;
-        });
-        MaterialDesc mix;
-        mix.mix = true;
-        mix.first = statement.required(first, "first");
-        mix.second = statement.required(second, "second");
-        mix.scale = statement.required(scale, "scale");
-        mix.veins = veins;
-        mix.threshold = threshold;
-        return mix;
-    }
-
-    BasicMaterialDesc basicNamed(Statement& statement) const
-    {
-        const std::string_view name{statement.peek().value_or("")};
-        const MaterialDesc& material{scene.materials[materialNamed(statement)]};
-        if (material.mix) {
-            statement.fail(std::format("material {} is a mix, and a mix cannot hold another mix", quoted(name)));
-        }
-        return material.first;
-    }
-
-    std::uint32_t materialNamed(Statement& statement) const
-    {
-        const std::string_view name{statement.name("a material name")};
+        const std::string_view name{readName(line, "a material name")};
         const auto found{material_ids.find(name)};
         if (found == material_ids.end()) {
-            statement.fail(std::format("material {} is not defined", quoted(name)));
+            line.fail(std::format("material {} is not defined", quoted(name)));
         }
         return found->second;
     }
 
-    void countObject(const Statement& statement)
+    void countObject(const LineWords& line)
     {
-        if (object_count >= kMaxObjects) {
-            statement.fail(std::format("more than {} objects", kMaxObjects));
+        if (objects >= kMaxObjects) {
+            line.fail(std::format("more than {} objects", kMaxObjects));
         }
-        ++object_count;
+        ++objects;
     }
-
-    void readSphere(Statement& statement)
-    {
-        countObject(statement);
-        const Vec3 center{statement.point("the sphere center")};
-        std::optional<double> radius;
-        std::optional<std::uint32_t> material;
-        statement.readFields([&](std::string_view field) {
-            if (field == "radius") {
-                radius = statement.number("a radius");
-            } else if (field == "material") {
-                material = materialNamed(statement);
-            } else {
-                return false;
-            }
-            return true;
-        });
-        const double r{statement.required(radius, "radius")};
-        try {
-            validateSphere(center, r);
-        } catch (const std::invalid_argument& error) {
-            statement.fail(error.what());
-        }
-        if (!material) {
-            statement.fail("missing 'material'");
-        }
-        scene.addSphere(center, r, *material);
-    }
-
-    void readPointLight(Statement& statement)
-    {
-        countObject(statement);
-        const Vec3 position{statement.point("the light position")};
-        std::optional<Rgb> intensity;
-        statement.readFields([&](std::string_view field) {
-            if (field != "intensity") {
-                return false;
-            }
-            intensity = statement.emission("the intensity");
-            return true;
-        });
-        scene.addPointLight(position, statement.required(intensity, "intensity"));
-    }
-
-    void readAreaLight(Statement& statement)
-    {
-        countObject(statement);
-        const Vec3 center{statement.point("the light center")};
-        std::optional<double> radius;
-        std::optional<Rgb> radiance;
-        std::optional<std::uint32_t> material;
-        statement.readFields([&](std::string_view field) {
-            if (field == "radius") {
-                radius = statement.number("a radius");
-            } else if (field == "radiance") {
-                radiance = statement.emission("the radiance");
-            } else if (field == "material") {
-                material = materialNamed(statement);
-            } else {
-                return false;
-            }
-            return true;
-        });
-        const double r{statement.required(radius, "radius")};
-        try {
-            validateSphere(center, r);
-        } catch (const std::invalid_argument& error) {
-            statement.fail(error.what());
-        }
-        const Rgb emitted{statement.required(radiance, "radiance")};
-        if (!material) {
-            // An area light without a material is black diffuse (scene/scene_file.cpp:819).
-            material = scene.addMaterial(MaterialDesc{});
-        }
-        scene.addAreaLight(center, r, emitted, *material);
-    }
-
-    void readMesh(Statement& statement)
-    {
-        if (base_directory.empty()) {
-            statement.fail("meshes can only be read from a scene file, which they sit beside");
-        }
-        if (meshes.size() >= kMaxMeshes) {
-            statement.fail(std::format("more than {} meshes", kMaxMeshes));
-        }
-        const std::string_view name{statement.name("a mesh name")};
-        if (meshes.contains(name)) {
-            statement.fail(std::format("mesh {} is already defined", quoted(name)));
-        }
-        const std::string_view path{statement.word("a mesh file")};
-        const bool smooth{statement.peek() == "smooth"};
-        if (smooth) {
-            static_cast<void>(statement.next());
-        }
-        statement.expectEnd();
-        const std::filesystem::path file{meshFile(statement, base_directory, path)};
-        ObjMesh obj;
-        try {
-            obj = readObj(file, budget);
-        } catch (const ObjError& error) {
-            statement.fail(std::format("mesh {}: {}", quoted(path), error.what()));
-        } catch (const std::runtime_error&) {
-            statement.fail(std::format("cannot read mesh file {}", quoted(path)));
-        }
-        LoadedMesh loaded;
-        std::vector<bool> used(obj.positions.size(), false);
-        for (const auto& f : obj.faces) {
-            if (formsTriangle(obj.positions[f[0]], obj.positions[f[1]], obj.positions[f[2]])) {
-                used[f[0]] = used[f[1]] = used[f[2]] = true;
-            }
-        }
-        for (std::size_t i{0}; i < obj.positions.size(); ++i) {
-            if (used[i]) {
-                loaded.points.push_back(obj.positions[i]);
-            }
-        }
-        if (loaded.points.empty()) {
-            statement.fail(std::format("mesh {} has no triangles", quoted(path)));
-        }
-        try {
-            loaded.id = scene.addMesh(obj.positions, obj.faces, obj.uvs, obj.texture_faces, smooth);
-        } catch (const std::exception& error) {
-            statement.fail(std::format("mesh {}: {}", quoted(path), error.what()));
-        }
-        budget.vertices -= obj.positions.size();
-        budget.texture_coordinates -= obj.uvs.size();
-        budget.triangles -= obj.faces.size();
-        meshes.emplace(std::string{name}, std::move(loaded));
-    }
-
-    void readInstance(Statement& statement)
-    {
-        countObject(statement);
-        const std::string_view mesh_name{statement.name("a mesh name")};
-        const auto found{meshes.find(mesh_name)};
-        if (found == meshes.end()) {
-            statement.fail(std::format("mesh {} is not defined", quoted(mesh_name)));
-        }
-        const LoadedMesh& mesh{found->second};
-        std::optional<std::uint32_t> material;
-        Transform placement{};
-        std::size_t operations{0};
-        while (const auto word{statement.next()}) {
-            if (*word == "material") {
-                if (material) {
-                    statement.fail("'material' is given twice");
-                }
-                material = materialNamed(statement);
-                continue;
-            }
-            if (++operations > kMaxInstanceOperations) {
-                statement.fail(std::format("more than {} operations", kMaxInstanceOperations));
-            }
-            placement = applied(statement, *word, mesh, placement);
-        }
-        if (!material) {
-            statement.fail("missing 'material'");
-        }
-        try {
-            scene.addInstance(mesh.id, placement, *material);
-        } catch (const std::invalid_argument& error) {
-            statement.fail(error.what());
-        }
-    }
-
-    // scene/scene_file.cpp:962-1038.
-    Transform applied(Statement& statement, std::string_view name, const LoadedMesh& mesh, const Transform& placement)
-    {
-        try {
-            if (name == "translate") {
-                return Transform::translation(statement.point("the translation")) * placement;
-            }
-            if (name == "scale") {
-                const double first{statement.number("a scale factor")};
-                const auto next{statement.peek()};
-                if (!next || isInstanceKeyword(*next)) {
-                    return Transform::scaling({first, first, first}) * placement;
-                }
-                const double y{statement.number("the y scale factor")};
-                return Transform::scaling({first, y, statement.number("the z scale factor")}) * placement;
-            }
-            if (name == "rotate") {
-                const Vec3 axis{statement.point("the rotation axis")};
-                return Transform::rotation(axis, statement.number("the rotation angle")) * placement;
-            }
-            if (name == "fit") {
-                const double size{statement.positive("the fitted size")};
-                const Box3 box{placement.applyBox(scene.meshes[mesh.id].bounds)};
-                if (!isFinite(box.min) || !isFinite(box.max)) {
-                    statement.fail("the instance is out of range before 'fit'");
-                }
-                const Vec3 extent{box.extent()};
-                const double scale{size / std::max({extent.x, extent.y, extent.z})};
-                if (!std::isfinite(scale) || !(scale > 0)) {
-                    statement.fail("the instance is too large or too small to fit");
-                }
-                const Vec3 center{box.min.x / 2 + box.max.x / 2, box.min.y / 2 + box.max.y / 2,
-                                  box.min.z / 2 + box.max.z / 2};
-                return Transform::scaling({scale, scale, scale}) * Transform::translation(-center) * placement;
-            }
-            if (name == "ground") {
-                if (mesh.points.size() > ground_points_left) {
-                    statement.fail(
-                        std::format("'ground' would examine more than {} points in the scene", kMaxGroundPoints));
-                }
-                ground_points_left -= mesh.points.size();
-                std::optional<double> lowest;
-                for (const Vec3& p : mesh.points) {
-                    const double height{placement.applyPoint(p).y};
-                    if (!std::isfinite(height)) {
-                        lowest.reset();
-                        break;
-                    }
-                    lowest = lowest ? std::min(*lowest, height) : height;
-                }
-                if (!lowest) {
-                    statement.fail("the instance is out of range before 'ground'");
-                }
-                return Transform::translation({0, -*lowest, 0}) * placement;
-            }
-        } catch (const std::invalid_argument& error) {
-            statement.fail(error.what());
-        }
-        statement.fail(std::format("unknown instance operation {}", quoted(name)));
-    }
-
-    std::filesystem::path base_directory;
-    HostScene scene;
-    bool sky_given{false};
-    std::map<std::string, std::uint32_t, std::less<>> material_ids;
-    std::map<std::string, LoadedMesh, std::less<>> meshes;
-    ObjBudget budget{};
-    std::size_t ground_points_left{kMaxGroundPoints};
-    std::size_t object_count{0};
 };
+
+Value readValue(LineWords& line, const Field& field, const SceneState& state)
+{
+    switch (field.kind) {
+    case Kind::Point:
+        return readPoint(line, field.noun);
+    case Kind::Color:
+        return readColor(line, field.noun, field.low, field.high);
+    case Kind::Material:
+        return state.materialNamed(line);
+    case Kind::Basic: {
+        const std::string_view name{line.peek().value_or("")};
+        const std::uint32_t id{state.materialNamed(line)};
+        if (state.scene.materials[id].mix) {
+            line.fail(std::format("material {} is a mix, and a mix cannot hold another mix", quoted(name)));
+        }
+        return id;
+    }
+    default:
+        return readScalar(line, field.kind, field.noun, field.low, field.high);
+    }
+}
+
+// The generic field loop: the rest of the line is key / value pairs from `table`.
+FieldValues readFields(LineWords& line, std::span<const Field> table, const SceneState& state)
+{
+    FieldValues values{table};
+    while (const auto key{line.take()}) {
+        const auto slot{values.slot(*key)};
+        if (slot && values.given(*slot)) {
+            line.fail(std::format("{} is given twice", quoted(*key)));
+        }
+        if (!slot) {
+            line.fail(std::format("unknown field {}", quoted(*key)));
+        }
+        values.set(*slot, readValue(line, table[*slot], state));
+    }
+    return values;
+}
+
+// ------------------------------------------------ materials
+
+struct MaterialType {
+    std::string_view name;
+    std::span<const Field> fields;
+    MaterialDesc (*build)(const FieldValues&, const LineWords&, const SceneState&);
+};
+
+MaterialDesc diffuseMaterial(const FieldValues& f, const LineWords& line, const SceneState&)
+{
+    MaterialDesc m;
+    m.first.texture = {TextureKind::Constant, f.need<Rgb>(line, "color")};
+    return m;
+}
+
+MaterialDesc checkerMaterial(const FieldValues& f, const LineWords& line, const SceneState&)
+{
+    MaterialDesc m;
+    const Rgb even{f.need<Rgb>(line, "even")};
+    const Rgb odd{f.need<Rgb>(line, "odd")};
+    m.first.texture = {TextureKind::Checker, even, odd, f.need<double>(line, "frequency")};
+    return m;
+}
+
+MaterialDesc perlinMaterial(const FieldValues& f, const LineWords& line, const SceneState&)
+{
+    MaterialDesc m;
+    const Rgb low{f.need<Rgb>(line, "low")};
+    const Rgb high{f.need<Rgb>(line, "high")};
+    const double scale{f.need<double>(line, "scale")};
+    m.first.texture = {TextureKind::Perlin, low, high, scale, f.get<double>("veins").value_or(0)};
+    return m;
+}
+
+MaterialDesc conductorMaterial(const FieldValues& f, const LineWords& line, const SceneState&)
+{
+    MaterialDesc m;
+    m.first.kind = BasicKind::Conductor;
+    m.first.eta = f.need<Rgb>(line, "eta");
+    m.first.k = f.need<Rgb>(line, "k");
+    m.first.roughness = f.get<double>("roughness").value_or(0);
+    const std::array<double, 3> eta{m.first.eta.r, m.first.eta.g, m.first.eta.b};
+    const std::array<double, 3> k{m.first.k.r, m.first.k.g, m.first.k.b};
+    for (std::size_t c{0}; c < 3; ++c) {
+        // Such a channel reflects nothing: the Fresnel term is 0/0.
+        if (eta[c] == 1 && k[c] == 0) {
+            line.fail("a conductor channel cannot have eta 1 and k 0");
+        }
+    }
+    return m;
+}
+
+MaterialDesc dielectricMaterial(const FieldValues& f, const LineWords& line, const SceneState&)
+{
+    MaterialDesc m;
+    m.first.kind = BasicKind::Dielectric;
+    m.first.ior = f.need<double>(line, "ior");
+    m.first.roughness = f.get<double>("roughness").value_or(0);
+    return m;
+}
+
+MaterialDesc mixMaterial(const FieldValues& f, const LineWords& line, const SceneState& state)
+{
+    MaterialDesc m;
+    m.mix = true;
+    m.first = state.scene.materials[f.need<std::uint32_t>(line, "first")].first;
+    m.second = state.scene.materials[f.need<std::uint32_t>(line, "second")].first;
+    m.scale = f.need<double>(line, "scale");
+    m.veins = f.get<double>("veins").value_or(0);
+    m.threshold = f.get<double>("threshold").value_or(0.5);
+    return m;
+}
+
+constexpr std::array kMaterialTypes{
+    MaterialType{"diffuse", kDiffuseFields, &diffuseMaterial},
+    MaterialType{"checker", kCheckerFields, &checkerMaterial},
+    MaterialType{"perlin", kPerlinFields, &perlinMaterial},
+    MaterialType{"conductor", kConductorFields, &conductorMaterial},
+    MaterialType{"dielectric", kDielectricFields, &dielectricMaterial},
+    MaterialType{"mix", kMixFields, &mixMaterial},
+};
+
+// ------------------------------------------------ statements
+
+void cameraStatement(SceneState& state, LineWords& line)
+{
+    if (state.scene.has_camera) {
+        line.fail("the scene already has a camera");
+    }
+    const FieldValues f{readFields(line, kCameraFields, state)};
+    CameraSettings settings{};
+    settings.look_from = f.need<Vec3>(line, "from");
+    settings.look_at = f.need<Vec3>(line, "at");
+    settings.up = f.get<Vec3>("up").value_or(settings.up);
+    settings.vertical_fov_degrees = f.get<double>("fov").value_or(settings.vertical_fov_degrees);
+    try {
+        static_cast<void>(buildCameraFrame(settings, 16.0 / 9.0));
+    } catch (const std::invalid_argument& error) {
+        line.fail(error.what());
+    }
+    state.scene.camera = settings;
+    state.scene.has_camera = true;
+}
+
+void skyStatement(SceneState& state, LineWords& line)
+{
+    if (state.sky_given) {
+        line.fail("the scene already has a sky");
+    }
+    const auto first{line.peek()};
+    if (first && (*first == "nadir" || *first == "zenith")) {
+        const FieldValues f{readFields(line, kSkyFields, state)};
+        const Rgb nadir{f.need<Rgb>(line, "nadir")};
+        state.scene.setSky(nadir, f.need<Rgb>(line, "zenith"));
+    } else {
+        // One radiance for the whole sky.
+        const Rgb radiance{readColor(line, "the sky's radiance", 0, kMaxEmission)};
+        line.end();
+        state.scene.setSky(radiance, radiance);
+    }
+    state.sky_given = true;
+}
+
+void materialStatement(SceneState& state, LineWords& line)
+{
+    if (state.material_ids.size() >= kMaxMaterials) {
+        line.fail(std::format("more than {} materials", kMaxMaterials));
+    }
+    const std::string_view name{readName(line, "a material name")};
+    if (state.material_ids.contains(name)) {
+        line.fail(std::format("material {} is already defined", quoted(name)));
+    }
+    const std::string_view type{line.expect("a material type")};
+    const auto found{std::ranges::find(kMaterialTypes, type, &MaterialType::name)};
+    if (found == kMaterialTypes.end()) {
+        line.fail(std::format("unknown material type {}", quoted(type)));
+    }
+    const FieldValues f{readFields(line, found->fields, state)};
+    const MaterialDesc material{found->build(f, line, state)};
+    state.material_ids.emplace(std::string{name}, state.scene.addMaterial(material));
+}
+
+void checkSphere(const LineWords& line, Vec3 center, double radius)
+{
+    try {
+        validateSphere(center, radius);
+    } catch (const std::invalid_argument& error) {
+        line.fail(error.what());
+    }
+}
+
+void sphereStatement(SceneState& state, LineWords& line)
+{
+    state.countObject(line);
+    const Vec3 center{readPoint(line, "the sphere center")};
+    const FieldValues f{readFields(line, kSphereFields, state)};
+    const double radius{f.need<double>(line, "radius")};
+    checkSphere(line, center, radius);
+    state.scene.addSphere(center, radius, f.need<std::uint32_t>(line, "material"));
+}
+
+void pointLightStatement(SceneState& state, LineWords& line)
+{
+    state.countObject(line);
+    const Vec3 position{readPoint(line, "the light position")};
+    const FieldValues f{readFields(line, kPointLightFields, state)};
+    state.scene.addPointLight(position, f.need<Rgb>(line, "intensity"));
+}
+
+void areaLightStatement(SceneState& state, LineWords& line)
+{
+    state.countObject(line);
+    const Vec3 center{readPoint(line, "the light center")};
+    const FieldValues f{readFields(line, kAreaLightFields, state)};
+    const double radius{f.need<double>(line, "radius")};
+    checkSphere(line, center, radius);
+    const Rgb radiance{f.need<Rgb>(line, "radiance")};
+    // Without a material the light's sphere is black diffuse (scene/scene_file.cpp:819).
+    std::optional<std::uint32_t> material{f.get<std::uint32_t>("material")};
+    if (!material) {
+        material = state.scene.addMaterial(MaterialDesc{});
+    }
+    state.scene.addAreaLight(center, radius, radiance, *material);
+}
+
+// Where a mesh statement's file lies. The path must be relative, without '..',
+// control bytes or a root, and lead to a regular file inside the scene's
+// directory (scene/scene_file.cpp:368-430 states the same rules).
+std::filesystem::path meshFile(const LineWords& line, const std::filesystem::path& directory, std::string_view text)
+{
+    for (const char c : text) {
+        const auto byte{static_cast<unsigned char>(c)};
+        if (byte < 0x20 || byte == 0x7F) {
+            line.fail(std::format("mesh path {} must be UTF-8 without control characters", quoted(text)));
+        }
+    }
+    const std::filesystem::path relative{std::string{text}};
+    const bool climbs{std::ranges::find(relative, std::filesystem::path{".."}) != relative.end()};
+    if (relative.is_absolute() || relative.has_root_name() || relative.has_root_directory() || climbs) {
+        line.fail(std::format("mesh path {} must be relative to the scene and not use '..'", quoted(text)));
+    }
+    std::error_code error;
+    const std::filesystem::path base{std::filesystem::canonical(directory, error)};
+    if (error) {
+        line.fail("the scene's directory cannot be resolved");
+    }
+    const std::filesystem::path file{std::filesystem::weakly_canonical(base / relative, error)};
+    if (error) {
+        line.fail(std::format("cannot resolve mesh path {}", quoted(text)));
+    }
+    if (std::ranges::mismatch(base, file).in1 != base.end()) {
+        line.fail(std::format("mesh path {} leads outside the scene's directory", quoted(text)));
+    }
+    switch (std::filesystem::status(file, error).type()) {
+    case std::filesystem::file_type::regular:
+        return file;
+    case std::filesystem::file_type::not_found:
+        line.fail(std::format("mesh file {} does not exist", quoted(text)));
+    default:
+        line.fail(std::format("mesh path {} is not a regular file", quoted(text)));
+    }
+}
+
+// The positions that the mesh's kept triangles use, each once, in order: the
+// points 'ground' examines.
+std::vector<Vec3> usedPositions(const ObjMesh& obj)
+{
+    std::vector<bool> used(obj.positions.size(), false);
+    for (const auto& f : obj.faces) {
+        if (formsTriangle(obj.positions[f[0]], obj.positions[f[1]], obj.positions[f[2]])) {
+            used[f[0]] = used[f[1]] = used[f[2]] = true;
+        }
+    }
+    std::vector<Vec3> points;
+    for (std::size_t i{0}; i < obj.positions.size(); ++i) {
+        if (used[i]) {
+            points.push_back(obj.positions[i]);
+        }
+    }
+    return points;
+}
+
+void meshStatement(SceneState& state, LineWords& line)
+{
+    if (state.directory.empty()) {
+        line.fail("meshes can only be read from a scene file, which they sit beside");
+    }
+    if (state.meshes.size() >= kMaxMeshes) {
+        line.fail(std::format("more than {} meshes", kMaxMeshes));
+    }
+    const std::string_view name{readName(line, "a mesh name")};
+    if (state.meshes.contains(name)) {
+        line.fail(std::format("mesh {} is already defined", quoted(name)));
+    }
+    const std::string_view path{line.expect("a mesh file")};
+    const bool smooth{line.peek() == "smooth"};
+    if (smooth) {
+        static_cast<void>(line.take());
+    }
+    line.end();
+    const std::filesystem::path file{meshFile(line, state.directory, path)};
+    ObjMesh obj;
+    try {
+        obj = readObj(file, state.budget);
+    } catch (const ObjError& error) {
+        line.fail(std::format("mesh {}: {}", quoted(path), error.what()));
+    } catch (const std::runtime_error&) {
+        line.fail(std::format("cannot read mesh file {}", quoted(path)));
+    }
+    MeshEntry entry{.id = 0, .points = usedPositions(obj)};
+    if (entry.points.empty()) {
+        line.fail(std::format("mesh {} has no triangles", quoted(path)));
+    }
+    try {
+        entry.id = state.scene.addMesh(obj.positions, obj.faces, obj.uvs, obj.texture_faces, smooth);
+    } catch (const std::exception& error) {
+        line.fail(std::format("mesh {}: {}", quoted(path), error.what()));
+    }
+    state.budget.vertices -= obj.positions.size();
+    state.budget.texture_coordinates -= obj.uvs.size();
+    state.budget.triangles -= obj.faces.size();
+    state.meshes.emplace(std::string{name}, std::move(entry));
+}
+
+// ------------------------------------------------ instance placement
+//
+// An instance's words after the mesh name are 'material <name>' once and up to
+// kMaxInstanceOperations placement operations, each applied after the ones
+// before it (scene/scene_file.cpp:962-1038 defines them).
+
+using Operation = Transform (*)(SceneState&, LineWords&, const MeshEntry&, const Transform&);
+
+Transform translateOperation(SceneState&, LineWords& line, const MeshEntry&, const Transform& placement)
+{
+    return Transform::translation(readPoint(line, "the translation")) * placement;
+}
+
+bool startsInstanceWord(std::string_view word);
+
+// 'scale s' or 'scale sx sy sz': one factor when the next word is missing or
+// starts the next operation.
+Transform scaleOperation(SceneState&, LineWords& line, const MeshEntry&, const Transform& placement)
+{
+    const double sx{readNumber(line, "a scale factor")};
+    const auto next{line.peek()};
+    if (!next || startsInstanceWord(*next)) {
+        return Transform::scaling({sx, sx, sx}) * placement;
+    }
+    const double sy{readNumber(line, "the y scale factor")};
+    const double sz{readNumber(line, "the z scale factor")};
+    return Transform::scaling({sx, sy, sz}) * placement;
+}
+
+Transform rotateOperation(SceneState&, LineWords& line, const MeshEntry&, const Transform& placement)
+{
+    const Vec3 axis{readPoint(line, "the rotation axis")};
+    return Transform::rotation(axis, readNumber(line, "the rotation angle")) * placement;
+}
+
+// 'fit size': scales the placed mesh's box about its centre so that its
+// largest extent is `size`, and moves that centre to the origin.
+Transform fitOperation(SceneState& state, LineWords& line, const MeshEntry& mesh, const Transform& placement)
+{
+    const double size{readScalar(line, Kind::Positive, "the fitted size", 0, 0)};
+    const Box3 box{placement.applyBox(state.scene.meshes[mesh.id].bounds)};
+    if (!isFinite(box.min) || !isFinite(box.max)) {
+        line.fail("the instance is out of range before 'fit'");
+    }
+    const Vec3 extent{box.extent()};
+    const double factor{size / std::max({extent.x, extent.y, extent.z})};
+    if (!std::isfinite(factor) || !(factor > 0)) {
+        line.fail("the instance is too large or too small to fit");
+    }
+    const Vec3 middle{box.min.x / 2 + box.max.x / 2, box.min.y / 2 + box.max.y / 2, box.min.z / 2 + box.max.z / 2};
+    return Transform::scaling({factor, factor, factor}) * Transform::translation(-middle) * placement;
+}
+
+// 'ground': lifts or lowers the placed mesh so that its lowest used vertex
+// sits at y = 0; all 'ground' operations of a file examine at most
+// kMaxGroundPoints vertices between them.
+Transform groundOperation(SceneState& state, LineWords& line, const MeshEntry& mesh, const Transform& placement)
+{
+    if (mesh.points.size() > state.ground_points_left) {
+        line.fail(std::format("'ground' would examine more than {} points in the scene", kMaxGroundPoints));
+    }
+    state.ground_points_left -= mesh.points.size();
+    double lowest{std::numeric_limits<double>::infinity()};
+    for (const Vec3& p : mesh.points) {
+        const double height{placement.applyPoint(p).y};
+        if (!std::isfinite(height)) {
+            line.fail("the instance is out of range before 'ground'");
+        }
+        lowest = std::min(lowest, height);
+    }
+    return Transform::translation({0, -lowest, 0}) * placement;
+}
+
+constexpr std::array<std::pair<std::string_view, Operation>, 5> kOperations{{
+    {"translate", &translateOperation},
+    {"scale", &scaleOperation},
+    {"rotate", &rotateOperation},
+    {"fit", &fitOperation},
+    {"ground", &groundOperation},
+}};
+
+bool startsInstanceWord(std::string_view word)
+{
+    return word == "material" ||
+           std::ranges::find(kOperations, word, &std::pair<std::string_view, Operation>::first) != kOperations.end();
+}
+
+void instanceStatement(SceneState& state, LineWords& line)
+{
+    state.countObject(line);
+    const std::string_view mesh_name{readName(line, "a mesh name")};
+    const auto mesh{state.meshes.find(mesh_name)};
+    if (mesh == state.meshes.end()) {
+        line.fail(std::format("mesh {} is not defined", quoted(mesh_name)));
+    }
+    std::optional<std::uint32_t> material;
+    Transform placement{};
+    std::size_t operations{0};
+    while (const auto word{line.take()}) {
+        if (*word == "material") {
+            if (material) {
+                line.fail("'material' is given twice");
+            }
+            material = state.materialNamed(line);
+            continue;
+        }
+        if (++operations > kMaxInstanceOperations) {
+            line.fail(std::format("more than {} operations", kMaxInstanceOperations));
+        }
+        const auto found{std::ranges::find(kOperations, *word, &std::pair<std::string_view, Operation>::first)};
+        if (found == kOperations.end()) {
+            line.fail(std::format("unknown instance operation {}", quoted(*word)));
+        }
+        try {
+            placement = found->second(state, line, mesh->second, placement);
+        } catch (const std::invalid_argument& error) {
+            line.fail(error.what());
+        }
+    }
+    if (!material) {
+        line.fail("missing 'material'");
+    }
+    try {
+        state.scene.addInstance(mesh->second.id, placement, *material);
+    } catch (const std::invalid_argument& error) {
+        line.fail(error.what());
+    }
+}
+
+// ------------------------------------------------ the file
+
+using StatementReader = void (*)(SceneState&, LineWords&);
+
+constexpr std::array<std::pair<std::string_view, StatementReader>, 8> kStatements{{
+    {"camera", &cameraStatement},
+    {"sky", &skyStatement},
+    {"material", &materialStatement},
+    {"sphere", &sphereStatement},
+    {"point_light", &pointLightStatement},
+    {"area_light", &areaLightStatement},
+    {"mesh", &meshStatement},
+    {"instance", &instanceStatement},
+}};
 
 HostScene readSceneStream(std::istream& input, const std::filesystem::path& base_directory)
 {
-    SceneReader reader{base_directory};
+    SceneState state;
+    state.directory = base_directory;
     forEachLine(
-        input, kMaxSceneLine, [&](std::string_view line, std::size_t number) { reader.readLine(line, number); },
-        [](std::size_t number) { throw SceneParseError{number, std::format("line longer than {} bytes", kMaxSceneLine)}; });
-    return std::move(reader).finish();
+        input, kMaxSceneLine,
+        [&](std::string_view text, std::size_t number) {
+            LineWords line{text.substr(0, text.find('#')), number};
+            const auto keyword{line.take()};
+            if (!keyword) {
+                return;
+            }
+            const auto found{
+                std::ranges::find(kStatements, *keyword, &std::pair<std::string_view, StatementReader>::first)};
+            if (found == kStatements.end()) {
+                line.fail(std::format("unknown statement {}", quoted(*keyword)));
+            }
+            found->second(state, line);
+        },
+        [](std::size_t number) {
+            throw SceneParseError{number, std::format("line longer than {} bytes", kMaxSceneLine)};
+        });
+    if (!state.scene.has_camera) {
+        throw SceneParseError{0, "the scene has no camera"};
+    }
+    state.scene.finalize();
+    return std::move(state.scene);
 }
 
 } // namespace

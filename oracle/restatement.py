@@ -30,6 +30,9 @@ def lib():
         l.oracle_intersect.restype = None
         l.oracle_intersect.argtypes = [c_void_p, _D, c_int64, c_double, c_double, c_int, _I32, _D, _I64, _I64, _D, _D,
                                        _D, _I32, _I64]
+        l.oracle_classify.restype = None
+        l.oracle_classify.argtypes = [c_void_p, _D, c_int64, c_double, c_double, c_double, c_int, _I32, _I64, _I64,
+                                      _I32, _D]
         _lib = l
     return _lib
 
@@ -51,3 +54,29 @@ def intersect(scene, rays: np.ndarray, t_min=0.0, t_max=float("inf"), threads: i
                            out["normal"].ctypes.data_as(_D), out["shading_normal"].ctypes.data_as(_D),
                            out["front"].ctypes.data_as(_I32), out["counts"].ctypes.data_as(_I64))
     return out
+
+
+# The FP32 error bound of the near-tie classification, in units of 2^-24 times
+# the largest coordinate magnitude involved (see trace_oracle.cpp).
+TIE_ULPS = 32.0
+
+
+def classify(scene, rays: np.ndarray, device: dict, t_min=0.0, t_max=float("inf"), ulps=TIE_ULPS,
+             threads: int = 8) -> dict:
+    """Classifies device closest-hit answers (dict with hit, object, triangle) against
+    the FP64 restatement: class 0 = the FP64 answer, 1 = a near-tie FP32 rounding
+    explains, 2 = unexplained; `detail` as oracle_classify documents it."""
+    from albedo_b200._lib import library
+
+    view = library().albedo_scene_host_view(scene.handle)
+    rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 6)
+    n = len(rays)
+    hit = np.ascontiguousarray(device["hit"], dtype=np.int32)
+    obj = np.ascontiguousarray(device["object"], dtype=np.int64)
+    tri = np.ascontiguousarray(device["triangle"], dtype=np.int64)
+    out = np.zeros(n, np.int32)
+    detail = np.zeros((n, 4))
+    lib().oracle_classify(view, rays.ctypes.data_as(_D), n, t_min, t_max, ulps, threads, hit.ctypes.data_as(_I32),
+                          obj.ctypes.data_as(_I64), tri.ctypes.data_as(_I64), out.ctypes.data_as(_I32),
+                          detail.ctypes.data_as(_D))
+    return {"class": out, "detail": detail}

@@ -296,6 +296,184 @@ bool objectHit(const HostScene& scene, std::uint32_t id, const Ray& ray, double 
     }
 }
 
+// ---------------------------------------------------------------- near-tie classification
+//
+// A device answer that differs from the FP64 one is a near-tie only when FP32
+// rounding can explain it. Rounding moves the primitives relative to the ray by
+// at most delta = ulps * 2^-24 * M, where M is the largest coordinate magnitude
+// among the ray origin, the crossing point and the primitive (its vertices, or
+// its centre and radius), in the primitive's own space (object space inside an
+// instance). So, for every primitive, its margin is measured in the plane
+// perpendicular to the ray: the distance from the ray to the primitive's
+// outline, positive when the ray passes through it, negative when it passes
+// beside it. A primitive may be hit by a rounded ray if margin >= -delta and is
+// surely hit if margin > delta (both with the crossing distance inside the query
+// range by more than delta). A device hit on a primitive is explained if that
+// primitive may be hit and lies no farther than the nearest sure hit plus both
+// deltas; a device miss is explained if no primitive is surely hit.
+
+struct Candidate {
+    double t{kInf};      // distance parameter of the crossing (closest approach for a miss)
+    double margin{-kInf};
+    double delta{0};
+    double scale{1};     // |d| in the primitive's space: t * scale is a distance there
+};
+
+double maxAbs(Vec3 v) { return std::max({std::abs(v.x), std::abs(v.y), std::abs(v.z)}); }
+
+// The signed distance in 2D from the origin to triangle (a, b, c): positive
+// inside (the ray passes through), minus the distance to the outline outside.
+double signedDistance2(const double a[2], const double b[2], const double c[2])
+{
+    const double* p[3]{a, b, c};
+    double area{(b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])};
+    if (area == 0) {
+        return -kInf;
+    }
+    const double orient{area > 0 ? 1.0 : -1.0};
+    bool inside{true};
+    double nearest_edge{kInf};
+    double outside{kInf};
+    for (int e{0}; e < 3; ++e) {
+        const double* u{p[e]};
+        const double* v{p[(e + 1) % 3]};
+        const double ex{v[0] - u[0]};
+        const double ey{v[1] - u[1]};
+        const double length{std::sqrt(ex * ex + ey * ey)};
+        // Signed distance of the origin from the edge's line, positive on the inner side.
+        const double side{orient * (ex * (0 - u[1]) - ey * (0 - u[0])) / length};
+        nearest_edge = std::min(nearest_edge, std::abs(side));
+        if (side < 0) {
+            inside = false;
+        }
+        // Distance from the origin to the segment.
+        double s{-(u[0] * ex + u[1] * ey) / (length * length)};
+        s = std::clamp(s, 0.0, 1.0);
+        const double qx{u[0] + s * ex};
+        const double qy{u[1] + s * ey};
+        outside = std::min(outside, std::sqrt(qx * qx + qy * qy));
+    }
+    return inside ? nearest_edge : -outside;
+}
+
+// An orthonormal pair perpendicular to unit `w`.
+void perpendicularPair(Vec3 w, Vec3& u, Vec3& v)
+{
+    const Vec3 helper{std::abs(w.x) < 0.6 ? Vec3{1, 0, 0} : Vec3{0, 1, 0}};
+    u = normalized(cross(helper, w));
+    v = cross(w, u);
+}
+
+Candidate triangleCandidate(const TriangleDesc& tri, const Ray& ray, double ulps)
+{
+    Candidate c;
+    const double length{std::sqrt(lengthSquared(ray.d))};
+    const Vec3 w{ray.d / length};
+    Vec3 u;
+    Vec3 v;
+    perpendicularPair(w, u, v);
+    double p2[3][2];
+    for (int k{0}; k < 3; ++k) {
+        const Vec3 off{tri.v[k] - ray.o};
+        p2[k][0] = dot(off, u);
+        p2[k][1] = dot(off, v);
+    }
+    c.margin = signedDistance2(p2[0], p2[1], p2[2]);
+    const Vec3 n{cross(tri.v[1] - tri.v[0], tri.v[2] - tri.v[0])};
+    const double denom{dot(n, ray.d)};
+    c.t = denom != 0 ? dot(n, tri.v[0] - ray.o) / denom : kInf;
+    double m{maxAbs(ray.o)};
+    for (const Vec3& p : tri.v) {
+        m = std::max(m, maxAbs(p));
+    }
+    if (std::isfinite(c.t)) {
+        m = std::max(m, maxAbs(ray.o + ray.d * c.t));
+    }
+    c.delta = ulps * 0x1p-24 * m;
+    c.scale = length;
+    return c;
+}
+
+// Both roots of a sphere (the closest approach twice for a miss).
+std::array<Candidate, 2> sphereCandidates(const SphereDesc& s, const Ray& ray, double ulps, bool wide)
+{
+    const double a{lengthSquared(ray.d)};
+    const double length{std::sqrt(a)};
+    const Vec3 oc{ray.o - s.center};
+    const double closest{-dot(ray.d, oc) / a};
+    const Vec3 l{oc + ray.d * closest};
+    const double miss_distance{std::sqrt(lengthSquared(l))};
+    Candidate c;
+    c.margin = s.radius - miss_distance;
+    c.scale = length;
+    // FP64-handled spheres (the device's wide spheres) round only the ray.
+    const double m{wide ? std::max(maxAbs(ray.o), maxAbs(ray.o + ray.d * closest))
+                        : std::max({maxAbs(ray.o), maxAbs(s.center) + s.radius})};
+    c.delta = ulps * 0x1p-24 * m;
+    std::array<Candidate, 2> roots{c, c};
+    if (c.margin >= 0) {
+        const double half{std::sqrt(std::max(s.radius * s.radius - miss_distance * miss_distance, 0.0)) / length};
+        roots[0].t = closest - half;
+        roots[1].t = closest + half;
+    } else {
+        roots[0].t = closest;
+        roots[1].t = closest;
+    }
+    return roots;
+}
+
+struct Verdict {
+    bool possible{false};
+    bool sure{false};
+};
+
+Verdict judge(const Candidate& c, double t_min, double t_max)
+{
+    const double along_min{(c.t - t_min) * c.scale};
+    const double along_max{(t_max - c.t) * c.scale};
+    Verdict v;
+    v.possible = c.margin >= -c.delta && along_min >= -c.delta && along_max >= -c.delta;
+    v.sure = c.margin > c.delta && along_min > c.delta && along_max > c.delta;
+    return v;
+}
+
+// Visits every primitive of the scene (no hierarchy: the classification must
+// not depend on the traversal it checks) with its world-space candidates.
+// visit(object, triangle (-1 for spheres and flattened triangles), candidate,
+// world distance per unit t).
+template <typename Visit>
+void forEachCandidate(const HostScene& scene, const Ray& world, double ulps, Visit&& visit)
+{
+    const double world_length{std::sqrt(lengthSquared(world.d))};
+    for (std::size_t id{0}; id < scene.objects.size(); ++id) {
+        const ObjectDesc& obj{scene.objects[id]};
+        switch (obj.kind) {
+        case ObjectKind::Sphere: {
+            const SphereDesc& s{scene.spheres[obj.index]};
+            const double extent{maxAbs(s.center) + s.radius};
+            for (const Candidate& c : sphereCandidates(s, world, ulps, extent >= 256.0)) {
+                visit(static_cast<std::int64_t>(id), std::int64_t{-1}, c, world_length);
+            }
+            break;
+        }
+        case ObjectKind::Triangle:
+            visit(static_cast<std::int64_t>(id), std::int64_t{-1},
+                  triangleCandidate(scene.triangles[obj.index], world, ulps), world_length);
+            break;
+        default: {
+            const InstanceDesc& inst{scene.instances[obj.index]};
+            const MeshDesc& mesh{scene.meshes[inst.mesh]};
+            const Ray local{inst.to_object.applyPoint(world.o), inst.to_object.applyVector(world.d)};
+            for (std::size_t k{0}; k < mesh.triangles.size(); ++k) {
+                visit(static_cast<std::int64_t>(id), static_cast<std::int64_t>(k),
+                      triangleCandidate(mesh.triangles[k], local, ulps), world_length);
+            }
+            break;
+        }
+        }
+    }
+}
+
 template <typename F>
 void parallelFor(std::int64_t count, int threads, F&& work)
 {
@@ -321,6 +499,24 @@ void parallelFor(std::int64_t count, int threads, F&& work)
     }
 }
 
+// Scene::intersect (scene/scene.cpp:107-133): the nearest object and its hit.
+std::int64_t nearestHit(const HostScene& scene, const Ray& ray, double t_min, double t_max, ShapeHit& nearest,
+                        Counts& counts)
+{
+    std::int64_t nearest_object{-1};
+    double range_max{t_max};
+    traverse(scene.tlas, ray, t_min, range_max, counts, [&](std::uint32_t id) {
+        ShapeHit h;
+        if (objectHit(scene, id, ray, t_min, range_max, h, counts)) {
+            nearest = h;
+            nearest_object = id;
+            range_max = h.t;
+        }
+        return false;
+    });
+    return nearest_object;
+}
+
 } // namespace
 
 extern "C" {
@@ -337,18 +533,8 @@ void oracle_intersect(const void* view, const double* rays, std::int64_t count, 
     parallelFor(count, threads, [&](std::int64_t i) {
         const Ray ray{{rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]}, {rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]}};
         Counts counts;
-        std::int64_t nearest_object{-1};
         ShapeHit nearest;
-        double range_max{t_max};
-        traverse(scene.tlas, ray, t_min, range_max, counts, [&](std::uint32_t id) {
-            ShapeHit h;
-            if (objectHit(scene, id, ray, t_min, range_max, h, counts)) {
-                nearest = h;
-                nearest_object = id;
-                range_max = h.t;
-            }
-            return false;
-        });
+        const std::int64_t nearest_object{nearestHit(scene, ray, t_min, t_max, nearest, counts)};
         out_hit[i] = nearest_object >= 0 ? 1 : 0;
         if (out_counts != nullptr) {
             out_counts[4 * i] = counts.boxes;
@@ -370,6 +556,73 @@ void oracle_intersect(const void* view, const double* rays, std::int64_t count, 
             out_point[3 * i + k] = comp(nearest.point, k);
             out_normal[3 * i + k] = comp(n, k);
             out_shading[3 * i + k] = comp(s, k);
+        }
+    });
+}
+
+// Classifies device closest-hit answers (hit flag, object id, triangle id within
+// an instanced mesh or -1) against the FP64 restatement: out_class[i] = 0 when
+// the device's answer is the FP64 one, 1 when it differs only by a near-tie
+// that FP32 rounding of `ulps` units explains (see Candidate above), 2 when
+// nothing explains it. For classes 1 and 2, out_detail (4 doubles per ray, may
+// be NULL) holds the device primitive's margin / delta, the nearest sure hit's
+// margin / delta, (t_device - t_sure) over the tie bound, and the number of
+// primitives that may be hit nearer than the sure one.
+void oracle_classify(const void* view, const double* rays, std::int64_t count, double t_min, double t_max,
+                     double ulps, int threads, const std::int32_t* device_hit, const std::int64_t* device_object,
+                     const std::int64_t* device_triangle, std::int32_t* out_class, double* out_detail)
+{
+    const HostScene& scene{*static_cast<const HostScene*>(view)};
+    parallelFor(count, threads, [&](std::int64_t i) {
+        const Ray ray{{rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]}, {rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]}};
+        Counts counts;
+        ShapeHit nearest;
+        const std::int64_t object{nearestHit(scene, ray, t_min, t_max, nearest, counts)};
+        const bool device_found{device_hit[i] != 0};
+        if ((object < 0 && !device_found) ||
+            (object >= 0 && device_found && device_object[i] == object && device_triangle[i] == nearest.triangle)) {
+            out_class[i] = 0;
+            return;
+        }
+        // The nearest sure hit, and the device's primitive among the candidates.
+        double sure_t{kInf};
+        Candidate sure;
+        Candidate mine;
+        bool mine_possible{false};
+        std::int64_t possible_nearer{0};
+        forEachCandidate(scene, ray, ulps, [&](std::int64_t id, std::int64_t tri, const Candidate& c, double) {
+            const Verdict v{judge(c, t_min, t_max)};
+            if (v.sure && c.t < sure_t) {
+                sure_t = c.t;
+                sure = c;
+            }
+            if (device_found && id == device_object[i] && tri == device_triangle[i] && v.possible) {
+                if (!mine_possible || std::abs(c.t) < std::abs(mine.t)) {
+                    mine = c;
+                }
+                mine_possible = true;
+            }
+        });
+        forEachCandidate(scene, ray, ulps, [&](std::int64_t, std::int64_t, const Candidate& c, double) {
+            if (judge(c, t_min, t_max).possible && c.t < sure_t) {
+                ++possible_nearer;
+            }
+        });
+        bool explained{false};
+        double tie{0};
+        if (!device_found) {
+            explained = !std::isfinite(sure_t);
+        } else if (mine_possible) {
+            const double bound{mine.delta / mine.scale + (std::isfinite(sure_t) ? sure.delta / sure.scale : 0)};
+            tie = std::isfinite(sure_t) ? (mine.t - sure_t) / bound : -kInf;
+            explained = !std::isfinite(sure_t) || mine.t - sure_t <= bound;
+        }
+        out_class[i] = explained ? 1 : 2;
+        if (out_detail != nullptr) {
+            out_detail[4 * i] = mine_possible ? mine.margin / mine.delta : -kInf;
+            out_detail[4 * i + 1] = std::isfinite(sure_t) ? sure.margin / sure.delta : kInf;
+            out_detail[4 * i + 2] = tie;
+            out_detail[4 * i + 3] = static_cast<double>(possible_nearer);
         }
     });
 }
