@@ -688,6 +688,36 @@ void fillTuning(albedo_tuning* out, const TuneOutcome& outcome)
 
 } // namespace
 
+namespace {
+
+// A render into host accumulators through the per-device staging buffer: one
+// copy in, the render, one copy out, then a synchronize. After the first call
+// of a size, a host render allocates nothing (an allocation can wait on the
+// driver for as long as a render takes); host renders on one device take turns
+// on the buffer.
+void renderThroughStaging(const albedo_scene& scene, const albedo_render_job& job, const albedo_camera* camera,
+                          albedo_accumulator* accumulators)
+{
+    static_cast<void>(renderArgsFor(scene, job));
+    const std::size_t bytes{static_cast<std::size_t>(job.width) * static_cast<std::size_t>(job.height) *
+                            sizeof(PixelAccum)};
+    int device{0};
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    HostStaging& staging{hostStaging(device)};
+    const std::lock_guard lock{staging.mutex};
+    if (staging.buffer.bytes < bytes) {
+        staging.buffer = DeviceBuffer{};
+        staging.buffer = DeviceBuffer{bytes};
+    }
+    check(cudaMemcpyAsync(staging.buffer.ptr, accumulators, bytes, cudaMemcpyHostToDevice, nullptr), "upload");
+    renderOnDevice(scene, job, staging.buffer.as<PixelAccum>(), nullptr, camera);
+    check(cudaMemcpyAsync(accumulators, staging.buffer.ptr, bytes, cudaMemcpyDeviceToHost, nullptr), "download");
+    check(cudaStreamSynchronize(nullptr), "render");
+    scene.collectKernelError();
+}
+
+} // namespace
+
 extern "C" {
 
 const char* albedo_last_error(void) { return g_last_error.c_str(); }
@@ -928,28 +958,13 @@ int albedo_render_view(const albedo_scene* scene, const albedo_render_job* job, 
 
 int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators)
 {
-    return guarded([&] {
-        static_cast<void>(renderArgsFor(*scene, *job));
-        const std::size_t bytes{static_cast<std::size_t>(job->width) * static_cast<std::size_t>(job->height) *
-                                sizeof(PixelAccum)};
-        // One device staging buffer per device, kept and grown as needed: after
-        // the first call of a size, a host render allocates nothing (an
-        // allocation can wait on the driver for as long as a render takes).
-        // Host renders on one device take turns on it.
-        int device{0};
-        check(cudaGetDevice(&device), "cudaGetDevice");
-        HostStaging& staging{hostStaging(device)};
-        const std::lock_guard lock{staging.mutex};
-        if (staging.buffer.bytes < bytes) {
-            staging.buffer = DeviceBuffer{};
-            staging.buffer = DeviceBuffer{bytes};
-        }
-        check(cudaMemcpyAsync(staging.buffer.ptr, accumulators, bytes, cudaMemcpyHostToDevice, nullptr), "upload");
-        renderOnDevice(*scene, *job, staging.buffer.as<PixelAccum>(), nullptr);
-        check(cudaMemcpyAsync(accumulators, staging.buffer.ptr, bytes, cudaMemcpyDeviceToHost, nullptr), "download");
-        check(cudaStreamSynchronize(nullptr), "render");
-        scene->collectKernelError();
-    });
+    return guarded([&] { renderThroughStaging(*scene, *job, nullptr, accumulators); });
+}
+
+int albedo_render_view_host(const albedo_scene* scene, const albedo_render_job* job, const albedo_camera* camera,
+                            albedo_accumulator* accumulators)
+{
+    return guarded([&] { renderThroughStaging(*scene, *job, camera, accumulators); });
 }
 
 int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* stream)
@@ -991,9 +1006,12 @@ int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* jo
         const cudaError_t e{renderNoAlloc(wf, scene->stack_capacity, 4 * sms, scene->error_flag.as<unsigned int>(),
                                           static_cast<cudaStream_t>(stream))};
         if (e == cudaErrorLaunchTimeout) {
-            throw DeviceError{"albedo_render_noalloc made no progress within its iteration bound"};
+            throw DeviceError{"albedo_render_noalloc exceeded its iteration bound before the image was complete"};
         }
         check(e, "albedo_render_noalloc");
+        // The render is complete on the stream: report a kernel-side error
+        // (a traversal stack overflow) now, as the host-buffer render does.
+        scene->collectKernelError();
     });
 }
 

@@ -51,12 +51,15 @@ void scanChunks(std::span<const Prim> prims, unsigned chunks, F&& scan)
         const std::size_t end{prims.size() * (c + 1) / chunks};
         return prims.subspan(begin, end - begin);
     };
-    std::vector<std::thread> workers;
+    // A jthread joins when destroyed, so an exception that leaves early (a
+    // thread that fails to start, or the calling thread's own share) still
+    // waits for the workers already running.
+    std::vector<std::jthread> workers;
     for (unsigned c{1}; c < chunks; ++c) {
         workers.emplace_back([&, c] { scan(c, piece(c)); });
     }
     scan(0u, piece(0));
-    for (std::thread& worker : workers) {
+    for (std::jthread& worker : workers) {
         worker.join();
     }
 }
@@ -358,12 +361,15 @@ BuiltBvh buildBvh(std::span<const Box3> primitive_bounds, unsigned threads)
         bvh.nodes.resize(root->total);
         std::vector<std::pair<const Piece*, std::size_t>> copies;
         layOut(*root, bvh.nodes, 0, copies);
-        std::vector<std::thread> workers;
+        // A jthread joins when destroyed, so an exception that leaves early (a
+        // thread that fails to start, or the calling thread's own share) still
+        // waits for the workers already running.
+        std::vector<std::jthread> workers;
         for (std::size_t t{1}; t < copies.size(); ++t) {
             workers.emplace_back([&, t] { copyPiece(*copies[t].first, bvh.nodes, copies[t].second); });
         }
         copyPiece(*copies[0].first, bvh.nodes, copies[0].second);
-        for (std::thread& worker : workers) {
+        for (std::jthread& worker : workers) {
             worker.join();
         }
     }

@@ -351,7 +351,10 @@ DeviceImage flattenScene(const HostScene& scene)
         const std::size_t chunks{count < (std::size_t{1} << 16)
                                      ? 1
                                      : std::max<std::size_t>(1, std::thread::hardware_concurrency())};
-        std::vector<std::thread> workers;
+        // A jthread joins when destroyed, so an exception that leaves early (a
+        // thread that fails to start, or the calling thread's own share) still
+        // waits for the workers already running.
+        std::vector<std::jthread> workers;
         const auto convert = [&](std::size_t chunk) {
             for (std::size_t pos{count * chunk / chunks}; pos < count * (chunk + 1) / chunks; ++pos) {
                 const std::uint32_t t{mesh.bvh.order[pos]};
@@ -364,7 +367,7 @@ DeviceImage flattenScene(const HostScene& scene)
             workers.emplace_back(convert, chunk);
         }
         convert(0);
-        for (std::thread& worker : workers) {
+        for (std::jthread& worker : workers) {
             worker.join();
         }
         const Emitted blas{emitBvh(mesh.bvh, base, image.nodes)};

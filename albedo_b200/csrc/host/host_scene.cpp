@@ -136,12 +136,15 @@ template <typename F>
 void forEachChunk(std::size_t n, std::size_t chunks, F&& body)
 {
     const auto range = [&](std::size_t chunk) { return n * chunk / chunks; };
-    std::vector<std::thread> workers;
+    // A jthread joins when destroyed, so an exception that leaves early (a
+    // thread that fails to start, or the calling thread's own share) still
+    // waits for the workers already running.
+    std::vector<std::jthread> workers;
     for (std::size_t chunk{1}; chunk < chunks; ++chunk) {
         workers.emplace_back([&, chunk] { body(chunk, range(chunk), range(chunk + 1)); });
     }
     body(0, range(0), range(1));
-    for (std::thread& worker : workers) {
+    for (std::jthread& worker : workers) {
         worker.join();
     }
 }

@@ -398,14 +398,17 @@ ObjMesh parseObj(std::string_view text, const ObjBudget& budget, unsigned pieces
         }
     }
     const auto onThreads = [&](auto&& work) {
-        std::vector<std::thread> workers;
+        // A jthread joins when destroyed, so an exception that leaves early (a
+        // thread that fails to start, or the calling thread's own share) still
+        // waits for the workers already running.
+        std::vector<std::jthread> workers;
         for (std::size_t k{1}; k < parts.size(); ++k) {
             workers.emplace_back([&, k] { work(k); });
         }
         if (!parts.empty()) {
             work(0);
         }
-        for (std::thread& worker : workers) {
+        for (std::jthread& worker : workers) {
             worker.join();
         }
     };

@@ -43,7 +43,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 std::mutex g_setup_mutex;
 void* g_scratch_address[kMaxDevices] = {};
 
-// Once per device, with that device current: the device address of the scratch.
+// Once per device, with that device current: the device address of the
+// scratch. The address is kept for the life of the process, so rendering on a
+// device after cudaDeviceReset (which ends the context the address belongs
+// to) is not supported.
 cudaError_t scratchAddress(void** out)
 {
     int device = 0;
@@ -106,8 +109,8 @@ WfBuffers carve(void* base, int slots, WfJob** job)
 int noAllocMaxPixels() { return kNoAllocMaxSlots; }
 
 // Renders one job with one path slot per pixel inside the static scratch.
-// Returns cudaSuccess, a CUDA error, or cudaErrorLaunchTimeout if the batch
-// stops making progress.
+// Returns cudaSuccess, a CUDA error, or cudaErrorLaunchTimeout if the render
+// is not complete within its iteration bound.
 cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int* error_flag, cudaStream_t stream)
 {
     const long long pixels = static_cast<long long>(job.width) * job.height;
@@ -142,9 +145,10 @@ cudaError_t renderNoAlloc(const WfJob& job, int stack, int blocks, unsigned int*
         return e;
     }
     const WfLaunch launch{blocks, 128, stack, per_sm * sms, 32, 0};
-    // A slot finishes its pixel within n^2 (max_depth + 2) iterations.
+    // A slot finishes its pixel within n^2 (max_depth + 2) iterations: the
+    // total iteration bound (computed in 64 bits; max_depth may be near INT_MAX).
     const unsigned long long bound = static_cast<unsigned long long>(job.samples_per_axis) * job.samples_per_axis *
-                                         static_cast<unsigned long long>(job.max_depth + 2) +
+                                         (static_cast<unsigned long long>(job.max_depth) + 2) +
                                      16;
     constexpr int kIterationsPerCheck = 8;
     WfControl snapshot{};

@@ -183,7 +183,7 @@ int WavefrontEngine::submit(const WfJob& input)
     job_pixels_.push_back(pixels);
     in_flight_.push_back(index);
     const auto n2{static_cast<unsigned long long>(input.samples_per_axis) * input.samples_per_axis};
-    stall_limit_ = std::max(stall_limit_, n2 * static_cast<unsigned long long>(input.max_depth + 2) + 16);
+    stall_limit_ = std::max(stall_limit_, n2 * (static_cast<unsigned long long>(input.max_depth) + 2) + 16);
     return index;
 }
 

@@ -377,3 +377,27 @@ def request_view(base: tuple, rng: np.random.Generator) -> tuple:
     target = (target[0] + rng.uniform(-0.5, 0.5), target[1] + rng.uniform(-0.3, 0.3),
               target[2] + rng.uniform(-0.5, 0.5))
     return eye, target, up, fov
+
+
+def flattened_parts(seed: int = 29) -> list[tuple]:
+    """A scene of meshes added flattened, every triangle its own object
+    (Scene::add(const TriangleMesh&, ...), scene/scene.cpp:33-61), between
+    spheres, in this add order: a trefoil tube placed by a seeded rotation and
+    scale, a sphere, a displaced level-5 icosphere (20,480 triangles), two
+    spheres. Positions are rounded to FP32 so both renderers hold the same
+    vertices. Parts are ("triangles", positions, faces) or ("sphere", centre,
+    radius)."""
+    rng = Pcg32(seed)
+    points, quads = trefoil_mesh(128, 16)
+    faces = np.concatenate([quads[:, [0, 1, 2]], quads[:, [0, 2, 3]]])
+    angle = rng.uniform(0, 2 * np.pi)
+    scale = rng.uniform(0.7, 0.9)
+    rot = np.array([[np.cos(angle), 0, np.sin(angle)], [0, 1, 0], [-np.sin(angle), 0, np.cos(angle)]])
+    knot = (points.astype(np.float64) @ rot.T) * scale * 0.5 + np.array([-0.8, 1.4, -0.6])
+    ball_points, ball_faces = displaced_icosphere(5, seed)
+    ball = ball_points.astype(np.float64) * 0.9 + np.array([1.1, 1.0, 0.2])
+    return [("triangles", knot.astype(np.float32).astype(np.float64), faces),
+            ("sphere", (0.0, 0.4, 1.4), 0.4),
+            ("triangles", ball.astype(np.float32).astype(np.float64), ball_faces),
+            ("sphere", (-1.6, 0.5, 1.2), 0.5),
+            ("sphere", (0.0, -1000.0, 0.0), 1000.0)]

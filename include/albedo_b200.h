@@ -195,6 +195,11 @@ int albedo_render_host(const albedo_scene* scene, const albedo_render_job* job, 
  * camera on a resident scene. */
 int albedo_render_view(const albedo_scene* scene, const albedo_render_job* job, const albedo_camera* camera,
                        albedo_accumulator* accumulators, void* stream);
+/* albedo_render_host from the given camera (NULL: the scene's): renderImage
+ * (render/render_image.hpp:36-49) with a host PixelBuffer and the job's own
+ * camera, as the C++ adapter include/albedo_b200_adapter.hpp calls it. */
+int albedo_render_view_host(const albedo_scene* scene, const albedo_render_job* job, const albedo_camera* camera,
+                            albedo_accumulator* accumulators);
 /* Renders only the listed pixels (x, y pairs) into one host accumulator each,
  * optionally also returning per-pixel sums of squared samples (3 doubles each). */
 int albedo_render_pixels_host(const albedo_scene* scene, const albedo_render_job* job, const int32_t* pixels,
@@ -228,7 +233,11 @@ int albedo_render_batch(const albedo_batch_item* items, int32_t count, void* str
  * capture. All calls share the array and it keeps the last call's contents:
  * each call clears what must start at zero, and calls that overlap on the GPU
  * race, so do not overlap them. `accumulators` is a device array of width *
- * height entries; the call returns after the render is complete on `stream`. */
+ * height entries. The call synchronizes `stream`: it returns once the render
+ * is complete, with a kernel-reported error (ALBEDO_TRAVERSAL_ERROR) already
+ * collected. The array's address is looked up once per device for the life of
+ * the process, so calls after cudaDeviceReset on that device are not
+ * supported. */
 int albedo_render_noalloc(const albedo_scene* scene, const albedo_render_job* job, albedo_accumulator* accumulators,
                           void* stream);
 /* Film output (image/ppm.cpp:22-85, color/srgb.cpp:18-36). albedo_resolve_srgb

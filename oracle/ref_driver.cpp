@@ -5,6 +5,7 @@
 // parity tests and the CPU baseline call; nothing in the product links it.
 // Every entry point only calls public reference API:
 //   readScene                         scene/scene_file.hpp:133-146
+//   Scene::add (shapes, TriangleMesh)  scene/scene.hpp:31-62
 //   renderImage / RenderJob           render/render_image.hpp:17-49
 //   SampleGenerator::forPixel         sampling/sample_generator.hpp:35-45
 //   PerspectiveCamera::generateRay    camera/perspective_camera.cpp:74-87
@@ -141,6 +142,48 @@ void* ref_scene_load(const char* path)
         return nullptr;
     }
     return scene;
+}
+
+// A scene built through Scene's own add calls (scene/scene.hpp:31-62) instead
+// of a file: ref_scene_create, then ref_scene_add_triangles (Scene::add of a
+// TriangleMesh: every triangle its own object, scene/scene.cpp:33-61) and
+// ref_scene_add_sphere in any order. Materials are black diffuse: these scenes
+// serve ray queries.
+void* ref_scene_create()
+{
+    RefScene* scene{nullptr};
+    if (guarded([&] { scene = new RefScene{}; }) != 0) {
+        return nullptr;
+    }
+    return scene;
+}
+
+int ref_scene_add_triangles(void* handle, const double* positions, std::int64_t position_count,
+                            const std::int64_t* faces, std::int64_t face_count)
+{
+    return guarded([&] {
+        std::vector<Point3r> points;
+        points.reserve(static_cast<std::size_t>(position_count));
+        for (std::int64_t i{0}; i < position_count; ++i) {
+            points.push_back({positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]});
+        }
+        std::vector<TriangleMesh::Face> corners;
+        corners.reserve(static_cast<std::size_t>(face_count));
+        for (std::int64_t f{0}; f < face_count; ++f) {
+            corners.push_back({static_cast<std::size_t>(faces[3 * f]), static_cast<std::size_t>(faces[3 * f + 1]),
+                               static_cast<std::size_t>(faces[3 * f + 2])});
+        }
+        static_cast<RefScene*>(handle)->description.scene.add(TriangleMesh{std::move(points), std::move(corners)},
+                                                              Material{DiffuseMaterial{}});
+    });
+}
+
+int ref_scene_add_sphere(void* handle, const double* center, double radius)
+{
+    return guarded([&] {
+        static_cast<RefScene*>(handle)->description.scene.add(Sphere{{center[0], center[1], center[2]}, radius},
+                                                              Material{DiffuseMaterial{}});
+    });
 }
 
 void ref_scene_free(void* handle) { delete static_cast<RefScene*>(handle); }

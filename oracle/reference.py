@@ -26,6 +26,9 @@ _PROTOTYPES = {
     "ref_available_threads": (c_int, []),
     "ref_scene_load": (c_void_p, [c_char_p]),
     "ref_scene_free": (None, [c_void_p]),
+    "ref_scene_create": (c_void_p, []),
+    "ref_scene_add_triangles": (c_int, [c_void_p, _D, c_int64, _I64, c_int64]),
+    "ref_scene_add_sphere": (c_int, [c_void_p, _D, c_double]),
     "ref_scene_object_count": (c_int64, [c_void_p]),
     "ref_render_image": (c_int, [c_void_p, c_int, c_int, c_int, c_uint64, c_int, c_int, c_int, _D]),
     "ref_render_pixels": (c_int, [c_void_p, c_int, c_int, c_int, c_uint64, c_int, c_int, c_int, c_int, _I32, c_int64,
@@ -89,6 +92,27 @@ class RefScene:
         if not handle:
             raise RuntimeError(lib().ref_last_error().decode())
         self.handle = c_void_p(handle)
+
+    @classmethod
+    def create(cls) -> "RefScene":
+        """An empty Scene filled by add_triangles / add_sphere (Scene::add)."""
+        scene = cls.__new__(cls)
+        handle = lib().ref_scene_create()
+        if not handle:
+            raise RuntimeError(lib().ref_last_error().decode())
+        scene.handle = c_void_p(handle)
+        return scene
+
+    def add_triangles(self, positions: np.ndarray, faces: np.ndarray) -> None:
+        """Scene::add(TriangleMesh, material): every triangle its own object."""
+        positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        faces = np.ascontiguousarray(faces, dtype=np.int64).reshape(-1, 3)
+        _check(lib().ref_scene_add_triangles(self.handle, _d(positions), len(positions), faces.ctypes.data_as(_I64),
+                                             len(faces)))
+
+    def add_sphere(self, center, radius: float) -> None:
+        c = np.ascontiguousarray(center, dtype=np.float64)
+        _check(lib().ref_scene_add_sphere(self.handle, _d(c), float(radius)))
 
     def __del__(self):
         if getattr(self, "handle", None) is not None and lib is not None:

@@ -18,7 +18,12 @@ from oracle import restatement
 
 pytestmark = pytest.mark.skipif(not (ref.available() and restatement.available()), reason="oracle not built")
 
-ASSETS = Path("/root/reference/assets")
+
+def _assets() -> Path | None:
+    from oracle import reference_root
+
+    root = reference_root()
+    return root / "assets" if root is not None else None
 
 
 def random_rays(count, seed, low, high):
@@ -31,8 +36,9 @@ def random_rays(count, seed, low, high):
 
 def scene_paths(room_path, trefoil_path):
     paths = [room_path, trefoil_path]
-    if (ASSETS / "meshes.scene").exists():
-        paths.append(ASSETS / "meshes.scene")
+    assets = _assets()
+    if assets is not None and (assets / "meshes.scene").exists():
+        paths.append(assets / "meshes.scene")
     return paths
 
 
@@ -70,3 +76,39 @@ def test_restatement_reports_triangles_inside_instances(trefoil_path):
     assert np.all(ours["triangle"][instanced] >= 0)
     assert np.all(ours["triangle"][hit & ~instanced] == -1)
     assert (ours["counts"][hit][:, 0] > 0).all()
+
+
+def build_flattened(parts):
+    """The same scene on both sides: ours through albedo_scene_add_triangles /
+    add_sphere, the reference's through Scene::add (TriangleMesh and Sphere)."""
+    ours = ab.Scene.create()
+    ours.set_camera((0, 2, 6), (0, 1, 0))
+    material = ours.add_material(ab.BasicMaterial("diffuse", a=(0.5, 0.5, 0.5)))
+    theirs = ref.RefScene.create()
+    for part in parts:
+        if part[0] == "triangles":
+            ours.add_triangles(part[1], part[2], material)
+            theirs.add_triangles(part[1], part[2])
+        else:
+            ours.add_sphere(part[1], part[2], material)
+            theirs.add_sphere(part[1], part[2])
+    return ours, theirs
+
+
+def test_flattened_meshes_give_the_reference_object_ids():
+    """Meshes added flattened make every triangle its own object, in add order,
+    under one TLAS: object ids, t and points equal the reference's bit for bit."""
+    from albedo_b200 import scenes
+
+    ours, theirs = build_flattened(scenes.flattened_parts())
+    ours.prepare()
+    assert ours.info()["objects"] == theirs.object_count() == 4096 + 20480 + 3
+    rays = random_rays(50_000, 33, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    mine = restatement.intersect(ours, rays)
+    their = theirs.intersect(rays)
+    np.testing.assert_array_equal(mine["hit"], their["hit"])
+    hit = mine["hit"] == 1
+    assert hit.mean() > 0.3
+    np.testing.assert_array_equal(mine["object"][hit], their["object"][hit])
+    np.testing.assert_array_equal(mine["t"][hit], their["t"][hit])
+    np.testing.assert_array_equal(mine["point"][hit], their["point"][hit])

@@ -7,6 +7,9 @@ calls it through the C ABI twice in a row, on the same scene and job, and checks
 each result against the existing wavefront entry point (albedo_render), with the
 tolerance the wavefront tests use: identical sample counts, image sums within
 1e-4 relative, and at most 0.5% of pixels differing by more than 1e-3 relative.
+The second call must leave the device's free memory (cudaMemGetInfo) and the
+torch allocator's counters exactly as they were: the first call on a device may
+still load kernels, the second has nothing left to load or allocate.
 It also checks that an image over the 65,536-pixel limit is refused. It is named
 to be collected last, so a run that stops at its first failure has run every
 other test before it.
@@ -60,7 +63,21 @@ def test_noalloc_matches_the_allocating_entry_point_twice(room_path):
     expected = existing_render(scene, job)
     assert np.all(counts(expected) == 16)
     first = noalloc_render(scene, job)
-    second = noalloc_render(scene, job)
+    acc = torch.zeros((job.width * job.height, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    allocated_before = torch.cuda.memory_allocated()
+    reserved_before = torch.cuda.memory_reserved()
+    c = job.to_c()
+    status = library().albedo_render_noalloc(scene.handle, byref(c), c_void_p(acc.data_ptr()), c_void_p(0))
+    assert status == 0, library().albedo_last_error().decode()
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert torch.cuda.memory_allocated() == allocated_before
+    assert torch.cuda.memory_reserved() == reserved_before
+    scene.check()
+    second = acc.cpu().numpy()
     assert_same_image(first, expected)
     assert_same_image(second, expected)
 
