@@ -550,6 +550,13 @@ def algorithmic_bytes(counts: dict, boxes: str = "reference_boxes") -> int:
     return 32 * counts[boxes] + 48 * counts["triangles"] + 32 * counts["spheres"] + 96 * counts["instances"]
 
 
+def read_sweep(data_ptr: int, nbytes: int, repeats: int, blocks: int, sink_ptr: int, stream: int = 0) -> None:
+    """Reads `nbytes` of device memory `repeats` times through L2 (asynchronous;
+    the caller times it): the L2 read bandwidth probe."""
+    _raise(library().albedo_probe_read_sweep(c_void_p(data_ptr), nbytes, repeats, blocks, c_void_p(sink_ptr),
+                                             c_void_p(stream)))
+
+
 def render_pixels(scene: Scene, job: RenderJob, pixels: np.ndarray, with_squares: bool = False):
     """Renders only the listed (x, y) pixels; returns accumulators (and sums of squares)."""
     pixels = np.ascontiguousarray(pixels, dtype=np.int32).reshape(-1, 2)
@@ -567,5 +574,5 @@ __all__ = [
     "MEGAKERNEL", "NORMALS", "PATH", "PixelBuffer", "RenderJob", "SCATTER_ONLY", "Scene", "SceneParseError",
     "Server", "Unsupported", "WAVEFRONT", "read_scene", "render_batch", "render_device", "render_image",
     "render_pixels", "Accumulator", "autotune_batch", "autotune_megakernel", "resolve_srgb", "save_ppm",
-    "set_tuning", "srgb_tables", "srgb_thresholds", "trace_work_counts", "tuning", "wavefront_last_rays", "write_ppm",
+    "read_sweep", "set_tuning", "srgb_tables", "srgb_thresholds", "trace_work_counts", "tuning", "wavefront_last_rays", "write_ppm",
 ]

@@ -78,6 +78,7 @@ PROTOTYPES: dict[str, tuple] = {
     "albedo_render": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p, c_void_p]),
     "albedo_render_host": (c_int32, [c_void_p, POINTER(RenderJobC), c_void_p]),
     "albedo_render_view": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(CameraC), c_void_p, c_void_p]),
+    "albedo_probe_read_sweep": (c_int32, [c_void_p, c_int64, c_int32, c_int32, c_void_p, c_void_p]),
     "albedo_render_view_host": (c_int32, [c_void_p, POINTER(RenderJobC), POINTER(CameraC), c_void_p]),
     "albedo_render_pixels_host": (c_int32, [c_void_p, POINTER(RenderJobC), _I, c_int64, c_void_p, _D3]),
     "albedo_scene_check": (c_int32, [c_void_p]),

@@ -1721,6 +1721,19 @@ int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, fl
     });
 }
 
+int albedo_probe_read_sweep(const void* data, int64_t bytes, int32_t repeats, int32_t blocks, void* sink,
+                            void* stream)
+{
+    return guarded([&] {
+        if (data == nullptr || sink == nullptr || bytes < 16 || bytes % 16 != 0 || repeats <= 0 || blocks <= 0 ||
+            reinterpret_cast<std::uintptr_t>(data) % 16 != 0 || reinterpret_cast<std::uintptr_t>(sink) % 16 != 0) {
+            throw std::invalid_argument{"read sweep: 16-byte aligned data and sink, bytes a positive multiple of 16, "
+                                        "positive repeats and blocks"};
+        }
+        check(launchReadSweep(data, bytes, repeats, blocks, sink, static_cast<cudaStream_t>(stream)), "read sweep");
+    });
+}
+
 int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64_t count, float t_min, float t_max,
                              int32_t any, int32_t persistent, int32_t* out_hit, uint32_t* out_t_bits,
                              uint32_t* out_object_position, uint32_t* out_triangle_position)

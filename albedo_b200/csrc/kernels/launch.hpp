@@ -138,6 +138,9 @@ cudaError_t launchLobeEval(int kind, const float* params, const float* wo_wi, in
 cudaError_t launchLobeSample(int kind, const float* params, const float* inputs, int count, int* out_valid,
                              float* out_dir, float* out_weight, float* out_pdf, int* out_specular, cudaStream_t stream);
 cudaError_t launchPerlin(const float* points, int count, float* out_noise, float* out_turbulence, cudaStream_t stream);
+// Reads `bytes` (a multiple of 16, 16-byte aligned) `repeats` times through L2.
+cudaError_t launchReadSweep(const void* data, long long bytes, int repeats, int blocks, void* sink,
+                            cudaStream_t stream);
 cudaError_t launchCameraRays(const DevCamera& camera, const float* film, int count, float* out_rays,
                              cudaStream_t stream);
 

@@ -1,6 +1,7 @@
 // Probe kernels: run one piece of device arithmetic over arrays of inputs so the
 // parity tests can compare it, input for input, with the reference: the pixel
-// random stream, the BSDF lobes, Perlin noise and camera rays.
+// random stream, the BSDF lobes, Perlin noise and camera rays. Also a read
+// sweep that measures the L2 read bandwidth the traversal roofline divides by.
 #include "estimator.cuh"
 
 namespace albedo_b200 {
@@ -106,7 +107,53 @@ __global__ void cameraRaysKernel(const DevCamera camera, const float* film, int 
     out_rays[6 * i + 5] = d.z;
 }
 
+// Reads `words` 16-byte words `repeats` times, grid-stride, four independent
+// loads in flight per thread, through L2 only (ld.global.cg: L1 is skipped, so
+// an SM re-reading its share is served by L2). The words fold into one value
+// per thread, stored only if it equals a pattern that seeded data does not
+// produce, so no load can be dropped.
+__global__ void __launch_bounds__(256) readSweepKernel(const uint4* __restrict__ data, long long words, int repeats,
+                                                       uint4* sink)
+{
+    uint4 acc = make_uint4(0u, 0u, 0u, 0u);
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    const long long first = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (int r = 0; r < repeats; ++r) {
+        long long i = first;
+        for (; i + 3 * stride < words; i += 4 * stride) {
+            const uint4 a = __ldcg(data + i);
+            const uint4 b = __ldcg(data + i + stride);
+            const uint4 c = __ldcg(data + i + 2 * stride);
+            const uint4 d = __ldcg(data + i + 3 * stride);
+            acc.x ^= a.x ^ b.x ^ c.x ^ d.x;
+            acc.y ^= a.y ^ b.y ^ c.y ^ d.y;
+            acc.z ^= a.z ^ b.z ^ c.z ^ d.z;
+            acc.w ^= a.w ^ b.w ^ c.w ^ d.w;
+        }
+        for (; i < words; i += stride) {
+            const uint4 a = __ldcg(data + i);
+            acc.x ^= a.x;
+            acc.y ^= a.y;
+            acc.z ^= a.z;
+            acc.w ^= a.w;
+        }
+    }
+    if (acc.x == 0x9e3779b9u && acc.y == 0x7f4a7c15u && acc.z == 0x85ebca6bu && acc.w == 0xc2b2ae35u) {
+        sink[0] = acc;
+    }
+}
+
 } // namespace
+
+cudaError_t launchReadSweep(const void* data, long long bytes, int repeats, int blocks, void* sink,
+                            cudaStream_t stream)
+{
+    if (bytes >= 16 && repeats > 0 && blocks > 0) {
+        readSweepKernel<<<blocks, 256, 0, stream>>>(static_cast<const uint4*>(data), bytes / 16, repeats,
+                                                   static_cast<uint4*>(sink));
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launchPixelStream(unsigned long long seed, int x, int y, int width, int count, unsigned int* out_u32,
                               float* out_real, cudaStream_t stream)

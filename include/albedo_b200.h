@@ -399,6 +399,14 @@ int albedo_probe_lobe_sample(int32_t kind, const float* params, const float* inp
 int albedo_probe_perlin(const float* points, int32_t count, float* out_noise, float* out_turbulence);
 int albedo_probe_camera_rays(const albedo_scene* scene, int32_t width, int32_t height, const float* film,
                              int32_t count, float* out_rays);
+/* Reads `bytes` of device memory at `data` (16-byte aligned, a multiple of 16
+ * bytes) `repeats` times through L2 (L1 skipped) with `blocks` blocks of 256
+ * threads, writing at most 16 bytes to the device `sink`; asynchronous on
+ * `stream`. Timed by the caller, it gives the L2 read bandwidth that the
+ * traversal of a scene resident in L2 is measured against. No counterpart in
+ * the reference. */
+int albedo_probe_read_sweep(const void* data, int64_t bytes, int32_t repeats, int32_t blocks, void* sink,
+                            void* stream);
 /* Closest-hit (any = 0) or any-hit queries of given rays, traced as the
  * wavefront's persistent kernels trace them (persistent = 1: a turn descends
  * nodes then handles a leaf; 2: a turn is one step) or one query per thread

@@ -1,13 +1,13 @@
 """Fixed render cases for profiling under ncu: one render, nothing else.
 
-    python -m albedo_b200.profiling megakernel --width 480 --height 270 --spp 64 [--autotune]
+    python tests/profile_cases.py megakernel --width 480 --height 270 --spp 64 [--autotune]
                                    [--accumulation fp64|kahan]
-    python -m albedo_b200.profiling wavefront --width 480 --height 270 --spp 16 [--autotune]
-    python -m albedo_b200.profiling resolve --width 3840 --height 2160
+    python tests/profile_cases.py wavefront --width 480 --height 270 --spp 16 [--autotune]
+    python tests/profile_cases.py resolve --width 3840 --height 2160
 
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
---scene icosphere6 (a displaced icosphere of 6 levels, 81,920 triangles), max
-depth 10, seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
+--scene icosphere6 or icosphere8 (displaced icospheres of 6 and 8 levels, 81,920 and
+1,310,720 triangles), max depth 10 (16 for icosphere8, as the bench frame), seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
 nodes then leaf, 1: one step). With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
@@ -20,8 +20,11 @@ from __future__ import annotations
 
 import argparse
 import math
+import sys
 import tempfile
 from pathlib import Path
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
 
 # Megakernel launches one tuning pass makes: every shape (3 tile widths x 3
 # kernel variants) once untimed and twice timed.
@@ -36,7 +39,8 @@ def main() -> None:
     parser.add_argument("--spp", type=int, default=16)
     parser.add_argument("--no-warmup", action="store_true")
     parser.add_argument("--autotune", action="store_true")
-    parser.add_argument("--scene", choices=["trefoil", "icosphere6"], default="trefoil")
+    parser.add_argument("--scene", choices=["trefoil", "icosphere6", "icosphere8"], default="trefoil")
+    parser.add_argument("--depth", type=int, default=None, help="max depth (default 10; 16 for icosphere8)")
     parser.add_argument("--trace-loop", type=int, choices=[0, 1], default=None)
     parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
                         help="megakernel per-pixel sums: FP64 or Kahan-compensated FP32")
@@ -52,8 +56,8 @@ def main() -> None:
         return
     n = int(round(math.sqrt(args.spp)))
     with tempfile.TemporaryDirectory() as tmp:
-        if args.scene == "icosphere6":
-            scene = ab.Scene.load(scenes.icosphere_scene(Path(tmp), levels=6))
+        if args.scene.startswith("icosphere"):
+            scene = ab.Scene.load(scenes.icosphere_scene(Path(tmp), levels=int(args.scene[-1])))
         else:
             scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
         if args.trace_loop is not None:
@@ -63,7 +67,8 @@ def main() -> None:
                           slot_count=shape["slot_count"], trace_loop=args.trace_loop)
         method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
         accumulation = ab.ACCUMULATE_KAHAN_FP32 if args.accumulation == "kahan" else ab.ACCUMULATE_FP64
-        job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=10, method=method,
+        depth = args.depth if args.depth is not None else (16 if args.scene == "icosphere8" else 10)
+        job = ab.RenderJob(args.width, args.height, samples_per_axis=n, max_depth=depth, method=method,
                            accumulation=accumulation)
         acc = torch.zeros((args.width * args.height, 4), dtype=torch.float64, device="cuda")
         before = 0
