@@ -99,18 +99,6 @@ ALB_DEV NeeCandidate directLightCandidate(const DevScene& s, const Surface& sf, 
     return nc;
 }
 
-// sampleDirectLight: the candidate, confirmed by a shadow query.
-template <typename Ctx>
-ALB_DEV float3 sampleDirectLight(const DevScene& s, const Ctx& c, const Surface& sf, const Scattering& sc,
-                                 float3 wo, Pcg32& g)
-{
-    const NeeCandidate nc = directLightCandidate(s, sf, sc, wo, g);
-    if (!nc.valid || (nc.needs_test && occluded(s, c, nc.origin, nc.dir, nc.range_max, nc.skip))) {
-        return gray(0.0f);
-    }
-    return nc.contribution;
-}
-
 // The state of one path between bounces: PathEstimator::radiance's loop
 // variables (estimator/path_estimator.cpp:155-160) plus the skip rule of the ray.
 struct PathState {
@@ -170,38 +158,57 @@ ALB_DEV float3 weightedSky(const DevScene& s, const PathState& p)
 
 // The part of a bounce after the surface is known: next-event estimation, BSDF
 // sampling and roulette. Returns false when the path ends.
+//
+// The light sample's shadow query runs last, once the path's next ray is
+// known: it draws no random numbers and its contribution is added to the
+// result exactly as before the BSDF sample (the sample never touches the
+// result), but the surface and its scattering are then dead, so the traversal
+// call does not carry them.
 template <typename Ctx>
 ALB_DEV bool scatterAtSurface(const DevScene& s, const Ctx& c, PathState& p, const Surface& sf, Pcg32& g,
                               int roulette_start)
 {
-    const Scattering sc = scatteringAt(s, sf);
-    const float3 wo = -p.d;
-    p.result = p.result + p.throughput * sampleDirectLight(s, c, sf, sc, wo, g);
-    const float u_choice = g.next1D();
-    const float ux = g.next1D();
-    const float uy = g.next1D();
-    ScatterSample smp;
-    if (!sc.sample(wo, u_choice, ux, uy, smp)) {
-        return false;
-    }
-    p.throughput = p.throughput * smp.weight;
-    if (isBlack(p.throughput)) {
-        return false;
-    }
-    if (p.depth >= roulette_start) {
-        const float survival = fminf(0.95f, fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z)));
-        if (g.next1D() >= survival) {
-            return false;
+    const float3 throughput_here = p.throughput;
+    NeeCandidate nc;
+    bool alive = true;
+    {
+        const Scattering sc = scatteringAt(s, sf);
+        const float3 wo = -p.d;
+        nc = directLightCandidate(s, sf, sc, wo, g);
+        const float u_choice = g.next1D();
+        const float ux = g.next1D();
+        const float uy = g.next1D();
+        ScatterSample smp;
+        if (!sc.sample(wo, u_choice, ux, uy, smp)) {
+            alive = false;
+        } else {
+            p.throughput = p.throughput * smp.weight;
+            if (isBlack(p.throughput)) {
+                alive = false;
+            } else {
+                if (p.depth >= roulette_start) {
+                    const float survival =
+                        fminf(0.95f, fmaxf(p.throughput.x, fmaxf(p.throughput.y, p.throughput.z)));
+                    if (g.next1D() >= survival) {
+                        alive = false;
+                    } else {
+                        p.throughput = p.throughput / survival;
+                    }
+                }
+                if (alive) {
+                    p.arrival_origin = sf.p;
+                    p.arrival_pdf = smp.pdf;
+                    p.arrival_specular = smp.specular;
+                    rayLeaving(sf, smp.dir, p.o, p.skip);
+                    p.d = smp.dir;
+                    ++p.depth;
+                }
+            }
         }
-        p.throughput = p.throughput / survival;
     }
-    p.arrival_origin = sf.p;
-    p.arrival_pdf = smp.pdf;
-    p.arrival_specular = smp.specular;
-    rayLeaving(sf, smp.dir, p.o, p.skip);
-    p.d = smp.dir;
-    ++p.depth;
-    return true;
+    const bool lit = nc.valid && !(nc.needs_test && occluded(s, c, nc.origin, nc.dir, nc.range_max, nc.skip));
+    p.result = p.result + throughput_here * (lit ? nc.contribution : gray(0.0f));
+    return alive;
 }
 
 // One iteration of PathEstimator::radiance's loop. Returns false when the path

@@ -98,7 +98,10 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
     const float width = static_cast<float>(args.width);
     const float height = static_cast<float>(args.height);
     PixelSums<ACC> sums;
-    double qr = 0.0, qg = 0.0, qb = 0.0;
+    // Sums of squared samples (for two-sample tests) go straight to memory, one
+    // read-modify-write per sample, only when asked for: no registers carry them
+    // through the traversal calls of an ordinary render.
+    double* const squares = args.sum_squares != nullptr ? args.sum_squares + 3 * slot : nullptr;
     // One bounce per iteration: a lane whose path ends starts the pixel's next
     // sample at once (drawing its jitter next from the same stream, as the
     // reference does), so a warp waits for the longest pixel, not the longest
@@ -113,9 +116,11 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
         }
         const float3 L = path.result;
         sums.add(L);
-        qr += static_cast<double>(L.x) * L.x;
-        qg += static_cast<double>(L.y) * L.y;
-        qb += static_cast<double>(L.z) * L.z;
+        if (squares != nullptr) {
+            squares[0] += static_cast<double>(L.x) * L.x;
+            squares[1] += static_cast<double>(L.y) * L.y;
+            squares[2] += static_cast<double>(L.z) * L.z;
+        }
         if (++sample == total) {
             break;
         }
@@ -127,11 +132,6 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
     a.g += total_sum.y;
     a.b += total_sum.z;
     a.count += static_cast<long long>(n) * n;
-    if (args.sum_squares != nullptr) {
-        args.sum_squares[3 * slot] += qr;
-        args.sum_squares[3 * slot + 1] += qg;
-        args.sum_squares[3 * slot + 2] += qb;
-    }
     if constexpr (COUNT) {
         atomicAdd(totals + 0, counts.boxes);
         atomicAdd(totals + 1, counts.triangles);
