@@ -402,7 +402,7 @@ def render_batch(items, stream: int = 0) -> None:
 
 
 _TUNING_FIELDS = ["tile_width", "blocks_per_sm", "trace_blocks_per_sm", "fetch_batch", "iterations_per_graph",
-                  "slot_count", "inline_traversal", "trace_loop", "evaluations", "best_ms", "default_ms"]
+                  "slot_count", "inline_traversal", "trace_loop", "ray_sort", "evaluations", "best_ms", "default_ms"]
 
 
 def _tuning_dict(t: TuningC) -> dict:
@@ -428,11 +428,11 @@ def autotune_batch(items) -> dict:
 
 def set_tuning(scene: Scene | None = None, **shape) -> None:
     """Pins a launch shape: tile_width, blocks_per_sm and inline_traversal for a scene's megakernel,
-    or (no scene) blocks_per_sm, trace_blocks_per_sm, fetch_batch, trace_loop,
+    or (no scene) blocks_per_sm, trace_blocks_per_sm, fetch_batch, trace_loop, ray_sort,
     iterations_per_graph and slot_count for the wavefront engine."""
     t = TuningC()
     for k, v in shape.items():
-        if k not in _TUNING_FIELDS[:8]:
+        if k not in _TUNING_FIELDS[:9]:
             raise ValueError(f"unknown shape field {k}")
         setattr(t, k, int(v))
     _raise(library().albedo_tuning_set(None if scene is None else scene.handle, byref(t)))

@@ -28,7 +28,7 @@ class TuningC(ctypes.Structure):
     _fields_ = [("tile_width", c_int32), ("blocks_per_sm", c_int32), ("trace_blocks_per_sm", c_int32),
                 ("fetch_batch", c_int32), ("iterations_per_graph", c_int32), ("slot_count", c_int32),
                 ("evaluations", c_int32), ("inline_traversal", c_int32), ("trace_loop", c_int32),
-                ("reserved", c_int32), ("best_ms", c_double), ("default_ms", c_double)]
+                ("ray_sort", c_int32), ("best_ms", c_double), ("default_ms", c_double)]
 
 
 class BatchItemC(ctypes.Structure):

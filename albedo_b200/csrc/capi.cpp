@@ -11,6 +11,7 @@
 #include "wavefront_engine.hpp"
 
 #include <algorithm>
+#include <array>
 #include <deque>
 #include <limits>
 #include <map>
@@ -213,6 +214,8 @@ struct albedo_scene {
     int stack_capacity{0};
     std::vector<DeviceBuffer> buffers;
     DeviceBuffer error_flag;
+    // Ray-binning cells of the scene (coherenceGrid), for the wavefront.
+    std::array<float, 4> grid{};
     // Megakernel launch shape the autotuner kept for this scene (0: default).
     int mega_tile_width{0};
     int mega_blocks_per_sm{0};
@@ -239,6 +242,7 @@ struct albedo_scene {
         }
         host.finalize();
         image = flattenScene(host);
+        grid = coherenceGrid(host);
         stack_capacity = stackCapacityFor(image.stack_need);
         if (stack_capacity == 0) {
             throw Unsupported{std::format("scene hierarchy needs {} traversal stack entries; the device kernels hold 64",
@@ -423,6 +427,9 @@ WfJob wavefrontJob(const albedo_scene& scene, const albedo_render_job& job, Pixe
     j.max_depth = job.max_depth;
     j.roulette_start = job.roulette_start;
     j.seed = job.seed;
+    for (int k{0}; k < 4; ++k) {
+        j.grid[k] = scene.grid[k];
+    }
     return j;
 }
 
@@ -1213,7 +1220,8 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
                                           {"trace_loop", {0, 1}},
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
-                                          {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}}};
+                                          {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}},
+                                          {"ray_sort", {0, 1}}};
         const WfShape kept_shape{engineShape()};
         int kept_slots{0};
         {
@@ -1227,6 +1235,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
             shape.trace_loop = v[2];
             shape.blocks_per_sm = v[3];
             shape.iterations_per_graph = v[4];
+            shape.ray_sort = v[6];
             const std::lock_guard lock{g_engine_mutex};
             if (g_engine && g_engine->slotCount() != v[5]) {
                 g_engine.reset();
@@ -1236,7 +1245,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         };
         const std::vector<int> start{kept_shape.trace_blocks_per_sm > 0 ? kept_shape.trace_blocks_per_sm : 4,
                                      kept_shape.fetch_batch, kept_shape.trace_loop, kept_shape.blocks_per_sm,
-                                     kept_shape.iterations_per_graph, kept_slots};
+                                     kept_shape.iterations_per_graph, kept_slots, kept_shape.ray_sort};
         TuneOutcome outcome;
         try {
             outcome = tuneCoordinateDescent(knobs, start, [&](const std::vector<int>& v) {
@@ -1257,6 +1266,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         out->blocks_per_sm = outcome.best[3];
         out->iterations_per_graph = outcome.best[4];
         out->slot_count = outcome.best[5];
+        out->ray_sort = outcome.best[6];
         fillTuning(out, outcome);
     });
 }
@@ -1288,11 +1298,15 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
         if (shape->trace_loop != 0 && shape->trace_loop != 1) {
             throw std::invalid_argument{"the traversal turn shape must be 0 or 1"};
         }
+        if (shape->ray_sort != 0 && shape->ray_sort != 1) {
+            throw std::invalid_argument{"ray binning must be 0 or 1"};
+        }
         WfShape next{};
         next.blocks_per_sm = shape->blocks_per_sm;
         next.trace_blocks_per_sm = shape->trace_blocks_per_sm;
         next.fetch_batch = shape->fetch_batch;
         next.trace_loop = shape->trace_loop;
+        next.ray_sort = shape->ray_sort;
         next.iterations_per_graph = shape->iterations_per_graph;
         const std::lock_guard lock{g_engine_mutex};
         if (g_engine && g_engine->slotCount() != shape->slot_count) {
@@ -1317,6 +1331,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out)
         out->trace_blocks_per_sm = g_engine_shape.trace_blocks_per_sm;
         out->fetch_batch = g_engine_shape.fetch_batch;
         out->trace_loop = g_engine_shape.trace_loop;
+        out->ray_sort = g_engine_shape.ray_sort;
         out->blocks_per_sm = g_engine_shape.blocks_per_sm;
         out->iterations_per_graph = g_engine_shape.iterations_per_graph;
         out->slot_count = g_engine_slots;

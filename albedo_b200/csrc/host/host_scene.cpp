@@ -4,6 +4,7 @@
 #include "host_scene.hpp"
 
 #include <algorithm>
+#include <cmath>
 #include <format>
 #include <numbers>
 #include <stdexcept>
@@ -393,6 +394,43 @@ CameraFrame buildCameraFrame(const CameraSettings& settings, double aspect_ratio
         throw std::invalid_argument{"field of view and aspect ratio make the film too large"};
     }
     return frame;
+}
+
+} // namespace albedo_b200
+
+namespace albedo_b200 {
+
+std::array<float, 4> coherenceGrid(const HostScene& scene)
+{
+    std::vector<Box3> boxes;
+    std::vector<double> diagonals;
+    for (const ObjectDesc& object : scene.objects) {
+        const Box3 box{scene.objectBounds(object)};
+        const double diagonal{std::sqrt(lengthSquared(box.extent()))};
+        if (!box.isEmpty() && std::isfinite(diagonal)) {
+            boxes.push_back(box);
+            diagonals.push_back(diagonal);
+        }
+    }
+    if (boxes.empty()) {
+        return {0.0f, 0.0f, 0.0f, 0.0f};
+    }
+    std::vector<double> sorted{diagonals};
+    std::nth_element(sorted.begin(), sorted.begin() + static_cast<std::ptrdiff_t>(sorted.size() / 2), sorted.end());
+    const double limit{16 * sorted[sorted.size() / 2]};
+    Box3 core;
+    for (std::size_t i{0}; i < boxes.size(); ++i) {
+        if (diagonals[i] <= limit) {
+            core = merged(core, boxes[i]);
+        }
+    }
+    const Vec3 extent{core.extent()};
+    const double largest{std::max({extent.x, extent.y, extent.z})};
+    if (core.isEmpty() || !(largest > 0) || !std::isfinite(largest)) {
+        return {0.0f, 0.0f, 0.0f, 0.0f};
+    }
+    return {static_cast<float>(core.min.x), static_cast<float>(core.min.y), static_cast<float>(core.min.z),
+            static_cast<float>(8.0 / largest)};
 }
 
 } // namespace albedo_b200

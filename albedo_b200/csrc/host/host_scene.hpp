@@ -148,6 +148,8 @@ public:
     void finalize();
 
     CameraFrame cameraFrame(double aspect_ratio) const;
+    // The world box of one object.
+    Box3 objectBounds(const ObjectDesc& object) const;
 
     std::vector<MaterialDesc> materials;
     std::vector<SphereDesc> spheres;
@@ -160,10 +162,14 @@ public:
     BuiltBvh tlas;
     CameraSettings camera{};
     bool has_camera{false};
-
-private:
-    Box3 objectBounds(const ObjectDesc& object) const;
 };
+
+// A grid of 8 x 8 x 8 cells over the scene's compact core, for binning rays by
+// where they start: {x0, y0, z0, cells per unit length}. The core is the box
+// of the objects whose box diagonal is at most 16 times the median one (room
+// walls and ground spheres of radius 1e4 are left out); cells per unit length
+// is 0 when the core has no finite extent (every ray then falls in one cell).
+std::array<float, 4> coherenceGrid(const HostScene& scene);
 
 // True when the three points form a triangle with a computable area
 // (geometry/triangle.cpp:197-205).

@@ -171,18 +171,133 @@ __global__ void __launch_bounds__(128) regenKernel(const WfJob* __restrict__ job
     }
 }
 
+// Ray binning. Between regeneration and extension the extend queue is
+// reordered so that a traversal warp's rays start in the same region of the
+// scene and point into the same octant, and so visit similar nodes in the same
+// order: a counting sort by a 14-bit key of (job, direction octant, origin cell
+// of an 8 x 8 x 8 grid over the scene's core, in Morton order). Each query's
+// result does not depend on when it is traced, so images are the same with or
+// without binning, and in any order within a bin.
+ALB_DEV unsigned int rayBinKey(const WfJob& job, int job_index, float4 o, float4 d)
+{
+    const auto cell = [&](float v, float lo) {
+        const int c = __float2int_rd((v - lo) * job.grid[3]);
+        return static_cast<unsigned int>(min(max(c, 0), 7));
+    };
+    const unsigned int cx = cell(o.x, job.grid[0]);
+    const unsigned int cy = cell(o.y, job.grid[1]);
+    const unsigned int cz = cell(o.z, job.grid[2]);
+    unsigned int morton = 0u;
+    for (int bit = 2; bit >= 0; --bit) {
+        morton = (morton << 3) | (((cx >> bit) & 1u) << 2) | (((cy >> bit) & 1u) << 1) | ((cz >> bit) & 1u);
+    }
+    const unsigned int octant = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+    return (static_cast<unsigned int>(job_index & 3) << 12) | (octant << 9) | morton;
+}
+
+// Adds `amount` to counter[key] once per group of lanes with the same key and
+// returns the counter's old value plus the lane's rank in its group.
+ALB_DEV unsigned int groupedAdd(unsigned int* counter, unsigned int key)
+{
+    const unsigned int active = __activemask();
+    const unsigned int peers = __match_any_sync(active, key);
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    const int leader = __ffs(peers) - 1;
+    unsigned int base = 0u;
+    if (lane == leader) {
+        base = atomicAdd(counter + key, static_cast<unsigned int>(__popc(peers)));
+    }
+    base = __shfl_sync(active, base, leader);
+    return base + static_cast<unsigned int>(__popc(peers & ((1u << lane) - 1u)));
+}
+
+__global__ void __launch_bounds__(128) binKeysKernel(const WfJob* __restrict__ jobs, WfBuffers b)
+{
+    const WfControl* ctl = b.control;
+    const int in = kQExtend0 + ctl->parity;
+    const int count = ctl->count[in];
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const int s = b.queue[in][i];
+        const int job = b.slots.where[s].x;
+        const unsigned int key = rayBinKey(jobs[job], job, b.slots.ray_o[s], b.slots.ray_d[s]);
+        b.bin_key[i] = key;
+        static_cast<void>(groupedAdd(b.bin_count, key));
+    }
+}
+
+// One block of 1024 threads: exclusive prefix sums of the bin counts into the
+// cursors, and the counts back to zero for the next iteration.
+__global__ void __launch_bounds__(1024) binScanKernel(WfBuffers b)
+{
+    constexpr int kPerThread = kBinCount / 1024;
+    __shared__ unsigned int warp_total[32];
+    const int t = static_cast<int>(threadIdx.x);
+    unsigned int local[kPerThread];
+    unsigned int sum = 0u;
+    for (int k = 0; k < kPerThread; ++k) {
+        local[k] = b.bin_count[t * kPerThread + k];
+        sum += local[k];
+    }
+    // Inclusive scan of the threads' sums: within each warp, then over warps.
+    const int lane = t & 31;
+    const int warp = t >> 5;
+    unsigned int inclusive = sum;
+    for (int offset = 1; offset < 32; offset <<= 1) {
+        const unsigned int up = __shfl_up_sync(0xFFFFFFFFu, inclusive, offset);
+        if (lane >= offset) {
+            inclusive += up;
+        }
+    }
+    if (lane == 31) {
+        warp_total[warp] = inclusive;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        unsigned int w = warp_total[lane];
+        for (int offset = 1; offset < 32; offset <<= 1) {
+            const unsigned int up = __shfl_up_sync(0xFFFFFFFFu, w, offset);
+            if (lane >= offset) {
+                w += up;
+            }
+        }
+        warp_total[lane] = w;
+    }
+    __syncthreads();
+    unsigned int running = inclusive - sum + (warp > 0 ? warp_total[warp - 1] : 0u);
+    for (int k = 0; k < kPerThread; ++k) {
+        b.bin_cursor[t * kPerThread + k] = running;
+        running += local[k];
+        b.bin_count[t * kPerThread + k] = 0u;
+    }
+}
+
+__global__ void __launch_bounds__(128) binScatterKernel(WfBuffers b)
+{
+    const WfControl* ctl = b.control;
+    const int in = kQExtend0 + ctl->parity;
+    const int count = ctl->count[in];
+    const int stride = static_cast<int>(gridDim.x * blockDim.x);
+    for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
+        const unsigned int position = groupedAdd(b.bin_cursor, b.bin_key[i]);
+        b.binned[position] = b.queue[in][i];
+    }
+}
+
 // Closest hit of every ray in the extend queue. The kernel is persistent: a lane
 // whose query ends files the result and takes the next queued ray, so a warp is
 // not held by its slowest ray. Each query runs the same traversal steps, in the
 // same order, as a query traced alone.
 template <int STACK, int LOOP>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJob* __restrict__ jobs, WfBuffers b,
-                                                                        unsigned int* error_flag, int fetch_batch)
+                                                                        unsigned int* error_flag, int fetch_batch,
+                                                                        bool binned)
 {
     extern __shared__ uint2 stack[];
     WfControl* ctl = b.control;
     const int parity = ctl->parity;
     const int in = kQExtend0 + parity;
+    const int* const order = binned ? b.binned : b.queue[in];
     const int ended = kQRegen0 + (parity ^ 1);
     const int count = ctl->count[in];
     const WfSlots& sl = b.slots;
@@ -198,7 +313,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) extendKernel(const WfJ
         const int i = fetch.take(&ctl->fetch_extend, count, !active);
         bool finished = false;
         if (i >= 0) {
-            s = b.queue[in][i];
+            s = order[i];
             scene = &jobs[sl.where[s].x].scene;
             const float4 o = sl.ray_o[s];
             const float4 d = sl.ray_d[s];
@@ -404,6 +519,9 @@ __global__ void resetKernel(WfBuffers b, unsigned long long total_items, int job
     if (i < job_count) {
         b.job_done[i] = 0;
     }
+    if (b.bin_count != nullptr && i < kBinCount) {
+        b.bin_count[i] = 0u;
+    }
     if (i == 0) {
         WfControl* ctl = b.control;
         for (int q = 0; q < kQueueCount; ++q) {
@@ -579,7 +697,8 @@ cudaError_t wfTraceBlocksPerSm(int stack, int* out)
 
 cudaError_t wfReset(const WfBuffers& b, unsigned long long total_items, int job_count, cudaStream_t stream)
 {
-    const int n = b.slot_count > job_count ? b.slot_count : job_count;
+    int n = b.slot_count > job_count ? b.slot_count : job_count;
+    n = n > kBinCount ? n : kBinCount;
     resetKernel<<<(n + 255) / 256, 256, 0, stream>>>(b, total_items, job_count);
     return cudaGetLastError();
 }
@@ -601,12 +720,18 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     const int fetch = launch.fetch_batch > 0 ? launch.fetch_batch : 32;
     const auto smemFor = [](int entries) { return static_cast<std::size_t>(entries) * 128 * sizeof(uint2); };
     regenKernel<<<g, 128, 0, stream>>>(jobs, b);
+    const bool binned = launch.ray_sort != 0 && b.binned != nullptr;
+    if (binned) {
+        binKeysKernel<<<g, 128, 0, stream>>>(jobs, b);
+        binScanKernel<<<1, 1024, 0, stream>>>(b);
+        binScatterKernel<<<g, 128, 0, stream>>>(b);
+    }
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
         if (launch.trace_loop == kLoopOneStep) {
-            extendKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+            extendKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         } else {
-            extendKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+            extendKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         }
         return 0;
     });

@@ -23,7 +23,13 @@ struct WfJob {
     unsigned long long seed;
     long long item_begin;   // first work item (pixel) of this job
     long long item_end;     // one past its last
+    float grid[4];          // ray-binning cells of the scene: x0, y0, z0, cells per unit (coherenceGrid)
 };
+
+// Ray binning before each extend: 2^kBinBits bins of (job, direction octant,
+// origin cell) keys.
+constexpr int kBinBits = 14;
+constexpr int kBinCount = 1 << kBinBits;
 
 // Path slots, one record per field group so a gather of one slot reads whole
 // 16-byte records. A slot owns one pixel for all of that pixel's samples, so its
@@ -83,6 +89,13 @@ struct WfBuffers {
     WfControl* control;
     unsigned long long* job_done; // per job: pixels whose last sample has been accumulated
     int slot_count;
+    // Ray binning (null where an engine has none): per extend-queue entry its
+    // bin key, the queue reordered by bin, bin counts (zero between iterations)
+    // and bin cursors.
+    unsigned int* bin_key;
+    int* binned;
+    unsigned int* bin_count;
+    unsigned int* bin_cursor;
 };
 
 struct WfLaunch {
@@ -92,6 +105,7 @@ struct WfLaunch {
     int trace_blocks; // grid of the persistent traversal kernels (blocks resident at once), or 0 for `blocks`
     int fetch_batch;  // queue entries a traversal warp claims at once (0: 32)
     int trace_loop;   // traversal turn shape of the persistent kernels (TraceLoop)
+    int ray_sort;     // 1: the extend queue is binned by ray coherence before the extend kernel
 };
 
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call

@@ -38,8 +38,10 @@ WavefrontEngine::WavefrontEngine(int slot_count, int job_capacity)
     const std::size_t u2{align256(n * sizeof(ulonglong2))};
     const std::size_t q{align256(n * sizeof(int))};
     const auto jobs{static_cast<std::size_t>(job_capacity)};
+    const std::size_t bins{align256(kBinCount * sizeof(unsigned int))};
     const std::size_t total{12 * f4 + f2 + u2 + kQueueCount * q + align256(sizeof(WfControl)) +
-                            align256(jobs * sizeof(unsigned long long)) + align256(jobs * sizeof(WfJob))};
+                            align256(jobs * sizeof(unsigned long long)) + align256(jobs * sizeof(WfJob)) + 2 * q +
+                            2 * bins};
     cudaCheck(cudaMalloc(&slab_, total), "wavefront slots");
     device_bytes_ = total;
     auto* p{static_cast<char*>(slab_)};
@@ -69,6 +71,10 @@ WavefrontEngine::WavefrontEngine(int slot_count, int job_capacity)
     buffers_.control = static_cast<WfControl*>(take(align256(sizeof(WfControl))));
     buffers_.job_done = static_cast<unsigned long long*>(take(align256(jobs * sizeof(unsigned long long))));
     device_jobs_ = static_cast<WfJob*>(take(align256(jobs * sizeof(WfJob))));
+    buffers_.bin_key = static_cast<unsigned int*>(take(q));
+    buffers_.binned = static_cast<int*>(take(q));
+    buffers_.bin_count = static_cast<unsigned int*>(take(bins));
+    buffers_.bin_cursor = static_cast<unsigned int*>(take(bins));
     buffers_.slot_count = slot_count;
     job_capacity_ = job_capacity;
     cudaCheck(cudaMallocHost(&host_control_, 2 * sizeof(WfControl)), "pinned control");
@@ -113,7 +119,8 @@ WavefrontEngine::~WavefrontEngine()
 void WavefrontEngine::setShape(const WfShape& shape)
 {
     if (shape.blocks_per_sm <= 0 || shape.iterations_per_graph <= 0 || shape.trace_blocks_per_sm < 0 ||
-        shape.fetch_batch <= 0 || shape.trace_loop < 0 || shape.trace_loop > 1) {
+        shape.fetch_batch <= 0 || shape.trace_loop < 0 || shape.trace_loop > 1 || shape.ray_sort < 0 ||
+        shape.ray_sort > 1) {
         throw std::invalid_argument{"wavefront launch shape values must be positive"};
     }
     shape_ = shape;
@@ -142,7 +149,7 @@ void WavefrontEngine::open(int stack, unsigned int* error_flag)
         trace_per_sm = std::min(trace_per_sm, shape_.trace_blocks_per_sm);
     }
     const WfLaunch launch{sm_count_ * shape_.blocks_per_sm, 128, stack, sm_count_ * trace_per_sm, shape_.fetch_batch,
-                          shape_.trace_loop};
+                          shape_.trace_loop, shape_.ray_sort};
     cudaGraph_t graph{nullptr};
     cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture begin");
     cudaError_t captured{cudaSuccess};

@@ -20,11 +20,13 @@ struct WfShape {
     int trace_blocks_per_sm{0};   // persistent traversal kernels: blocks per SM, 0 = as many as fit
     int fetch_batch{32};          // queue entries a traversal warp claims at once
     int trace_loop{0};            // traversal turn shape of the persistent kernels: 0 nodes then leaf, 1 one step
+    int ray_sort{0};              // 1: bin the extend queue by ray coherence before each extend
 };
 
 class WavefrontEngine {
 public:
-    // `slot_count` path slots (about 240 bytes each) and a table of `job_capacity`
+    // `slot_count` path slots (264 bytes each, queues and ray binning included)
+    // and a table of `job_capacity`
     // jobs on the current device.
     WavefrontEngine(int slot_count, int job_capacity);
     ~WavefrontEngine();

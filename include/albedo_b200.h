@@ -333,7 +333,8 @@ typedef struct albedo_tuning {
                                      path estimator), 0 = one out-of-line copy */
     int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
                                      1 = a turn is one node or one leaf (same steps, same results) */
-    int32_t reserved;
+    int32_t ray_sort;             /* wavefront: 1 = the rays of each bounce are binned by job, direction
+                                     octant and origin cell before they are traced (same results) */
     double best_ms;               /* the kept shape's time on the tuning work */
     double default_ms;            /* the default shape's time on the same work */
 } albedo_tuning;
@@ -344,7 +345,8 @@ typedef struct albedo_tuning {
 int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
 /* Tunes the wavefront engine on a batch (coordinate descent over traversal
  * blocks per SM, fetch batch, traversal turn shape, queue-kernel blocks per SM,
- * iterations per graph and slot count) and keeps the result for the process. */
+ * iterations per graph, slot count and ray binning) and keeps the result for
+ * the process. */
 int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_tuning* out);
 /* The shape renders use now: the scene's megakernel shape (scene not NULL) or
  * the process's wavefront shape (scene NULL); timing fields are zero. */
@@ -354,7 +356,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
  * inline_traversal 0 or 1, the latter with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive, and
- * trace_loop 0 or 1). Timing fields are ignored. Images do not depend on the
+ * trace_loop and ray_sort 0 or 1). Timing fields are ignored. Images do not depend on the
  * shape. */
 int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */

@@ -81,3 +81,30 @@ def test_wavefront_rejects_other_estimators(room_path):
     scene = ab.Scene.load(room_path)
     with pytest.raises(ab.Unsupported):
         render(scene, ab.RenderJob(16, 16, estimator=ab.NORMALS, method=ab.WAVEFRONT))
+
+
+def test_ray_binning_leaves_batches_unchanged(room_path, trefoil_path):
+    """Binning each bounce's rays by job, direction octant and origin cell before
+    they are traced (ray_sort) reorders the work, not its results: a batch of
+    jobs on two scenes renders bit for bit the same with and without it."""
+    room = ab.Scene.load(room_path)
+    trefoil = ab.Scene.load(trefoil_path)
+    jobs = [(room, ab.RenderJob(160, 90, samples_per_axis=3, seed=5, max_depth=8)),
+            (trefoil, ab.RenderJob(192, 108, samples_per_axis=2, seed=9, max_depth=10)),
+            (room, ab.RenderJob(64, 48, samples_per_axis=4, seed=1, max_depth=64))]
+    images = []
+    try:
+        for ray_sort in (0, 1):
+            ab.set_tuning(blocks_per_sm=8, trace_blocks_per_sm=4, fetch_batch=32, iterations_per_graph=4,
+                          slot_count=1 << 15, trace_loop=1, ray_sort=ray_sort)
+            assert ab.tuning()["ray_sort"] == ray_sort
+            accs = [torch.zeros((j.width * j.height, 4), dtype=torch.float64, device="cuda") for _, j in jobs]
+            ab.render_batch([(s, j, a.data_ptr()) for (s, j), a in zip(jobs, accs)])
+            torch.cuda.synchronize()
+            room.check()
+            trefoil.check()
+            images.append([a.cpu().numpy() for a in accs])
+    finally:
+        ab.wavefront_configure()
+    for unsorted, binned in zip(*images):
+        np.testing.assert_array_equal(binned.view(np.int64), unsorted.view(np.int64))
