@@ -74,12 +74,16 @@ def build(verbose: bool = False) -> Path:
         objects = list(pool.map(lambda s: _compile(s, headers, log), cpp + cu))
     if _stale(LIBRARY, objects):
         cuda = _cuda_home()
-        cmd = [str(cuda / "bin" / "nvcc")] + ARCH + ["-shared", "-cudart", "static", "-o", str(LIBRARY)] + [
+        # Linked beside the library and renamed over it, so a reader never sees
+        # a partly written file.
+        partial = LIBRARY.with_suffix(".so.partial")
+        cmd = [str(cuda / "bin" / "nvcc")] + ARCH + ["-shared", "-cudart", "static", "-o", str(partial)] + [
             str(o) for o in objects]
         result = subprocess.run(cmd, capture_output=True, text=True)
         log.append(f"$ {' '.join(cmd)}\n{result.stdout}{result.stderr}")
         if result.returncode != 0:
             raise RuntimeError(f"linking failed:\n{result.stdout}{result.stderr}")
+        os.replace(partial, LIBRARY)
     (BUILD / "build.log").write_text("\n".join(log))
     if verbose:
         print("\n".join(log))

@@ -1221,7 +1221,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
                                           {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}},
-                                          {"ray_sort", {0, 1}}};
+                                          {"ray_sort", {0, 1, 2}}};
         const WfShape kept_shape{engineShape()};
         int kept_slots{0};
         {
@@ -1298,8 +1298,8 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
         if (shape->trace_loop != 0 && shape->trace_loop != 1) {
             throw std::invalid_argument{"the traversal turn shape must be 0 or 1"};
         }
-        if (shape->ray_sort != 0 && shape->ray_sort != 1) {
-            throw std::invalid_argument{"ray binning must be 0 or 1"};
+        if (shape->ray_sort < 0 || shape->ray_sort > 2) {
+            throw std::invalid_argument{"ray binning must be 0, 1 or 2"};
         }
         WfShape next{};
         next.blocks_per_sm = shape->blocks_per_sm;

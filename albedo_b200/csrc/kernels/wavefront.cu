@@ -211,16 +211,27 @@ ALB_DEV unsigned int groupedAdd(unsigned int* counter, unsigned int key)
     return base + static_cast<unsigned int>(__popc(peers & ((1u << lane) - 1u)));
 }
 
+// The queue a binning pass reorders: the extend queue of this iteration, or
+// the shadow queue (SHADOW), whose rays are the shadow origins and directions.
+template <bool SHADOW>
+ALB_DEV int binnedQueue(const WfControl* ctl)
+{
+    return SHADOW ? static_cast<int>(kQShadow) : static_cast<int>(kQExtend0) + ctl->parity;
+}
+
+template <bool SHADOW>
 __global__ void __launch_bounds__(128) binKeysKernel(const WfJob* __restrict__ jobs, WfBuffers b)
 {
     const WfControl* ctl = b.control;
-    const int in = kQExtend0 + ctl->parity;
+    const int in = binnedQueue<SHADOW>(ctl);
     const int count = ctl->count[in];
     const int stride = static_cast<int>(gridDim.x * blockDim.x);
     for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
         const int s = b.queue[in][i];
         const int job = b.slots.where[s].x;
-        const unsigned int key = rayBinKey(jobs[job], job, b.slots.ray_o[s], b.slots.ray_d[s]);
+        const float4 o = SHADOW ? b.slots.shadow_o[s] : b.slots.ray_o[s];
+        const float4 d = SHADOW ? b.slots.shadow_d[s] : b.slots.ray_d[s];
+        const unsigned int key = rayBinKey(jobs[job], job, o, d);
         b.bin_key[i] = key;
         static_cast<void>(groupedAdd(b.bin_count, key));
     }
@@ -272,10 +283,11 @@ __global__ void __launch_bounds__(1024) binScanKernel(WfBuffers b)
     }
 }
 
+template <bool SHADOW>
 __global__ void __launch_bounds__(128) binScatterKernel(WfBuffers b)
 {
     const WfControl* ctl = b.control;
-    const int in = kQExtend0 + ctl->parity;
+    const int in = binnedQueue<SHADOW>(ctl);
     const int count = ctl->count[in];
     const int stride = static_cast<int>(gridDim.x * blockDim.x);
     for (int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x); i < count; i += stride) {
@@ -446,11 +458,13 @@ __global__ void __launch_bounds__(128) shadeKernel(const WfJob* __restrict__ job
 // their path. Persistent, like extendKernel.
 template <int STACK, int LOOP>
 __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJob* __restrict__ jobs, WfBuffers b,
-                                                                        unsigned int* error_flag, int fetch_batch)
+                                                                        unsigned int* error_flag, int fetch_batch,
+                                                                        bool binned)
 {
     extern __shared__ uint2 stack[];
     WfControl* ctl = b.control;
     const int count = ctl->count[kQShadow];
+    const int* const order = binned ? b.binned : b.queue[kQShadow];
     const WfSlots& sl = b.slots;
     uint2* const lane_stack = stack + threadIdx.x;
     const int stride = static_cast<int>(blockDim.x);
@@ -464,7 +478,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) shadowKernel(const WfJ
         const int i = fetch.take(&ctl->fetch_shadow, count, !active);
         bool finished = false;
         if (i >= 0) {
-            s = b.queue[kQShadow][i];
+            s = order[i];
             scene = &jobs[sl.where[s].x].scene;
             const float4 o = sl.shadow_o[s];
             const float4 d = sl.shadow_d[s];
@@ -722,9 +736,9 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
     regenKernel<<<g, 128, 0, stream>>>(jobs, b);
     const bool binned = launch.ray_sort != 0 && b.binned != nullptr;
     if (binned) {
-        binKeysKernel<<<g, 128, 0, stream>>>(jobs, b);
+        binKeysKernel<false><<<g, 128, 0, stream>>>(jobs, b);
         binScanKernel<<<1, 1024, 0, stream>>>(b);
-        binScatterKernel<<<g, 128, 0, stream>>>(b);
+        binScatterKernel<false><<<g, 128, 0, stream>>>(b);
     }
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
@@ -762,12 +776,22 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         shadeKernel<kClassDielectric><<<g, 128, 0, stream>>>(jobs, b);
         shadeKernel<kClassMix><<<g, 128, 0, stream>>>(jobs, b);
     }
+    // The shadow rays too, when binning is 2. The binned buffer is free again:
+    // the extend kernel has read it.
+    const bool binned_shadows = launch.ray_sort == 2 && b.binned != nullptr;
+    if (binned_shadows) {
+        binKeysKernel<true><<<g, 128, 0, stream>>>(jobs, b);
+        binScanKernel<<<1, 1024, 0, stream>>>(b);
+        binScatterKernel<true><<<g, 128, 0, stream>>>(b);
+    }
     withStack(launch.stack, [&](auto size) {
         constexpr int S = decltype(size)::value;
         if (launch.trace_loop == kLoopOneStep) {
-            shadowKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+            shadowKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
+                                                                           binned_shadows);
         } else {
-            shadowKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch);
+            shadowKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
+                                                                                 binned_shadows);
         }
         return 0;
     });

@@ -105,7 +105,8 @@ struct WfLaunch {
     int trace_blocks; // grid of the persistent traversal kernels (blocks resident at once), or 0 for `blocks`
     int fetch_batch;  // queue entries a traversal warp claims at once (0: 32)
     int trace_loop;   // traversal turn shape of the persistent kernels (TraceLoop)
-    int ray_sort;     // 1: the extend queue is binned by ray coherence before the extend kernel
+    int ray_sort;     // 1: the extend queue is binned by ray coherence before the extend kernel; 2: the shadow
+                      // queue too
 };
 
 // Opts the traversal kernels into `stack` entries of dynamic shared memory; call

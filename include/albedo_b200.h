@@ -334,7 +334,8 @@ typedef struct albedo_tuning {
     int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
                                      1 = a turn is one node or one leaf (same steps, same results) */
     int32_t ray_sort;             /* wavefront: 1 = the rays of each bounce are binned by job, direction
-                                     octant and origin cell before they are traced (same results) */
+                                     octant and origin cell before they are traced, 2 = the shadow rays
+                                     too (same results) */
     double best_ms;               /* the kept shape's time on the tuning work */
     double default_ms;            /* the default shape's time on the same work */
 } albedo_tuning;
@@ -356,7 +357,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
  * inline_traversal 0 or 1, the latter with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive, and
- * trace_loop and ray_sort 0 or 1). Timing fields are ignored. Images do not depend on the
+ * trace_loop 0 or 1, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the
  * shape. */
 int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */

@@ -85,8 +85,9 @@ def test_wavefront_rejects_other_estimators(room_path):
 
 def test_ray_binning_leaves_batches_unchanged(room_path, trefoil_path):
     """Binning each bounce's rays by job, direction octant and origin cell before
-    they are traced (ray_sort) reorders the work, not its results: a batch of
-    jobs on two scenes renders bit for bit the same with and without it."""
+    they are traced (ray_sort 1; 2 bins the shadow rays too) reorders the work,
+    not its results: a batch of jobs on two scenes renders bit for bit the same
+    with and without it."""
     room = ab.Scene.load(room_path)
     trefoil = ab.Scene.load(trefoil_path)
     jobs = [(room, ab.RenderJob(160, 90, samples_per_axis=3, seed=5, max_depth=8)),
@@ -94,7 +95,7 @@ def test_ray_binning_leaves_batches_unchanged(room_path, trefoil_path):
             (room, ab.RenderJob(64, 48, samples_per_axis=4, seed=1, max_depth=64))]
     images = []
     try:
-        for ray_sort in (0, 1):
+        for ray_sort in (0, 1, 2):
             ab.set_tuning(blocks_per_sm=8, trace_blocks_per_sm=4, fetch_batch=32, iterations_per_graph=4,
                           slot_count=1 << 15, trace_loop=1, ray_sort=ray_sort)
             assert ab.tuning()["ray_sort"] == ray_sort
@@ -106,5 +107,6 @@ def test_ray_binning_leaves_batches_unchanged(room_path, trefoil_path):
             images.append([a.cpu().numpy() for a in accs])
     finally:
         ab.wavefront_configure()
-    for unsorted, binned in zip(*images):
-        np.testing.assert_array_equal(binned.view(np.int64), unsorted.view(np.int64))
+    for variant in images[1:]:
+        for unsorted, binned in zip(images[0], variant):
+            np.testing.assert_array_equal(binned.view(np.int64), unsorted.view(np.int64))
