@@ -219,7 +219,7 @@ struct albedo_scene {
     // Megakernel launch shape the autotuner kept for this scene (0: default).
     int mega_tile_width{0};
     int mega_blocks_per_sm{0};
-    bool mega_inline{false};
+    int mega_inline{0}; // 0 out-of-line traversal, 1 both queries inlined, 2 the closest-hit query inlined
 
     void requireOpen() const
     {
@@ -355,7 +355,7 @@ RenderArgs renderArgsFor(const albedo_scene& scene, const albedo_render_job& job
     args.accumulation = job.accumulation;
     // The inlined-traversal kernel exists for the path estimator; the other
     // estimators keep the out-of-line traversal (images do not depend on it).
-    args.inline_traversal = scene.mega_inline && job.estimator == ALBEDO_PATH ? 1 : 0;
+    args.inline_traversal = job.estimator == ALBEDO_PATH ? scene.mega_inline : 0;
     return args;
 }
 
@@ -1155,18 +1155,20 @@ int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job
         DeviceBuffer scratch{pixels * sizeof(PixelAccum)};
         TuneTimer timer;
         // Kernel variants: 0 = 3 blocks/SM, 1 = 4 blocks/SM (both with the
-        // out-of-line traversal), 2 = 3 blocks/SM with the traversal inlined
-        // (path estimator only).
+        // out-of-line traversal), 2 = 3 blocks/SM with both queries' traversal
+        // inlined, 3 = 3 blocks/SM with the closest-hit traversal inlined and
+        // the shadow query out of line (path estimator only).
         const bool can_inline{probe.estimator == ALBEDO_PATH};
-        const std::vector<TuneKnob> knobs{{"tile_width", {8, 16, 32}},
-                                          {"variant", can_inline ? std::vector<int>{0, 1, 2} : std::vector<int>{0, 1}}};
+        const std::vector<TuneKnob> knobs{
+            {"tile_width", {8, 16, 32}},
+            {"variant", can_inline ? std::vector<int>{0, 1, 2, 3} : std::vector<int>{0, 1}}};
         const int kept_tile{scene->mega_tile_width};
         const int kept_blocks{scene->mega_blocks_per_sm};
-        const bool kept_inline{scene->mega_inline};
+        const int kept_inline{scene->mega_inline};
         const auto apply = [&](const std::vector<int>& v) {
             scene->mega_tile_width = v[0];
             scene->mega_blocks_per_sm = v[1] == 1 ? 4 : 3;
-            scene->mega_inline = v[1] == 2;
+            scene->mega_inline = v[1] == 2 ? 1 : (v[1] == 3 ? 2 : 0);
         };
         TuneOutcome outcome;
         try {
@@ -1185,7 +1187,7 @@ int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job
         scene->collectKernelError();
         out->tile_width = scene->mega_tile_width;
         out->blocks_per_sm = scene->mega_blocks_per_sm;
-        out->inline_traversal = scene->mega_inline ? 1 : 0;
+        out->inline_traversal = scene->mega_inline;
         fillTuning(out, outcome);
     });
 }
@@ -1283,12 +1285,13 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
                 throw std::invalid_argument{std::format("megakernel blocks per SM must be 3 or 4, got {}",
                                                         shape->blocks_per_sm)};
             }
-            if (shape->inline_traversal != 0 && (shape->inline_traversal != 1 || shape->blocks_per_sm != 3)) {
-                throw std::invalid_argument{"the inlined-traversal megakernel runs at 3 blocks per SM"};
+            if (shape->inline_traversal != 0 &&
+                (shape->inline_traversal < 0 || shape->inline_traversal > 2 || shape->blocks_per_sm != 3)) {
+                throw std::invalid_argument{"the inlined-traversal megakernels (1 or 2) run at 3 blocks per SM"};
             }
             scene->mega_tile_width = shape->tile_width;
             scene->mega_blocks_per_sm = shape->blocks_per_sm;
-            scene->mega_inline = shape->inline_traversal == 1;
+            scene->mega_inline = shape->inline_traversal;
             return;
         }
         if (shape->blocks_per_sm <= 0 || shape->trace_blocks_per_sm <= 0 || shape->fetch_batch <= 0 ||
@@ -1324,7 +1327,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out)
         if (scene != nullptr) {
             out->tile_width = scene->mega_tile_width > 0 ? scene->mega_tile_width : 16;
             out->blocks_per_sm = scene->mega_blocks_per_sm > 0 ? scene->mega_blocks_per_sm : 3;
-            out->inline_traversal = scene->mega_inline ? 1 : 0;
+            out->inline_traversal = scene->mega_inline;
             return;
         }
         const std::lock_guard lock{g_engine_mutex};

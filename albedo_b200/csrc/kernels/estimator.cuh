@@ -16,11 +16,13 @@
 namespace albedo_b200 {
 
 // Where a thread's queries keep their stack, and how they are traced: INLINE
-// places the traversal in the calling kernel, COUNT counts its work into
+// places the closest-hit traversal in the calling kernel, INLINE_SHADOW the
+// shadow queries' traversal (by default as INLINE), COUNT counts the work into
 // `counts` (traceScene).
-template <bool INLINE, bool COUNT = false>
+template <bool INLINE, bool COUNT = false, bool INLINE_SHADOW = INLINE>
 struct TraceContext {
     static constexpr bool kInline = INLINE;
+    static constexpr bool kInlineShadow = INLINE_SHADOW;
     static constexpr bool kCount = COUNT;
     uint2* stack;
     int stride;
@@ -41,8 +43,8 @@ template <typename Ctx>
 ALB_DEV bool occluded(const DevScene& s, const Ctx& c, float3 o, float3 d, float tmax, const SkipRule& skip)
 {
     TraceHit hit;
-    return traceScene<true, Ctx::kInline, Ctx::kCount>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride,
-                                                       c.capacity, c.error_flag, c.counts);
+    return traceScene<true, Ctx::kInlineShadow, Ctx::kCount>(s, o, d, 0.0f, tmax, skip, hit, c.stack, c.stride,
+                                                             c.capacity, c.error_flag, c.counts);
 }
 
 // Next-event estimation from one uniformly chosen light, MIS-weighted, before

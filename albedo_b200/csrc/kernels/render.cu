@@ -62,8 +62,12 @@ struct PixelSums<kAccumulateKahan> {
     }
 };
 
+// INL: 0 = both queries call the shared out-of-line traversal, 1 = both are
+// inlined, 2 = the closest-hit query is inlined and the shadow query calls the
+// out-of-line copy (a smaller kernel than 1, no register saves around the
+// per-bounce call).
 template <int STACK, int EST, bool COUNT = false, int MINB = kMegaBlocksPerSm, int ACC = kAccumulateFp64,
-          bool INL = false>
+          int INL = 0>
 __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene, const DevCamera camera,
                                                           const RenderArgs args, PixelAccum* accum,
                                                           unsigned int* error_flag,
@@ -71,7 +75,8 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
 {
     extern __shared__ uint2 stack[];
     TraversalCounts counts{0, 0, 0, 0, 0, 0};
-    const TraceContext<INL, COUNT> ctx{stack + threadIdx.x, kBlock, STACK, error_flag, COUNT ? &counts : nullptr};
+    const TraceContext<INL != 0, COUNT, INL == 1> ctx{stack + threadIdx.x, kBlock, STACK, error_flag,
+                                                      COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
         slot = blockIdx.x * kBlock + threadIdx.x;
@@ -299,9 +304,15 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                                     accum, error_flag, no_totals);
         default:
             if (args.accumulation == kAccumulateKahan) {
-                if (args.inline_traversal != 0) {
+                if (args.inline_traversal == 1) {
                     return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan,
-                                                       true>,
+                                                       1>,
+                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
+                                            no_totals);
+                }
+                if (args.inline_traversal == 2) {
+                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan,
+                                                       2>,
                                             megaBlocks(args), stream, scene, camera, args, accum, error_flag,
                                             no_totals);
                 }
@@ -313,8 +324,12 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                 return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan>,
                                         megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
             }
-            if (args.inline_traversal != 0) {
-                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, true>,
+            if (args.inline_traversal == 1) {
+                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, 1>,
+                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
+            }
+            if (args.inline_traversal == 2) {
+                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, 2>,
                                         megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
             }
             if (args.blocks_per_sm == 4) {

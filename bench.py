@@ -724,7 +724,7 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
     tiles = {}
     for shape in mega_shapes:
         key = (f"{shape['tile_width']}x{128 // shape['tile_width']}/{shape['blocks_per_sm']}"
-               + ("/inline" if shape["inline_traversal"] else ""))
+               + {0: "", 1: "/inline", 2: "/inline-closest"}[shape["inline_traversal"]])
         tiles[key] = tiles.get(key, 0) + 1
     wave = {"mpaths_per_s": paths / batch_s / 1e6, "mrays_per_s": rays / batch_s / 1e6,
             "ms_per_step": batch_s * 1e3, "rays_per_step": rays,

@@ -329,8 +329,10 @@ typedef struct albedo_tuning {
     int32_t iterations_per_graph; /* wavefront: iterations per captured CUDA graph */
     int32_t slot_count;           /* wavefront: path slots */
     int32_t evaluations;          /* shapes timed */
-    int32_t inline_traversal;     /* megakernel: 1 = traversal inlined into the kernel (3 blocks per SM;
-                                     path estimator), 0 = one out-of-line copy */
+    int32_t inline_traversal;     /* megakernel: 0 = one out-of-line traversal copy serves both queries,
+                                     1 = both queries' traversal inlined into the kernel, 2 = the
+                                     closest-hit query's inlined and the shadow query's out of line
+                                     (1 and 2: 3 blocks per SM, path estimator) */
     int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
                                      1 = a turn is one node or one leaf (same steps, same results) */
     int32_t ray_sort;             /* wavefront: 1 = the rays of each bounce are binned by job, direction
@@ -341,8 +343,9 @@ typedef struct albedo_tuning {
 } albedo_tuning;
 /* Tunes the megakernel for `scene` on `job` and keeps the result in the scene:
  * every tile width with every kernel variant (3 or 4 blocks per SM with an
- * out-of-line traversal, or 3 with the traversal inlined, which is faster on
- * some scenes and slower on others). */
+ * out-of-line traversal; or 3 with the traversal inlined for both queries, or
+ * for the closest-hit query only, which are faster on some scenes and slower
+ * on others). */
 int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
 /* Tunes the wavefront engine on a batch (coordinate descent over traversal
  * blocks per SM, fetch batch, traversal turn shape, queue-kernel blocks per SM,
@@ -354,7 +357,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
 int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
 /* Pins a shape, as the autotuner would keep it: the scene's megakernel shape
  * (scene not NULL: tile_width 8, 16 or 32, blocks_per_sm 3 or 4, and
- * inline_traversal 0 or 1, the latter with 3 blocks per SM) or the
+ * inline_traversal 0, 1 or 2, the last two with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive, and
  * trace_loop 0 or 1, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the

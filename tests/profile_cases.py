@@ -26,9 +26,9 @@ from pathlib import Path
 
 sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
 
-# Megakernel launches one tuning pass makes: every shape (3 tile widths x 3
+# Megakernel launches one tuning pass makes: every shape (3 tile widths x 4
 # kernel variants) once untimed and twice timed.
-MEGAKERNEL_TUNING_LAUNCHES = 9 * 3
+MEGAKERNEL_TUNING_LAUNCHES = 12 * 3
 
 
 def main() -> None:

@@ -332,12 +332,13 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
     # fuse multiply-adds differently there, so it agrees within the tolerance
     # used between kernel variants (sample counts identical, image sum within
     # 1e-4, at most 0.5% of pixels beyond 1e-3 relative), not bit for bit.
-    ab.set_tuning(scene, tile_width=16, blocks_per_sm=3, inline_traversal=1)
-    inlined = render(scene, job)
-    np.testing.assert_array_equal(inlined[:, 3], base[:, 3])
-    assert abs(inlined[:, :3].sum() - base[:, :3].sum()) / base[:, :3].sum() < 1e-4
-    rel = np.abs(inlined[:, :3] - base[:, :3]) / np.maximum(np.abs(base[:, :3]), 1e-3)
-    assert np.mean(rel.max(axis=1) > 1e-3) < 0.005
+    for mode in (1, 2):
+        ab.set_tuning(scene, tile_width=16, blocks_per_sm=3, inline_traversal=mode)
+        inlined = render(scene, job)
+        np.testing.assert_array_equal(inlined[:, 3], base[:, 3])
+        assert abs(inlined[:, :3].sum() - base[:, :3].sum()) / base[:, :3].sum() < 1e-4
+        rel = np.abs(inlined[:, :3] - base[:, :3]) / np.maximum(np.abs(base[:, :3]), 1e-3)
+        assert np.mean(rel.max(axis=1) > 1e-3) < 0.005
     ab.set_tuning(scene, tile_width=16, blocks_per_sm=3, inline_traversal=0)
     wave_job = ab.RenderJob(160, 90, samples_per_axis=3, seed=4, max_depth=10, method=ab.WAVEFRONT)
     wave = render(scene, wave_job)
