@@ -112,3 +112,25 @@ def test_flattened_meshes_give_the_reference_object_ids():
     np.testing.assert_array_equal(mine["object"][hit], their["object"][hit])
     np.testing.assert_array_equal(mine["t"][hit], their["t"][hit])
     np.testing.assert_array_equal(mine["point"][hit], their["point"][hit])
+
+
+@pytest.mark.parametrize("which", ["room", "trefoil"])
+def test_near_tie_classifier_flags_planted_mistakes(which, room_path, trefoil_path):
+    """The FP64 restatement's near-tie classifier (oracle_classify), which the GPU
+    ray-id tests rely on: the restatement's own answers are all class 0; answers
+    with a wrong object or a wrong miss planted in them are class 2 (unexplained)."""
+    scene = ab.Scene.read(room_path if which == "room" else trefoil_path)
+    rays = random_rays(20_000, 41, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
+    mine = restatement.intersect(scene, rays)
+    exact = restatement.classify(scene, rays, mine)["class"]
+    assert np.all(exact == 0)
+    planted = np.flatnonzero(mine["hit"])[:50]
+    wrong_object = {k: mine[k].copy() for k in ("hit", "object", "triangle")}
+    wrong_object["object"][planted] = (wrong_object["object"][planted] + 1) % scene.info()["objects"]
+    wrong_object["triangle"][planted] = -1
+    klass = restatement.classify(scene, rays, wrong_object)["class"]
+    assert np.all(klass[planted] == 2) and np.count_nonzero(klass) == len(planted)
+    wrong_miss = {k: mine[k].copy() for k in ("hit", "object", "triangle")}
+    wrong_miss["hit"][planted] = 0
+    klass = restatement.classify(scene, rays, wrong_miss)["class"]
+    assert np.all(klass[planted] == 2) and np.count_nonzero(klass) == len(planted)
