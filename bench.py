@@ -716,6 +716,24 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
         batch_ms = timed(batched)
         rays = ab.wavefront_last_rays()
         mega_ms = timed(one_at_a_time)
+    iterations = ab.wavefront_last_iterations()
+    # The fixed cost of one iteration (its graph's launches, the queue kernels on
+    # nearly empty queues, the host's completion polling): a 4 x 4-pixel job at
+    # 1 spp, whose iterations do almost no work, timed per iteration. Times the
+    # batch's iteration count, it bounds what one persistent launch for the whole
+    # batch could save.
+    tiny_acc = torch.zeros((16, 4), dtype=torch.float64, device="cuda")
+    tiny = [(loaded[jobs[0].scene], ab.RenderJob(4, 4, samples_per_axis=1, max_depth=8, method=ab.WAVEFRONT),
+             tiny_acc.data_ptr())]
+    ab.render_batch(tiny)
+    torch.cuda.synchronize()
+    tiny_ms = []
+    for _ in range(5):
+        start = time.perf_counter()
+        ab.render_batch(tiny)
+        torch.cuda.synchronize()
+        tiny_ms.append((time.perf_counter() - start) * 1e3 / max(ab.wavefront_last_iterations(), 1))
+    per_iteration_ms = statistics.median(tiny_ms)
     for s in loaded.values():
         s.check()
     batch_s = statistics.mean(batch_ms) / 1e3
@@ -729,7 +747,8 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
     wave = {"mpaths_per_s": paths / batch_s / 1e6, "mrays_per_s": rays / batch_s / 1e6,
             "ms_per_step": batch_s * 1e3, "rays_per_step": rays,
             "traversal_gbs": alg_bytes / batch_s / 1e9, "traversal_frac_of_hbm": alg_bytes / batch_s / 1e9 / peak,
-            "iterations": ab.wavefront_last_iterations()}
+            "iterations": iterations, "empty_iteration_ms": per_iteration_ms,
+            "fixed_cost_share": per_iteration_ms * iterations / (batch_s * 1e3)}
     if l2 is not None:
         wave["traversal_frac_of_l2"] = alg_bytes / batch_s / 1e9 / l2["gbs"]
     return {
