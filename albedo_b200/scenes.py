@@ -384,8 +384,8 @@ def flattened_parts(seed: int = 29) -> list[tuple]:
     (Scene::add(const TriangleMesh&, ...), scene/scene.cpp:33-61), between
     spheres, in this add order: a trefoil tube placed by a seeded rotation and
     scale, a sphere, a displaced level-5 icosphere (20,480 triangles), two
-    spheres. Positions are rounded to FP32 so both renderers hold the same
-    vertices. Parts are ("triangles", positions, faces) or ("sphere", centre,
+    spheres. Positions, centres and radii are FP32 values, so both renderers
+    hold the same geometry. Parts are ("triangles", positions, faces) or ("sphere", centre,
     radius)."""
     rng = Pcg32(seed)
     points, quads = trefoil_mesh(128, 16)
@@ -397,7 +397,7 @@ def flattened_parts(seed: int = 29) -> list[tuple]:
     ball_points, ball_faces = displaced_icosphere(5, seed)
     ball = ball_points.astype(np.float64) * 0.9 + np.array([1.1, 1.0, 0.2])
     return [("triangles", knot.astype(np.float32).astype(np.float64), faces),
-            ("sphere", (0.0, 0.4, 1.4), 0.4),
+            ("sphere", (0.0, 0.375, 1.375), 0.375),
             ("triangles", ball.astype(np.float32).astype(np.float64), ball_faces),
-            ("sphere", (-1.6, 0.5, 1.2), 0.5),
+            ("sphere", (-1.625, 0.5, 1.25), 0.5),
             ("sphere", (0.0, -1000.0, 0.0), 1000.0)]

@@ -25,8 +25,8 @@ launch's measured time, against the measured HBM copy peak and, beside it, the
 L2 read peak measured in the same run by a read sweep of this library.
 `cpu_baseline` is the reference renderer, built from its own sources, timed on
 this machine's host cores rendering the same frame through its own renderImage
-at 1 sample per pixel. `precision` holds every form's error on this frame
-against the FP64 oracle (the reference at 65,536 spp on 256 seeded pixels).
+at 36 samples per pixel. `precision` holds every form's error on this frame
+against the FP64 oracle (the reference at 65,536 spp on 2,048 seeded pixels).
 
 `forms` (1 GPU, unless --no-forms) adds the other configurations: the 1M-triangle
 random soup at the same frame; the instanced trefoil frame (960x540, 64 spp),
@@ -79,9 +79,12 @@ class Frame:
 LARGE = Frame("icosphere_8_levels_1310720_tris_rough_glass_1920x1080_256spp_depth16", 1920, 1080, 16, 16)
 SOUP = Frame("soup_1000000_tris_1920x1080_256spp_depth16", 1920, 1080, 16, 16)
 TREFOIL = Frame("trefoil_x3_instanced_960x540_64spp_depth10", 960, 540, 8, 10)
-# The reference renders the large frame at 1 x 1 samples per pixel per step: a
-# bounded sample (Mpaths/s barely depends on spp) of its own renderImage call.
-REFERENCE_SAMPLES_PER_AXIS = 1
+# The reference renders the large frame at 4 x 4 samples per pixel per step of
+# the reference arm (about 4 s on 16 host threads) and at 6 x 6 for the CPU
+# baseline in our line (about 10 s): bounded samples of its own renderImage
+# call on the same frame (a path's cost does not depend on the pixel's spp).
+REFERENCE_SAMPLES_PER_AXIS = 4
+BASELINE_SAMPLES_PER_AXIS = 6
 
 
 def parse_args():
@@ -290,7 +293,7 @@ def reference_frame_sample(scene_path: Path, frame: Frame, samples_per_axis: int
 def run_reference(args, rank: int) -> None:
     """The reference arm: the reference renderer built from its own sources,
     rendering the headline frame through renderImage on the host's cores; each
-    step is the full frame at 1 spp."""
+    step is the full frame at 16 spp."""
     if rank != 0:
         return
     from albedo_b200 import scenes
@@ -320,12 +323,14 @@ def run_reference(args, rank: int) -> None:
 # ------------------------------------------------------------------ forms
 
 
-def precision_errors(scene_path: Path, frame: Frame, images: dict, pixel_count: int = 256) -> dict:
+def precision_errors(scene_path: Path, frame: Frame, images: dict, pixel_count: int = 2048) -> dict:
     """Every image's error against the FP64 oracle (the reference renderer at
     65,536 spp, accumulated in FP64, on `pixel_count` seeded pixels, host cores)
     next to the reference renderer's own error at the frame's spp on the same
     pixels: relative RMSE and mean relative error over pixels whose oracle
-    luminance exceeds 1e-3."""
+    luminance exceeds 1e-3, and the paired statistic of each image's per-pixel
+    squared errors against the reference's (mean difference over its standard
+    error: |t| < 4 is matched RMSE)."""
     from oracle import reference as ref
 
     rng = np.random.default_rng(91)
@@ -343,13 +348,22 @@ def precision_errors(scene_path: Path, frame: Frame, images: dict, pixel_count: 
     lum = oracle.mean(axis=1)
     keep = lum > 1e-3
 
+    def squared(rgb):
+        return np.sum(((rgb - oracle)[keep] / lum[keep, None]) ** 2, axis=1)
+
     def errors(rgb):
         err = (rgb - oracle)[keep] / lum[keep, None]
         return {"rel_rmse": float(np.sqrt(np.mean(err ** 2))), "mean_rel": float(np.mean(np.abs(err)))}
 
+    theirs = theirs_sum / spp
     index = pixels[:, 1] * frame.width + pixels[:, 0]
-    out = {label: errors(img[index, :3] / spp) for label, img in images.items()}
-    out["reference_cpu_equal_spp"] = errors(theirs_sum / spp)
+    out = {}
+    for label, img in images.items():
+        ours = img[index, :3] / spp
+        d = squared(ours) - squared(theirs)
+        se = d.std(ddof=1) / np.sqrt(len(d))
+        out[label] = {**errors(ours), "paired_t_vs_reference": float(d.mean() / se) if se > 0 else 0.0}
+    out["reference_cpu_equal_spp"] = errors(theirs)
     out["oracle"] = {"pixels": pixel_count, "spp": 65536, "seconds": oracle_s, "pixels_lit": int(keep.sum())}
     return out
 
@@ -417,7 +431,7 @@ def soup_form(tmp: Path, flush) -> dict:
         out[label] = {"mpaths_per_s": SOUP.paths / (ms[0] / 1e3) / 1e6, "ms_per_frame": ms[0]}
         images[label] = acc.cpu().numpy()
     scene.check()
-    out["error_vs_fp64_oracle"] = precision_errors(path, SOUP, images)
+    out["error_vs_fp64_oracle"] = precision_errors(path, SOUP, images, pixel_count=512)
     scene.close()
     return out
 
@@ -717,6 +731,16 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
         rays = ab.wavefront_last_rays()
         mega_ms = timed(one_at_a_time)
     iterations = ab.wavefront_last_iterations()
+    # The tuned shape with each ray-binning setting (0 none, 1 the extension rays,
+    # 2 the shadow rays too), one timed batch each.
+    ray_sort_ms = {}
+    for ray_sort in (0, 1, 2):
+        ab.set_tuning(**{k: wave_shape[k] for k in ("blocks_per_sm", "trace_blocks_per_sm", "fetch_batch",
+                                                     "iterations_per_graph", "slot_count", "trace_loop")},
+                      ray_sort=ray_sort)
+        ray_sort_ms[ray_sort] = statistics.mean(timed(batched)) if steps > 0 else None
+    ab.set_tuning(**{k: wave_shape[k] for k in ("blocks_per_sm", "trace_blocks_per_sm", "fetch_batch",
+                                                 "iterations_per_graph", "slot_count", "trace_loop", "ray_sort")})
     # The fixed cost of one iteration (its graph's launches, the queue kernels on
     # nearly empty queues, the host's completion polling): a 4 x 4-pixel job at
     # 1 spp, whose iterations do almost no work, timed per iteration. Times the
@@ -748,7 +772,8 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
             "ms_per_step": batch_s * 1e3, "rays_per_step": rays,
             "traversal_gbs": alg_bytes / batch_s / 1e9, "traversal_frac_of_hbm": alg_bytes / batch_s / 1e9 / peak,
             "iterations": iterations, "empty_iteration_ms": per_iteration_ms,
-            "fixed_cost_share": per_iteration_ms * iterations / (batch_s * 1e3)}
+            "fixed_cost_share": per_iteration_ms * iterations / (batch_s * 1e3),
+            "ray_sort_ms": {str(k): v for k, v in ray_sort_ms.items()}}
     if l2 is not None:
         wave["traversal_frac_of_l2"] = alg_bytes / batch_s / 1e9 / l2["gbs"]
     return {
@@ -916,7 +941,7 @@ def main():
             "autotune": tuned,
         }
         if world == 1:
-            line["cpu_baseline"] = reference_frame_sample(scene_path, frame)
+            line["cpu_baseline"] = reference_frame_sample(scene_path, frame, BASELINE_SAMPLES_PER_AXIS)
             if not args.no_forms and method == ab.MEGAKERNEL:
                 accum.zero_()
                 ab.render_device(scene, job, accum.data_ptr())

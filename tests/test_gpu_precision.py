@@ -17,8 +17,10 @@ megakernel (both accumulation modes) and the wavefront:
                  test; the oracle's own noise enters both sides alike, and rough
                  glass gives heavy-tailed per-pixel errors, which make a ratio of
                  two RMSEs over a few hundred pixels unstable)
-  bias           at 4,096 spp the mean relative error against the oracle is
-                 below 1%, and |z| > 4 on at most 1% of pixel channels
+  bias           at 4,096 spp the mean of the image over the pixels is within
+                 1% of the oracle's (both carry noise: the per-pixel mean
+                 absolute error, about 1.5% at this spp, measures noise, not
+                 bias), and |z| > 4 on at most 1% of pixel channels
 and the two accumulation modes agree within 1e-6 relative on every lit pixel.
 """
 
@@ -119,8 +121,8 @@ def test_megakernel_against_the_fp64_oracle(which, precision_scenes, oracles):
         t = paired_t(ours, theirs, oracle)
         assert abs(t) < 4, (mode, t, rel_rmse(ours, oracle), rel_rmse(theirs, oracle))
         mean, var = megakernel_means(scene, ORACLE_N, pixels, 7, mode)
-        mean_rel = np.mean(np.abs(mean - oracle)[keep] / lum[keep, None])
-        assert mean_rel < 0.01, (mode, mean_rel)
+        bias = abs(mean[keep].mean() - oracle[keep].mean()) / oracle[keep].mean()
+        assert bias < 0.01, (mode, bias)
         z = (mean - oracle) / np.sqrt(var + o["oracle_var"] + 1e-16)
         assert np.mean(np.abs(z) > 4) < 0.01, (mode, np.mean(np.abs(z) > 4))
         converged[mode] = mean
@@ -141,8 +143,8 @@ def test_wavefront_against_the_fp64_oracle(which, precision_scenes, oracles):
     lum = oracle.mean(axis=1)
     keep = lum > 1e-3
     mean = wavefront_means(scene, ORACLE_N, pixels, 7)
-    mean_rel = np.mean(np.abs(mean - oracle)[keep] / lum[keep, None])
-    assert mean_rel < 0.01, mean_rel
+    bias = abs(mean[keep].mean() - oracle[keep].mean()) / oracle[keep].mean()
+    assert bias < 0.01, bias
     # The wavefront keeps no sums of squares: the megakernel's variance at the
     # same spp stands in for it (the two sample the same estimator).
     _, var = megakernel_means(scene, ORACLE_N, pixels, 7, ab.ACCUMULATE_FP64)
