@@ -742,22 +742,32 @@ def batched_figures(steps: int, warmup: int, count: int = 64, l2: dict | None = 
     ab.set_tuning(**{k: wave_shape[k] for k in ("blocks_per_sm", "trace_blocks_per_sm", "fetch_batch",
                                                  "iterations_per_graph", "slot_count", "trace_loop", "ray_sort")})
     # The fixed cost of one iteration (its graph's launches, the queue kernels on
-    # nearly empty queues, the host's completion polling): a 4 x 4-pixel job at
-    # 1 spp, whose iterations do almost no work, timed per iteration. Times the
-    # batch's iteration count, it bounds what one persistent launch for the whole
-    # batch could save.
+    # nearly empty queues, the host's completion polling): two 4 x 4-pixel jobs
+    # whose iterations do almost no work, at 1 and at 8 x 8 samples per pixel (a
+    # pixel's samples run one after another, so the second takes about 64 times
+    # the iterations); the difference of their times over the difference of
+    # their iteration counts leaves out the per-call costs. Times the batch's
+    # iteration count, it bounds what one persistent launch for the whole batch
+    # could save.
     tiny_acc = torch.zeros((16, 4), dtype=torch.float64, device="cuda")
-    tiny = [(loaded[jobs[0].scene], ab.RenderJob(4, 4, samples_per_axis=1, max_depth=8, method=ab.WAVEFRONT),
-             tiny_acc.data_ptr())]
-    ab.render_batch(tiny)
-    torch.cuda.synchronize()
-    tiny_ms = []
-    for _ in range(5):
-        start = time.perf_counter()
+    tiny_scene = loaded[jobs[0].scene]
+
+    def tiny_run(n):
+        tiny = [(tiny_scene, ab.RenderJob(4, 4, samples_per_axis=n, max_depth=8, method=ab.WAVEFRONT),
+                 tiny_acc.data_ptr())]
         ab.render_batch(tiny)
         torch.cuda.synchronize()
-        tiny_ms.append((time.perf_counter() - start) * 1e3 / max(ab.wavefront_last_iterations(), 1))
-    per_iteration_ms = statistics.median(tiny_ms)
+        runs = []
+        for _ in range(3):
+            start = time.perf_counter()
+            ab.render_batch(tiny)
+            torch.cuda.synchronize()
+            runs.append(((time.perf_counter() - start) * 1e3, ab.wavefront_last_iterations()))
+        return min(runs)
+
+    short_ms, short_iterations = tiny_run(1)
+    long_ms, long_iterations = tiny_run(8)
+    per_iteration_ms = (long_ms - short_ms) / max(long_iterations - short_iterations, 1)
     for s in loaded.values():
         s.check()
     batch_s = statistics.mean(batch_ms) / 1e3

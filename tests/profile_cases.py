@@ -8,7 +8,7 @@
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
 --scene icosphere6 or icosphere8 (displaced icospheres of 6 and 8 levels, 81,920 and
 1,310,720 triangles), max depth 10 (16 for icosphere8, as the bench frame), seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
-nodes then leaf, 1: one step). With --autotune the launch shape is tuned first (as bench.py
+nodes then leaf, 1: one step), --ray-sort its ray binning. With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
 for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel). `resolve` resolves
@@ -42,6 +42,8 @@ def main() -> None:
     parser.add_argument("--scene", choices=["trefoil", "icosphere6", "icosphere8"], default="trefoil")
     parser.add_argument("--depth", type=int, default=None, help="max depth (default 10; 16 for icosphere8)")
     parser.add_argument("--trace-loop", type=int, choices=[0, 1], default=None)
+    parser.add_argument("--ray-sort", type=int, choices=[0, 1, 2], default=None,
+                        help="wavefront: pin ray binning (0 none, 1 extension rays, 2 shadow rays too)")
     parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
                         help="megakernel per-pixel sums: FP64 or Kahan-compensated FP32")
     args = parser.parse_args()
@@ -60,11 +62,13 @@ def main() -> None:
             scene = ab.Scene.load(scenes.icosphere_scene(Path(tmp), levels=int(args.scene[-1])))
         else:
             scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
-        if args.trace_loop is not None:
+        if args.trace_loop is not None or args.ray_sort is not None:
             shape = ab.tuning()
             ab.set_tuning(blocks_per_sm=shape["blocks_per_sm"], trace_blocks_per_sm=4,
                           fetch_batch=shape["fetch_batch"], iterations_per_graph=shape["iterations_per_graph"],
-                          slot_count=shape["slot_count"], trace_loop=args.trace_loop)
+                          slot_count=shape["slot_count"],
+                          trace_loop=args.trace_loop if args.trace_loop is not None else shape["trace_loop"],
+                          ray_sort=args.ray_sort if args.ray_sort is not None else shape["ray_sort"])
         method = ab.WAVEFRONT if args.method == "wavefront" else ab.MEGAKERNEL
         accumulation = ab.ACCUMULATE_KAHAN_FP32 if args.accumulation == "kahan" else ab.ACCUMULATE_FP64
         depth = args.depth if args.depth is not None else (16 if args.scene == "icosphere8" else 10)
