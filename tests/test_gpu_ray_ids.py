@@ -57,13 +57,23 @@ def ulp_distance(ours_f32, reference_f64):
 
 def classify(scene, rays, ours):
     """(agree, ties) masks: the device's answer equals the FP64 restatement's, or
-    differs by an explained near-tie; asserts that nothing is unexplained."""
-    klass = restatement.classify(scene, rays, ours)
-    unexplained = np.flatnonzero(klass["class"] == 2)
-    assert len(unexplained) == 0, (len(unexplained), unexplained[:10], klass["detail"][unexplained[:10]])
-    ties = klass["class"] == 1
-    assert ties.sum() <= MAX_TIES * len(rays) / 1e6, ties.sum()
-    return klass["class"] == 0, ties
+    differs by an explained near-tie; asserts that nothing is unexplained. The
+    disagreements are counted first (the classification tests every primitive of
+    the scene for each of them), so a broken traversal fails at once."""
+    mine = restatement.intersect(scene, rays.astype(np.float64))
+    differ = (ours["hit"] != mine["hit"]) | ((ours["hit"] == 1) & ((ours["object"] != mine["object"]) |
+                                                                   (ours["triangle"] != mine["triangle"])))
+    assert differ.sum() <= MAX_TIES * len(rays) / 1e6, differ.sum()
+    subset = np.flatnonzero(differ)
+    klass = np.zeros(len(rays), np.int32)
+    if len(subset):
+        picked = {k: ours[k][subset] for k in ("hit", "object", "triangle")}
+        result = restatement.classify(scene, rays[subset], picked)
+        klass[subset] = result["class"]
+        unexplained = np.flatnonzero(result["class"] == 2)
+        assert len(unexplained) == 0, (len(unexplained), subset[unexplained[:10]], result["detail"][unexplained[:10]])
+    assert np.all(klass[subset] == 1)
+    return klass == 0, klass == 1
 
 
 @pytest.mark.parametrize("which", ["room", "trefoil"])
