@@ -422,16 +422,16 @@ std::array<Candidate, 2> sphereCandidates(const SphereDesc& s, const Ray& ray, d
     return roots;
 }
 
-struct Verdict {
+struct Reach {
     bool possible{false};
     bool sure{false};
 };
 
-Verdict judge(const Candidate& c, double t_min, double t_max)
+Reach reachOf(const Candidate& c, double t_min, double t_max)
 {
     const double along_min{(c.t - t_min) * c.scale};
     const double along_max{(t_max - c.t) * c.scale};
-    Verdict v;
+    Reach v;
     v.possible = c.margin >= -c.delta && along_min >= -c.delta && along_max >= -c.delta;
     v.sure = c.margin > c.delta && along_min > c.delta && along_max > c.delta;
     return v;
@@ -591,7 +591,7 @@ void oracle_classify(const void* view, const double* rays, std::int64_t count, d
         bool mine_possible{false};
         std::int64_t possible_nearer{0};
         forEachCandidate(scene, ray, ulps, [&](std::int64_t id, std::int64_t tri, const Candidate& c, double) {
-            const Verdict v{judge(c, t_min, t_max)};
+            const Reach v{reachOf(c, t_min, t_max)};
             if (v.sure && c.t < sure_t) {
                 sure_t = c.t;
                 sure = c;
@@ -604,7 +604,7 @@ void oracle_classify(const void* view, const double* rays, std::int64_t count, d
             }
         });
         forEachCandidate(scene, ray, ulps, [&](std::int64_t, std::int64_t, const Candidate& c, double) {
-            if (judge(c, t_min, t_max).possible && c.t < sure_t) {
+            if (reachOf(c, t_min, t_max).possible && c.t < sure_t) {
                 ++possible_nearer;
             }
         });
