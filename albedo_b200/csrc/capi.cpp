@@ -1217,7 +1217,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         }
         unsigned int* error_flag{items[0].scene->error_flag.as<unsigned int>()};
         TuneTimer timer;
-        const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {2, 3, 4}},
+        const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {3, 4, 5}},
                                           {"fetch_batch", {16, 32, 64, 128}},
                                           {"trace_loop", {0, 1}},
                                           {"blocks_per_sm", {4, 8, 16}},
@@ -1245,7 +1245,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
             g_engine_slots = v[5];
             g_engine_shape = shape;
         };
-        const std::vector<int> start{kept_shape.trace_blocks_per_sm > 0 ? kept_shape.trace_blocks_per_sm : 4,
+        const std::vector<int> start{kept_shape.trace_blocks_per_sm > 0 ? kept_shape.trace_blocks_per_sm : 5,
                                      kept_shape.fetch_batch, kept_shape.trace_loop, kept_shape.blocks_per_sm,
                                      kept_shape.iterations_per_graph, kept_slots, kept_shape.ray_sort};
         TuneOutcome outcome;

@@ -71,10 +71,9 @@ auto withStack(int capacity, F&& f)
 // Lets `kernel` use `entries` stack entries of dynamic shared memory per thread
 // in 128-thread blocks (above the 48 KB default when needed).
 template <typename Kernel>
-cudaError_t allowStackMemory(Kernel kernel, int entries)
+cudaError_t allowStackMemory(Kernel kernel, int entries, int entry_bytes = static_cast<int>(sizeof(uint2)))
 {
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                entries * 128 * static_cast<int>(sizeof(uint2)));
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, entries * 128 * entry_bytes);
 }
 
 // The plain megakernel: one thread per pixel, serial over that pixel's n x n

@@ -13,7 +13,13 @@
 //
 // The traversal stack lives in shared memory: entry i of thread `lane` is at
 // stack[i * stride + lane] (entry-major, so a warp touching the same depth hits
-// consecutive banks). Each entry is (child reference, entry distance).
+// consecutive banks). An entry is either (child reference, entry distance), 8
+// bytes, and a popped entry whose box is entered beyond the current hit is
+// dropped as the reference drops it; or the child reference alone, 4 bytes,
+// and the popped node or leaf is visited and culled by its own box tests. Both
+// give the same hits: a primitive below a node entered beyond the current hit
+// cannot be hit nearer than it. The 4-byte form halves the shared memory of
+// the wavefront's persistent traversal kernels, so more of them fit on an SM.
 #pragma once
 
 #include "common.cuh"
@@ -345,10 +351,21 @@ __device__ __forceinline__ void countReferenceBoxes(const float4& lx, const floa
     }
 }
 
+// One stack entry: child reference and entry distance, or the reference alone.
+__device__ __forceinline__ void pushEntry(uint2* slot, std::uint32_t ref, float entry)
+{
+    *slot = make_uint2(ref, __float_as_uint(entry));
+}
+__device__ __forceinline__ void pushEntry(unsigned* slot, std::uint32_t ref, float)
+{
+    *slot = ref;
+}
+
 // A 4-wide node: tests every child box, continues with the hit child the
 // reference reaches first and pushes the other hit children, last first, so
 // leaves are reached in the reference's depth-first near-first order.
-__device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, uint2* stack, int stride, int stack_size,
+template <typename Stack>
+__device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, Stack* stack, int stride, int stack_size,
                                         unsigned int* error_flag, TraversalCounts* counts)
 {
     const float4* np = reinterpret_cast<const float4*>(s.nodes + q.ref);
@@ -400,7 +417,7 @@ __device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, uint2*
             q.ref = child;
         } else {
             const float entry = c == 0u ? e0 : (c == 1u ? e1 : (c == 2u ? e2 : e3));
-            stack[q.sp * stride] = make_uint2(child, __float_as_uint(entry));
+            pushEntry(stack + q.sp * stride, child, entry);
             ++q.sp;
         }
     }
@@ -410,7 +427,8 @@ __device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, uint2*
 // A leaf. In the TLAS: spheres, scene triangles and instances in leaf order; an
 // instance is entered at once (the rest of the leaf and an exit marker are
 // pushed). In a BLAS: the current instance's triangles.
-__device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const SkipRule& skip, uint2* stack,
+template <typename Stack>
+__device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const SkipRule& skip, Stack* stack,
                                         int stride, int stack_size, unsigned int* error_flag,
                                         TraversalCounts* counts, bool any)
 {
@@ -429,10 +447,10 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
                     return kStepFinished;
                 }
                 if (k + 1 < count) {
-                    stack[q.sp * stride] = make_uint2(leafRef(pos + 1, count - k - 1), __float_as_uint(-INFINITY));
+                    pushEntry(stack + q.sp * stride, leafRef(pos + 1, count - k - 1), -INFINITY);
                     ++q.sp;
                 }
-                stack[q.sp * stride] = make_uint2(kExitMarker, 0u);
+                pushEntry(stack + q.sp * stride, kExitMarker, 0.0f);
                 ++q.sp;
                 const DevInstance& inst = s.instances[obj.index];
                 if (counts != nullptr) {
@@ -529,6 +547,26 @@ __device__ __forceinline__ bool popNext(TraceState& q, const uint2* stack, int s
     }
 }
 
+// The same for 4-byte entries: no entry distance, so nothing is dropped here;
+// the popped node's or leaf's own tests cull it.
+__device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, int stride)
+{
+    for (;;) {
+        if (q.sp == 0) {
+            return false;
+        }
+        --q.sp;
+        const unsigned ref = stack[q.sp * stride];
+        if (ref == kExitMarker) {
+            q.r.setup(q.origin, q.dir);
+            q.inst_pos = kNoPrim;
+            continue;
+        }
+        q.ref = ref;
+        return true;
+    }
+}
+
 // One turn of a query in a persistent kernel; returns whether the query has more
 // work (false: finished). LOOP picks how much a turn does (the wavefront's
 // autotuner chooses per workload; both visit the same nodes and leaves in the
@@ -540,8 +578,8 @@ __device__ __forceinline__ bool popNext(TraceState& q, const uint2* stack, int s
 //                       sooner.
 enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1 };
 
-template <int LOOP>
-__device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, uint2* stack,
+template <int LOOP, typename Stack>
+__device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, Stack* stack,
                                              int stride, int stack_size, unsigned int* error_flag,
                                              TraversalCounts* counts, bool any)
 {

@@ -64,7 +64,7 @@ def main() -> None:
             scene = ab.Scene.load(scenes.trefoil_scene(Path(tmp)))
         if args.trace_loop is not None or args.ray_sort is not None:
             shape = ab.tuning()
-            ab.set_tuning(blocks_per_sm=shape["blocks_per_sm"], trace_blocks_per_sm=4,
+            ab.set_tuning(blocks_per_sm=shape["blocks_per_sm"], trace_blocks_per_sm=5,
                           fetch_batch=shape["fetch_batch"], iterations_per_graph=shape["iterations_per_graph"],
                           slot_count=shape["slot_count"],
                           trace_loop=args.trace_loop if args.trace_loop is not None else shape["trace_loop"],

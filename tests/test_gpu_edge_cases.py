@@ -348,7 +348,7 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
                        slot_count=1 << 14, trace_loop=1),
                   dict(blocks_per_sm=16, trace_blocks_per_sm=4, fetch_batch=128, iterations_per_graph=8,
                        slot_count=1 << 20, trace_loop=0),
-                  dict(blocks_per_sm=8, trace_blocks_per_sm=4, fetch_batch=32, iterations_per_graph=4,
+                  dict(blocks_per_sm=8, trace_blocks_per_sm=5, fetch_batch=32, iterations_per_graph=4,
                        slot_count=1 << 16, trace_loop=1, ray_sort=1),
                   dict(blocks_per_sm=8, trace_blocks_per_sm=3, fetch_batch=64, iterations_per_graph=4,
                        slot_count=1 << 20, trace_loop=0, ray_sort=2)):

@@ -252,10 +252,11 @@ def trace_modes(scene, rays, any_hit, persistent, t_max=float("inf")):
 @pytest.mark.parametrize("mode", [1, 2])
 def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, mode, room_path, trefoil_path):
     """The wavefront's persistent kernels (warp fetch; a turn descends nodes then
-    handles a leaf, mode 1, or takes one step, mode 2) trace every query with the
-    same steps as the per-thread traversal the ray-query tests compare with the
-    reference: hit flags, FP32 t, object and triangle are identical bit for bit,
-    for closest-hit and any-hit queries."""
+    handles a leaf, mode 1, or takes one step, mode 2; 4-byte stack entries that
+    keep no entry distance) reach the leaves in the same order as the per-thread
+    traversal the ray-query tests compare with the reference, and give the same
+    hits: hit flags, FP32 t, object and triangle are identical bit for bit, for
+    closest-hit and any-hit queries."""
     scene = ab.Scene.load(room_path if which == "room" else trefoil_path)
     rays = random_rays(100_000, 12, [-2.8, 0.05, -3.5], [2.8, 4.5, 3.0])
     t_max = 3.0 if any_hit else float("inf")
