@@ -1157,18 +1157,20 @@ int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job
         // Kernel variants: 0 = 3 blocks/SM, 1 = 4 blocks/SM (both with the
         // out-of-line traversal), 2 = 3 blocks/SM with both queries' traversal
         // inlined, 3 = 3 blocks/SM with the closest-hit traversal inlined and
-        // the shadow query out of line (path estimator only).
+        // the shadow query out of line, 4 = 4 blocks/SM with both inlined
+        // (path estimator only). The 4-blocks/SM kernels of the path estimator
+        // keep the path's state in shared memory.
         const bool can_inline{probe.estimator == ALBEDO_PATH};
         const std::vector<TuneKnob> knobs{
             {"tile_width", {8, 16, 32}},
-            {"variant", can_inline ? std::vector<int>{0, 1, 2, 3} : std::vector<int>{0, 1}}};
+            {"variant", can_inline ? std::vector<int>{0, 1, 2, 3, 4} : std::vector<int>{0, 1}}};
         const int kept_tile{scene->mega_tile_width};
         const int kept_blocks{scene->mega_blocks_per_sm};
         const int kept_inline{scene->mega_inline};
         const auto apply = [&](const std::vector<int>& v) {
             scene->mega_tile_width = v[0];
-            scene->mega_blocks_per_sm = v[1] == 1 ? 4 : 3;
-            scene->mega_inline = v[1] == 2 ? 1 : (v[1] == 3 ? 2 : 0);
+            scene->mega_blocks_per_sm = v[1] == 1 || v[1] == 4 ? 4 : 3;
+            scene->mega_inline = v[1] == 2 || v[1] == 4 ? 1 : (v[1] == 3 ? 2 : 0);
         };
         TuneOutcome outcome;
         try {
@@ -1219,10 +1221,10 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         TuneTimer timer;
         const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {3, 4, 5}},
                                           {"fetch_batch", {16, 32, 64, 128}},
-                                          {"trace_loop", {0, 1}},
+                                          {"trace_loop", {0, 1, 2}},
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
-                                          {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21}},
+                                          {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22}},
                                           {"ray_sort", {0, 1, 2}}};
         const WfShape kept_shape{engineShape()};
         int kept_slots{0};
@@ -1285,9 +1287,10 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
                 throw std::invalid_argument{std::format("megakernel blocks per SM must be 3 or 4, got {}",
                                                         shape->blocks_per_sm)};
             }
-            if (shape->inline_traversal != 0 &&
-                (shape->inline_traversal < 0 || shape->inline_traversal > 2 || shape->blocks_per_sm != 3)) {
-                throw std::invalid_argument{"the inlined-traversal megakernels (1 or 2) run at 3 blocks per SM"};
+            if (shape->inline_traversal < 0 || shape->inline_traversal > 2 ||
+                (shape->inline_traversal == 2 && shape->blocks_per_sm != 3)) {
+                throw std::invalid_argument{"megakernel traversal placement must be 0 (out of line), 1 (inlined) or "
+                                            "2 (closest hit inlined, 3 blocks per SM only)"};
             }
             scene->mega_tile_width = shape->tile_width;
             scene->mega_blocks_per_sm = shape->blocks_per_sm;
@@ -1298,8 +1301,8 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
             shape->iterations_per_graph <= 0 || shape->slot_count <= 0) {
             throw std::invalid_argument{"wavefront shape values must be positive"};
         }
-        if (shape->trace_loop != 0 && shape->trace_loop != 1) {
-            throw std::invalid_argument{"the traversal turn shape must be 0 or 1"};
+        if (shape->trace_loop < 0 || shape->trace_loop > 2) {
+            throw std::invalid_argument{"the traversal turn shape must be 0, 1 or 2"};
         }
         if (shape->ray_sort < 0 || shape->ray_sort > 2) {
             throw std::invalid_argument{"ray binning must be 0, 1 or 2"};
@@ -1769,8 +1772,8 @@ int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64
         DeviceBuffer obj{n * sizeof(unsigned int)};
         DeviceBuffer tri{n * sizeof(unsigned int)};
         check(cudaMemset(counter.ptr, 0, sizeof(int)), "cudaMemset");
-        if (persistent < 0 || persistent > 2) {
-            throw std::invalid_argument{"persistent must be 0, 1 or 2"};
+        if (persistent < 0 || persistent > 3) {
+            throw std::invalid_argument{"persistent must be 0, 1, 2 or 3"};
         }
         check(launchTraceModes(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max, any != 0,
                                persistent, scene->stack_capacity, counter.as<int>(),

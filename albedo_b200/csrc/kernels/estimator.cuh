@@ -18,13 +18,14 @@ namespace albedo_b200 {
 // Where a thread's queries keep their stack, and how they are traced: INLINE
 // places the closest-hit traversal in the calling kernel, INLINE_SHADOW the
 // shadow queries' traversal (by default as INLINE), COUNT counts the work into
-// `counts` (traceScene).
-template <bool INLINE, bool COUNT = false, bool INLINE_SHADOW = INLINE>
+// `counts` (traceScene). Stack entries are uint2 (child reference and entry
+// distance) or unsigned (the reference alone).
+template <bool INLINE, bool COUNT = false, bool INLINE_SHADOW = INLINE, typename Stack = uint2>
 struct TraceContext {
     static constexpr bool kInline = INLINE;
     static constexpr bool kInlineShadow = INLINE_SHADOW;
     static constexpr bool kCount = COUNT;
-    uint2* stack;
+    Stack* stack;
     int stride;
     int capacity;
     unsigned int* error_flag;

@@ -7,6 +7,8 @@
 // shared memory (STACK entries of 8 bytes).
 #include "estimator.cuh"
 
+#include <type_traits>
+
 namespace albedo_b200 {
 
 namespace {
@@ -26,9 +28,11 @@ constexpr int kMegaBlocksPerSm = ALBEDO_MEGA_BLOCKS_PER_SM;
 template <int ACC>
 struct PixelSums;
 
+// reset() zeroes them.
 template <>
 struct PixelSums<kAccumulateFp64> {
-    double r = 0.0, g = 0.0, b = 0.0;
+    double r, g, b;
+    ALB_DEV void reset() { r = g = b = 0.0; }
     ALB_DEV void add(float3 v)
     {
         r += v.x;
@@ -40,8 +44,9 @@ struct PixelSums<kAccumulateFp64> {
 
 template <>
 struct PixelSums<kAccumulateKahan> {
-    float r = 0.0f, g = 0.0f, b = 0.0f;
-    float cr = 0.0f, cg = 0.0f, cb = 0.0f;
+    float r, g, b;
+    float cr, cg, cb;
+    ALB_DEV void reset() { r = g = b = cr = cg = cb = 0.0f; }
     // Kahan 1965: c carries the low-order part lost by the previous addition.
     static ALB_DEV void kahan(float& sum, float& c, float v)
     {
@@ -62,21 +67,38 @@ struct PixelSums<kAccumulateKahan> {
     }
 };
 
+// A path's state kept in shared memory by the lean variants: 23 words a thread
+// (an odd stride, so a warp's accesses to one field hit 32 different banks).
+struct alignas(4) SharedPath {
+    PathState p;
+    float pad;
+};
+static_assert(sizeof(SharedPath) % 8 == 4, "odd word stride");
+
+// Stack entry type of a megakernel variant: LEAN kernels keep the child
+// reference alone (4 bytes).
+template <bool LEAN>
+using MegaStackEntry = std::conditional_t<LEAN, unsigned, uint2>;
+
 // INL: 0 = both queries call the shared out-of-line traversal, 1 = both are
 // inlined, 2 = the closest-hit query is inlined and the shadow query calls the
 // out-of-line copy (a smaller kernel than 1, no register saves around the
-// per-bounce call).
+// per-bounce call). LEAN: the path's state between bounces lives in shared
+// memory rather than registers and the stack entries are 4 bytes, so fewer
+// registers carry state across the traversal and more blocks fit an SM.
 template <int STACK, int EST, bool COUNT = false, int MINB = kMegaBlocksPerSm, int ACC = kAccumulateFp64,
-          int INL = 0>
+          int INL = 0, bool LEAN = false>
 __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene, const DevCamera camera,
                                                           const RenderArgs args, PixelAccum* accum,
                                                           unsigned int* error_flag,
                                                           unsigned long long* totals = nullptr)
 {
-    extern __shared__ uint2 stack[];
+    using Entry = MegaStackEntry<LEAN>;
+    extern __shared__ uint2 stack_memory[];
+    Entry* const stack = reinterpret_cast<Entry*>(stack_memory);
     TraversalCounts counts{0, 0, 0, 0, 0, 0};
-    const TraceContext<INL != 0, COUNT, INL == 1> ctx{stack + threadIdx.x, kBlock, STACK, error_flag,
-                                                      COUNT ? &counts : nullptr};
+    const TraceContext<INL != 0, COUNT, INL == 1, Entry> ctx{stack + threadIdx.x, kBlock, STACK, error_flag,
+                                                             COUNT ? &counts : nullptr};
     int x, y, slot;
     if (args.pixels != nullptr) {
         slot = blockIdx.x * kBlock + threadIdx.x;
@@ -103,6 +125,7 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
     const float width = static_cast<float>(args.width);
     const float height = static_cast<float>(args.height);
     PixelSums<ACC> sums;
+    sums.reset();
     // Sums of squared samples (for two-sample tests) go straight to memory, one
     // read-modify-write per sample, only when asked for: no registers carry them
     // through the traversal calls of an ordinary render.
@@ -113,7 +136,13 @@ __global__ void __launch_bounds__(kBlock, MINB) megakernel(const DevScene scene,
     // path of every sample.
     const int total = n * n;
     int sample = 0;
-    PathState path;
+    PathState local_path;
+    PathState* path_ptr = &local_path;
+    if constexpr (LEAN) {
+        __shared__ SharedPath shared_paths[kBlock];
+        path_ptr = &shared_paths[threadIdx.x].p;
+    }
+    PathState& path = *path_ptr;
     startSample(camera, path, g, x, y, 0, n, inv_n, width, height);
     for (;;) {
         if (estimatorBounce<EST>(scene, ctx, path, g, args)) {
@@ -235,7 +264,10 @@ __global__ void __launch_bounds__(kBlock) occludedKernel(const DevScene scene, c
                           : 0;
 }
 
-constexpr std::size_t stackBytes(int stack) { return static_cast<std::size_t>(stack) * kBlock * sizeof(uint2); }
+constexpr std::size_t stackBytes(int stack, std::size_t entry_bytes = sizeof(uint2))
+{
+    return static_cast<std::size_t>(stack) * kBlock * entry_bytes;
+}
 
 int megaBlocks(const RenderArgs& args)
 {
@@ -247,18 +279,19 @@ int megaBlocks(const RenderArgs& args)
     return ((args.width + tile_w - 1) / tile_w) * ((args.height + tile_h - 1) / tile_h);
 }
 
-// Launches `kernel` over `blocks` blocks with a STACK-entry shared-memory stack.
-template <int STACK, typename Kernel, typename... Args>
+// Launches `kernel` over `blocks` blocks with a STACK-entry shared-memory stack
+// of ENTRY-byte entries.
+template <int STACK, int ENTRY = static_cast<int>(sizeof(uint2)), typename Kernel, typename... Args>
 cudaError_t launchStacked(Kernel kernel, int blocks, cudaStream_t stream, Args... args)
 {
     if (blocks == 0) {
         return cudaSuccess;
     }
-    const cudaError_t e = allowStackMemory(kernel, STACK);
+    const cudaError_t e = allowStackMemory(kernel, STACK, ENTRY);
     if (e != cudaSuccess) {
         return e;
     }
-    kernel<<<blocks, kBlock, stackBytes(STACK), stream>>>(args...);
+    kernel<<<blocks, kBlock, stackBytes(STACK, ENTRY), stream>>>(args...);
     return cudaGetLastError();
 }
 
@@ -289,6 +322,36 @@ int stackCapacityFor(std::uint32_t stack_need)
     return 0;
 }
 
+// Path-estimator megakernel of the shape `args` names: blocks_per_sm 3 (state
+// in registers, 8-byte stack entries) or 4 (lean: state in shared memory,
+// 4-byte stack entries), and how its traversal is placed (inline_traversal).
+template <int S, int ACC>
+cudaError_t launchPathMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args,
+                                 PixelAccum* accum, unsigned int* error_flag, cudaStream_t stream)
+{
+    unsigned long long* no_totals = nullptr;
+    const int blocks = megaBlocks(args);
+    if (args.blocks_per_sm == 4) {
+        constexpr int kEntry = static_cast<int>(sizeof(unsigned));
+        if (args.inline_traversal == 1) {
+            return launchStacked<S, kEntry>(megakernel<S, kEstimatorPath, false, 4, ACC, 1, true>, blocks, stream,
+                                            scene, camera, args, accum, error_flag, no_totals);
+        }
+        return launchStacked<S, kEntry>(megakernel<S, kEstimatorPath, false, 4, ACC, 0, true>, blocks, stream, scene,
+                                        camera, args, accum, error_flag, no_totals);
+    }
+    if (args.inline_traversal == 1) {
+        return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, ACC, 1>, blocks, stream, scene,
+                                camera, args, accum, error_flag, no_totals);
+    }
+    if (args.inline_traversal == 2) {
+        return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, ACC, 2>, blocks, stream, scene,
+                                camera, args, accum, error_flag, no_totals);
+    }
+    return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, ACC>, blocks, stream, scene, camera,
+                            args, accum, error_flag, no_totals);
+}
+
 cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, const RenderArgs& args, PixelAccum* accum,
                              unsigned int* error_flag, int stack_capacity, cudaStream_t stream)
 {
@@ -304,40 +367,9 @@ cudaError_t launchMegakernel(const DevScene& scene, const DevCamera& camera, con
                                     accum, error_flag, no_totals);
         default:
             if (args.accumulation == kAccumulateKahan) {
-                if (args.inline_traversal == 1) {
-                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan,
-                                                       1>,
-                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
-                                            no_totals);
-                }
-                if (args.inline_traversal == 2) {
-                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan,
-                                                       2>,
-                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
-                                            no_totals);
-                }
-                if (args.blocks_per_sm == 4) {
-                    return launchStacked<S>(megakernel<S, kEstimatorPath, false, 4, kAccumulateKahan>,
-                                            megaBlocks(args), stream, scene, camera, args, accum, error_flag,
-                                            no_totals);
-                }
-                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateKahan>,
-                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
+                return launchPathMegakernel<S, kAccumulateKahan>(scene, camera, args, accum, error_flag, stream);
             }
-            if (args.inline_traversal == 1) {
-                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, 1>,
-                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
-            }
-            if (args.inline_traversal == 2) {
-                return launchStacked<S>(megakernel<S, kEstimatorPath, false, kMegaBlocksPerSm, kAccumulateFp64, 2>,
-                                        megaBlocks(args), stream, scene, camera, args, accum, error_flag, no_totals);
-            }
-            if (args.blocks_per_sm == 4) {
-                return launchStacked<S>(megakernel<S, kEstimatorPath, false, 4>, megaBlocks(args), stream, scene,
-                                        camera, args, accum, error_flag, no_totals);
-            }
-            return launchStacked<S>(megakernel<S, kEstimatorPath>, megaBlocks(args), stream, scene, camera, args,
-                                    accum, error_flag, no_totals);
+            return launchPathMegakernel<S, kAccumulateFp64>(scene, camera, args, accum, error_flag, stream);
         }
     });
 }

@@ -70,18 +70,19 @@ struct TraceHit {
 // The ray as traversal and the watertight test need it (accel/bvh.hpp:60-78,
 // geometry/triangle.cpp:81-106).
 struct TravRay {
-    float3 o, d, inv;
+    float3 o, inv; // the direction itself is the caller's (spheres, the only users, are in world space)
     std::uint32_t neg; // bit a set when d[a] < 0
     int kx, ky, kz;
     float sx, sy, sz;
-    bool usable; // |d|^2 is a normal number
+    std::uint32_t planes; // bit a set when inv[a] is negative (-0 directions included): the box test's near planes
+    bool usable;          // |d|^2 is a normal number
 
     ALB_DEV void setup(float3 origin, float3 dir)
     {
         o = origin;
-        d = dir;
         inv = mk(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
         neg = (dir.x < 0.0f ? 1u : 0u) | (dir.y < 0.0f ? 2u : 0u) | (dir.z < 0.0f ? 4u : 0u);
+        planes = (signbit(inv.x) ? 1u : 0u) | (signbit(inv.y) ? 2u : 0u) | (signbit(inv.z) ? 4u : 0u);
         usable = isNormalF(lengthSquared(dir));
         const float mx = fabsf(dir.x);
         const float my = fabsf(dir.y);
@@ -128,28 +129,97 @@ ALB_DEV bool slabTest(float lox, float hix, float loy, float hiy, float loz, flo
     return lo <= hi;
 }
 
+// Three-input FP32 maximum and minimum (one instruction each on sm_100a). With
+// no NaN operand they are the plain maximum and minimum.
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// slabTest without branches, given the box's near and far planes on each axis:
+// lo and hi where the inverse direction's sign bit is clear, hi and lo where it
+// is set (a -0 direction component gives a -infinite inverse, so it counts as
+// negative). It returns slabTest's answer and entry distance (up to the sign of
+// a zero entry distance, which only comparisons read):
+//   - With a finite nonzero inverse no distance is NaN, and rounding is
+//     monotone, so (near - o) * inv <= (far - o) * inv: these are the clip's
+//     entry and exit distances after its swap.
+//   - The entry is the largest of tmin and the three axis entries, in any order;
+//     the three-input maximum and minimum skip a NaN operand as the clip's
+//     comparisons do.
+//   - The exit widening w(f) = f * (f < 0 ? 2 - W : W) is nondecreasing, so
+//     min(tmax, w(fx), w(fy), w(fz)) = min(tmax, w(min(fx, fy, fz))); and
+//     w(f) = max(f * W, f * (2 - W)) since W > 1.
+//   - An infinite inverse (a zero or subnormal direction component) gives the
+//     clip's answer on that axis too, with one exception: for a -infinite
+//     inverse and an origin lying exactly on one of the slab's two planes (not
+//     both), the clip's NaN, left in place by its swap rule, rejects the box,
+//     and this test enters it. Entering a box more can only add primitive tests,
+//     never lose a hit.
+// The four children of a node test independently.
+__device__ __forceinline__ bool slabTestOrdered(float nx, float fx, float ny, float fy, float nz, float fz,
+                                                const TravRay& r, float tmin, float tmax, float& entry)
+{
+    const float tnx = __fmul_rn(__fsub_rn(nx, r.o.x), r.inv.x);
+    const float tfx = __fmul_rn(__fsub_rn(fx, r.o.x), r.inv.x);
+    const float tny = __fmul_rn(__fsub_rn(ny, r.o.y), r.inv.y);
+    const float tfy = __fmul_rn(__fsub_rn(fy, r.o.y), r.inv.y);
+    const float tnz = __fmul_rn(__fsub_rn(nz, r.o.z), r.inv.z);
+    const float tfz = __fmul_rn(__fsub_rn(fz, r.o.z), r.inv.z);
+    const float lo = max3f(tnx, tny, fmaxf(tnz, tmin));
+    const float f = min3f(tfx, tfy, tfz);
+    const float hi = fminf(fmaxf(__fmul_rn(f, kBoxExitWidening), __fmul_rn(f, 2.0f - kBoxExitWidening)), tmax);
+    entry = lo;
+    return lo <= hi;
+}
+
+// Explicitly rounded arithmetic: every product and sum rounds on its own, as the
+// reference (built without contraction) rounds in FP64. Traversal code uses them
+// so that every kernel compiles a query to the same operations: an FMA the
+// compiler may contract in one kernel and not in another would give two kernels
+// different hit distances.
+ALB_DEV float rmul(float a, float b) { return __fmul_rn(a, b); }
+ALB_DEV float radd(float a, float b) { return __fadd_rn(a, b); }
+ALB_DEV float rsub(float a, float b) { return __fsub_rn(a, b); }
+ALB_DEV double rmul(double a, double b) { return __dmul_rn(a, b); }
+ALB_DEV double radd(double a, double b) { return __dadd_rn(a, b); }
+ALB_DEV double rsub(double a, double b) { return __dsub_rn(a, b); }
+template <typename T>
+ALB_DEV T rdot(T ax, T ay, T az, T bx, T by, T bz)
+{
+    return radd(radd(rmul(ax, bx), rmul(ay, by)), rmul(az, bz));
+}
+
 // Haines' sphere test in precision T (geometry/sphere.cpp:92-135), returning the
 // nearest root strictly inside (tmin, tmax), honouring the skip mode.
 template <typename T>
 ALB_DEV bool sphereRoot(T ox, T oy, T oz, T dx, T dy, T dz, T cx, T cy, T cz, T radius, T tmin, T tmax, int mode,
                         T& t_out)
 {
-    const T ocx = ox - cx;
-    const T ocy = oy - cy;
-    const T ocz = oz - cz;
-    const T a = dx * dx + dy * dy + dz * dz;
-    const T h = dx * ocx + dy * ocy + dz * ocz;
-    const T r2 = radius * radius;
-    const T c = (ocx * ocx + ocy * ocy + ocz * ocz) - r2;
+    const T ocx = rsub(ox, cx);
+    const T ocy = rsub(oy, cy);
+    const T ocz = rsub(oz, cz);
+    const T a = rdot(dx, dy, dz, dx, dy, dz);
+    const T h = rdot(dx, dy, dz, ocx, ocy, ocz);
+    const T r2 = rmul(radius, radius);
+    const T c = rsub(rdot(ocx, ocy, ocz, ocx, ocy, ocz), r2);
     const T k = h / a;
-    const T lx = ocx - dx * k;
-    const T ly = ocy - dy * k;
-    const T lz = ocz - dz * k;
-    const T disc = a * (r2 - (lx * lx + ly * ly + lz * lz));
+    const T lx = rsub(ocx, rmul(dx, k));
+    const T ly = rsub(ocy, rmul(dy, k));
+    const T lz = rsub(ocz, rmul(dz, k));
+    const T disc = rmul(a, rsub(r2, rdot(lx, ly, lz, lx, ly, lz)));
     if (disc < T(0)) {
         return false;
     }
-    const T q = -(h + copysign(sqrt(disc), h));
+    const T q = -radd(h, copysign(sqrt(disc), h));
     T near_root = T(0);
     T far_root = T(0);
     if (q != T(0)) {
@@ -169,18 +239,19 @@ ALB_DEV bool sphereRoot(T ox, T oy, T oz, T dx, T dy, T dz, T cx, T cy, T cz, T 
         }
     }
     // A hit point that rounds onto the center has no normal: a miss (geometry/sphere.cpp:121-126).
-    const T px = ox + dx * t - cx;
-    const T py = oy + dy * t - cy;
-    const T pz = oz + dz * t - cz;
-    if (!(px * px + py * py + pz * pz > T(0))) {
+    const T px = rsub(radd(ox, rmul(dx, t)), cx);
+    const T py = rsub(radd(oy, rmul(dy, t)), cy);
+    const T pz = rsub(radd(oz, rmul(dz, t)), cz);
+    if (!(rdot(px, py, pz, px, py, pz) > T(0))) {
         return false;
     }
     t_out = t;
     return true;
 }
 
-ALB_DEV bool intersectSphere(const TravRay& r, const DevSphere& s, bool wide, float tmin, float tmax, int mode,
-                             float& t)
+// `r` is the world-space ray whose direction is `d`.
+ALB_DEV bool intersectSphere(const TravRay& r, float3 d, const DevSphere& s, bool wide, float tmin, float tmax,
+                             int mode, float& t)
 {
     if (!r.usable) {
         return false;
@@ -189,7 +260,7 @@ ALB_DEV bool intersectSphere(const TravRay& r, const DevSphere& s, bool wide, fl
         // Coordinates of order 1e4 (room-sized walls): o - c and |o - c|^2 - r^2
         // cancel catastrophically in FP32, so the quadratic runs in FP64.
         double td;
-        if (!sphereRoot<double>(r.o.x, r.o.y, r.o.z, r.d.x, r.d.y, r.d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, td)) {
+        if (!sphereRoot<double>(r.o.x, r.o.y, r.o.z, d.x, d.y, d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, td)) {
             return false;
         }
         const float tf = static_cast<float>(td);
@@ -199,7 +270,7 @@ ALB_DEV bool intersectSphere(const TravRay& r, const DevSphere& s, bool wide, fl
         t = tf;
         return true;
     }
-    return sphereRoot<float>(r.o.x, r.o.y, r.o.z, r.d.x, r.d.y, r.d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, t);
+    return sphereRoot<float>(r.o.x, r.o.y, r.o.z, d.x, d.y, d.z, s.cx, s.cy, s.cz, s.r, tmin, tmax, mode, t);
 }
 
 // Woop-Benthin-Wald watertight test (geometry/triangle.cpp:132-176). Every
@@ -252,15 +323,18 @@ ALB_DEV bool intersectTriangle(const TravRay& r, const float4& p0, const float4&
     return true;
 }
 
+// An instance's 3x4 row-major affine map applied to a point and to a vector,
+// explicitly rounded (the ray a query carries into an instance must be the
+// same in every kernel).
 ALB_DEV float3 affinePoint(const float* m, float3 p)
 {
-    return mk(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3], m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
-              m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+    return mk(radd(rdot(m[0], m[1], m[2], p.x, p.y, p.z), m[3]), radd(rdot(m[4], m[5], m[6], p.x, p.y, p.z), m[7]),
+              radd(rdot(m[8], m[9], m[10], p.x, p.y, p.z), m[11]));
 }
 ALB_DEV float3 affineVector(const float* m, float3 v)
 {
-    return mk(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
-              m[8] * v.x + m[9] * v.y + m[10] * v.z);
+    return mk(rdot(m[0], m[1], m[2], v.x, v.y, v.z), rdot(m[4], m[5], m[6], v.x, v.y, v.z),
+              rdot(m[8], m[9], m[10], v.x, v.y, v.z));
 }
 // Transpose of the linear part times v: how a normal maps under the inverse map.
 ALB_DEV float3 affineTransposedVector(const float* m, float3 v)
@@ -288,6 +362,7 @@ struct TraceState {
     int sp;
     bool found;
     TraceHit hit;
+    std::uint32_t pend; // a BLAS leaf reached and postponed (kLoopSpeculative), or kNoPrim
 };
 
 // What a traversal step leaves to do next.
@@ -307,6 +382,7 @@ ALB_DEV bool traceBegin(const DevScene& s, TraceState& q, float3 origin, float3 
     q.found = false;
     q.sp = 0;
     q.inst_pos = kNoPrim;
+    q.pend = kNoPrim;
     q.ref = s.tlas_root;
     if (s.tlas_root == kEmptyChild) {
         return false;
@@ -369,30 +445,35 @@ __device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, Stack*
                                         unsigned int* error_flag, TraversalCounts* counts)
 {
     const float4* np = reinterpret_cast<const float4*>(s.nodes + q.ref);
-    const float4 lx = __ldg(np);
-    const float4 hx = __ldg(np + 1);
-    const float4 ly = __ldg(np + 2);
-    const float4 hy = __ldg(np + 3);
-    const float4 lz = __ldg(np + 4);
-    const float4 hz = __ldg(np + 5);
     const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
     const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
     const int present = static_cast<int>(meta.z);
     const TravRay& r = q.r;
     if (counts != nullptr) {
         counts->boxes += static_cast<unsigned>(present);
-        countReferenceBoxes(lx, hx, ly, hy, lz, hz, meta.w, r, q.tmin, q.tmax, *counts);
+        countReferenceBoxes(__ldg(np), __ldg(np + 1), __ldg(np + 2), __ldg(np + 3), __ldg(np + 4), __ldg(np + 5),
+                            meta.w, r, q.tmin, q.tmax, *counts);
     }
     float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f, e3 = 0.0f;
-    unsigned mask = slabTest(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, r, q.tmin, q.tmax, e0) ? 1u : 0u;
-    if (present > 1 && slabTest(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, r, q.tmin, q.tmax, e1)) {
-        mask |= 2u;
-    }
-    if (present > 2 && slabTest(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, r, q.tmin, q.tmax, e2)) {
-        mask |= 4u;
-    }
-    if (present > 3 && slabTest(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, r, q.tmin, q.tmax, e3)) {
-        mask |= 8u;
+    unsigned mask;
+    {
+        // Near and far planes per axis by the sign of the inverse direction:
+        // axis a's lo array is np[2a], its hi array np[2a + 1].
+        const unsigned sx = r.planes & 1u;
+        const unsigned sy = (r.planes >> 1) & 1u;
+        const unsigned sz = (r.planes >> 2) & 1u;
+        const float4 nx = __ldg(np + sx);
+        const float4 fx = __ldg(np + (1u - sx));
+        const float4 ny = __ldg(np + 2u + sy);
+        const float4 fy = __ldg(np + (3u - sy));
+        const float4 nz = __ldg(np + 4u + sz);
+        const float4 fz = __ldg(np + (5u - sz));
+        mask = (slabTestOrdered(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, r, q.tmin, q.tmax, e0) ? 1u : 0u) |
+               (slabTestOrdered(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, r, q.tmin, q.tmax, e1) ? 2u : 0u) |
+               (slabTestOrdered(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, r, q.tmin, q.tmax, e2) ? 4u : 0u) |
+               (slabTestOrdered(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, r, q.tmin, q.tmax, e3) ? 8u : 0u);
+        // Absent children (zero boxes) are tested too and masked off here.
+        mask &= (1u << present) - 1u;
     }
     if (mask == 0u) {
         return kStepPop;
@@ -486,7 +567,7 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
                 if (counts != nullptr) {
                     counts->spheres += 1;
                 }
-                h = intersectSphere(q.r, s.spheres[obj.index], obj.kind == kObjSphereWide, q.tmin, q.tmax, mode, t);
+                h = intersectSphere(q.r, q.dir, s.spheres[obj.index], obj.kind == kObjSphereWide, q.tmin, q.tmax, mode, t);
             }
             if (h) {
                 q.found = true;
@@ -569,14 +650,47 @@ __device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, in
 
 // One turn of a query in a persistent kernel; returns whether the query has more
 // work (false: finished). LOOP picks how much a turn does (the wavefront's
-// autotuner chooses per workload; both visit the same nodes and leaves in the
-// same order):
+// autotuner chooses per workload; all visit the leaves in the same order and
+// give the same hits):
 //   kLoopNodesThenLeaf  descend through interior nodes, then handle the leaf
 //                       reached, so the lanes of a warp move through each phase
 //                       together;
 //   kLoopOneStep        one node or one leaf, so lanes return to take new rays
-//                       sooner.
-enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1 };
+//                       sooner;
+//   kLoopSpeculative    descend through interior nodes, continuing past boxes
+//                       missed, and a closest-hit query that reaches a leaf of a
+//                       mesh while its next stack entry is an interior node keeps
+//                       (postpones) that leaf and goes on descending, until it
+//                       reaches a second leaf or has no interior node left; then
+//                       it handles the postponed leaf. The lanes of a warp then
+//                       spend the descent phase descending rather than waiting
+//                       (Aila and Laine, "Understanding the Efficiency of Ray
+//                       Traversal on GPUs", HPG 2009, speculative traversal).
+//                       Leaves are still handled in the order they are reached;
+//                       nodes descended past a postponed leaf are tested with the
+//                       distance bound from before it, so at most more nodes are
+//                       visited and the hits are the same.
+enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1, kLoopSpeculative = 2 };
+
+__device__ __forceinline__ std::uint32_t entryRef(uint2 e) { return e.x; }
+__device__ __forceinline__ std::uint32_t entryRef(unsigned e) { return e; }
+
+// Whether the stack's top entry is an interior node (not a leaf, not an
+// instance's exit marker), and if so pops it into `ref`.
+template <typename Stack>
+__device__ __forceinline__ bool popInteriorNode(TraceState& q, const Stack* stack, int stride)
+{
+    if (q.sp == 0) {
+        return false;
+    }
+    const std::uint32_t top = entryRef(stack[(q.sp - 1) * stride]);
+    if ((top & kLeafBit) != 0u || top == kExitMarker) {
+        return false;
+    }
+    --q.sp;
+    q.ref = top;
+    return true;
+}
 
 template <int LOOP, typename Stack>
 __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, Stack* stack,
@@ -584,7 +698,57 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
                                              TraversalCounts* counts, bool any)
 {
     int step = kStepDescend;
-    if constexpr (LOOP == kLoopOneStep) {
+    if constexpr (LOOP == kLoopSpeculative) {
+        // Descent phase: q.ref becomes a leaf to handle, or kNoPrim when a
+        // postponed leaf is to be handled before anything else.
+        for (;;) {
+            if ((q.ref & kLeafBit) == 0u) {
+                step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
+                if (step == kStepDescend) {
+                    continue;
+                }
+                if (step == kStepFinished) {
+                    return false;
+                }
+                if (q.pend != kNoPrim) {
+                    if (popInteriorNode(q, stack, stride)) {
+                        continue;
+                    }
+                    q.ref = kNoPrim;
+                    break;
+                }
+                if (!popNext(q, stack, stride)) {
+                    return false;
+                }
+                continue;
+            }
+            if (!any && q.pend == kNoPrim && q.inst_pos != kNoPrim) {
+                const std::uint32_t leaf = q.ref;
+                if (popInteriorNode(q, stack, stride)) {
+                    q.pend = leaf;
+                    continue;
+                }
+            }
+            break;
+        }
+        if (q.pend != kNoPrim) {
+            // The postponed leaf (of the current instance's mesh: no instance is
+            // entered) comes before the leaf the descent stopped at, if any.
+            const std::uint32_t next = q.ref;
+            q.ref = q.pend;
+            q.pend = kNoPrim;
+            step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+            if (step == kStepFinished) {
+                return false;
+            }
+            if (next != kNoPrim) {
+                q.ref = next;
+                return true;
+            }
+            return popNext(q, stack, stride);
+        }
+        step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
+    } else if constexpr (LOOP == kLoopOneStep) {
         step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
                                         : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
     } else {
@@ -607,8 +771,9 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
 // launch, so pushes never exceed `stack_size`. It takes one step (a node or a
 // leaf) per loop turn: inside the megakernel, the nested node/leaf loops of
 // traceAdvance measured 3.4x slower.
+template <typename Stack>
 __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
-                                               const SkipRule& skip, TraceHit& hit, uint2* stack, int stride,
+                                               const SkipRule& skip, TraceHit& hit, Stack* stack, int stride,
                                                int stack_size, unsigned int* error_flag, TraversalCounts* counts,
                                                bool any)
 {
@@ -641,10 +806,10 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
 // keeps the kernels that call it small enough for the instruction cache. COUNT
 // selects the copy that counts work (the counting kernels); the timed kernels'
 // copy has no counting code at all.
-template <bool COUNT>
+template <bool COUNT, typename Stack>
 static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
                                                         float& tmax, const SkipRule& skip, TraceHit& hit,
-                                                        uint2* stack, int stride, int stack_size,
+                                                        Stack* stack, int stride, int stack_size,
                                                         unsigned int* error_flag, TraversalCounts* counts, bool any)
 {
     return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
@@ -657,9 +822,9 @@ static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float
 // it, but a larger kernel. Which is faster depends on the scene (the
 // megakernel's autotuner picks). COUNT adds the work counts into `counts`;
 // without it `counts` is ignored.
-template <bool INLINE = false, bool COUNT = false>
+template <bool INLINE = false, bool COUNT = false, typename Stack>
 ALB_DEV bool traceQuery(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
-                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
+                        TraceHit& hit, Stack* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts, bool any)
 {
     if constexpr (INLINE) {
@@ -671,9 +836,9 @@ ALB_DEV bool traceQuery(const DevScene& s, float3 origin, float3 dir, float tmin
     }
 }
 
-template <bool ANY, bool INLINE = false, bool COUNT = false>
+template <bool ANY, bool INLINE = false, bool COUNT = false, typename Stack>
 ALB_DEV bool traceScene(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax, const SkipRule& skip,
-                        TraceHit& hit, uint2* stack, int stride, int stack_size, unsigned int* error_flag,
+                        TraceHit& hit, Stack* stack, int stride, int stack_size, unsigned int* error_flag,
                         TraversalCounts* counts = nullptr)
 {
     return traceQuery<INLINE, COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,

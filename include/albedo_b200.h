@@ -322,7 +322,8 @@ int albedo_wavefront_configure(int32_t slot_count, int32_t blocks_per_sm, int32_
  * Images do not depend on the shape. Synchronous. */
 typedef struct albedo_tuning {
     int32_t tile_width;           /* megakernel: pixel tile width (8, 16 or 32; 128-pixel tiles) */
-    int32_t blocks_per_sm;        /* megakernel: register budget (3 or 4 resident blocks per SM);
+    int32_t blocks_per_sm;        /* megakernel: register budget (3 or 4 resident blocks per SM; at 4
+                                     the path estimator keeps each path's state in shared memory);
                                      wavefront: blocks per SM of the queue kernels */
     int32_t trace_blocks_per_sm;  /* wavefront: persistent traversal blocks per SM */
     int32_t fetch_batch;          /* wavefront: queue entries a traversal warp claims at once */
@@ -332,9 +333,11 @@ typedef struct albedo_tuning {
     int32_t inline_traversal;     /* megakernel: 0 = one out-of-line traversal copy serves both queries,
                                      1 = both queries' traversal inlined into the kernel, 2 = the
                                      closest-hit query's inlined and the shadow query's out of line
-                                     (1 and 2: 3 blocks per SM, path estimator) */
+                                     (path estimator; 2 at 3 blocks per SM only) */
     int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
-                                     1 = a turn is one node or one leaf (same steps, same results) */
+                                     1 = a turn is one node or one leaf, 2 = a turn descends past a
+                                     reached mesh leaf, postponed, to the next (same leaf order, same
+                                     results) */
     int32_t ray_sort;             /* wavefront: 1 = the rays of each bounce are binned by job, direction
                                      octant and origin cell before they are traced, 2 = the shadow rays
                                      too (same results) */
@@ -343,9 +346,9 @@ typedef struct albedo_tuning {
 } albedo_tuning;
 /* Tunes the megakernel for `scene` on `job` and keeps the result in the scene:
  * every tile width with every kernel variant (3 or 4 blocks per SM with an
- * out-of-line traversal; or 3 with the traversal inlined for both queries, or
- * for the closest-hit query only, which are faster on some scenes and slower
- * on others). */
+ * out-of-line traversal; 3 or 4 with the traversal inlined for both queries;
+ * or 3 with it inlined for the closest-hit query only: which is fastest
+ * depends on the scene). */
 int albedo_autotune_megakernel(albedo_scene* scene, const albedo_render_job* job, albedo_tuning* out);
 /* Tunes the wavefront engine on a batch (coordinate descent over traversal
  * blocks per SM, fetch batch, traversal turn shape, queue-kernel blocks per SM,
@@ -357,10 +360,10 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
 int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
 /* Pins a shape, as the autotuner would keep it: the scene's megakernel shape
  * (scene not NULL: tile_width 8, 16 or 32, blocks_per_sm 3 or 4, and
- * inline_traversal 0, 1 or 2, the last two with 3 blocks per SM) or the
+ * inline_traversal 0, 1 or 2, the last with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive, and
- * trace_loop 0 or 1, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the
+ * trace_loop 0, 1 or 2, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the
  * shape. */
 int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */
@@ -415,7 +418,8 @@ int albedo_probe_read_sweep(const void* data, int64_t bytes, int32_t repeats, in
                             void* stream);
 /* Closest-hit (any = 0) or any-hit queries of given rays, traced as the
  * wavefront's persistent kernels trace them (persistent = 1: a turn descends
- * nodes then handles a leaf; 2: a turn is one step) or one query per thread
+ * nodes then handles a leaf; 2: a turn is one step; 3: speculative turns that
+ * postpone a mesh leaf while interior nodes remain) or one query per thread
  * through the shared traversal (persistent = 0): raw hit flag, FP32 t
  * bits, object leaf position and triangle table position (0xFFFFFFFF if none),
  * so that tests can compare the two ways bit for bit. */

@@ -328,12 +328,13 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
     for tile in (8, 32, 16):
         ab.set_tuning(scene, tile_width=tile, blocks_per_sm=3)
         np.testing.assert_array_equal(render(scene, job), base)
-    # The inlined traversal is the same source in another kernel; the compiler may
-    # fuse multiply-adds differently there, so it agrees within the tolerance
-    # used between kernel variants (sample counts identical, image sum within
-    # 1e-4, at most 0.5% of pixels beyond 1e-3 relative), not bit for bit.
-    for mode in (1, 2):
-        ab.set_tuning(scene, tile_width=16, blocks_per_sm=3, inline_traversal=mode)
+    # The inlined traversal, and the 4-blocks/SM kernels with the path's state in
+    # shared memory, are the same source in other kernels; the compiler may fuse
+    # multiply-adds differently there, so they agree within the tolerance used
+    # between kernel variants (sample counts identical, image sum within 1e-4, at
+    # most 0.5% of pixels beyond 1e-3 relative), not bit for bit.
+    for blocks, mode in ((3, 1), (3, 2), (4, 0), (4, 1)):
+        ab.set_tuning(scene, tile_width=16, blocks_per_sm=blocks, inline_traversal=mode)
         inlined = render(scene, job)
         np.testing.assert_array_equal(inlined[:, 3], base[:, 3])
         assert abs(inlined[:, :3].sum() - base[:, :3].sum()) / base[:, :3].sum() < 1e-4
@@ -351,11 +352,13 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
                   dict(blocks_per_sm=8, trace_blocks_per_sm=5, fetch_batch=32, iterations_per_graph=4,
                        slot_count=1 << 16, trace_loop=1, ray_sort=1),
                   dict(blocks_per_sm=8, trace_blocks_per_sm=3, fetch_batch=64, iterations_per_graph=4,
-                       slot_count=1 << 20, trace_loop=0, ray_sort=2)):
+                       slot_count=1 << 20, trace_loop=0, ray_sort=2),
+                  dict(blocks_per_sm=8, trace_blocks_per_sm=5, fetch_batch=16, iterations_per_graph=4,
+                       slot_count=1 << 18, trace_loop=2)):
         ab.set_tuning(**shape)
         np.testing.assert_array_equal(render(scene, wave_job), wave)
     ab.wavefront_configure()
     with pytest.raises(ValueError):
         ab.set_tuning(scene, tile_width=12, blocks_per_sm=3)
     with pytest.raises(ValueError):
-        ab.set_tuning(scene, tile_width=16, blocks_per_sm=4, inline_traversal=1)
+        ab.set_tuning(scene, tile_width=16, blocks_per_sm=4, inline_traversal=2)
