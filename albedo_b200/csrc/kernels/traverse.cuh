@@ -362,7 +362,6 @@ struct TraceState {
     int sp;
     bool found;
     TraceHit hit;
-    std::uint32_t pend; // a BLAS leaf reached and postponed (kLoopSpeculative), or kNoPrim
 };
 
 // What a traversal step leaves to do next.
@@ -382,7 +381,6 @@ ALB_DEV bool traceBegin(const DevScene& s, TraceState& q, float3 origin, float3 
     q.found = false;
     q.sp = 0;
     q.inst_pos = kNoPrim;
-    q.pend = kNoPrim;
     q.ref = s.tlas_root;
     if (s.tlas_root == kEmptyChild) {
         return false;
@@ -650,47 +648,14 @@ __device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, in
 
 // One turn of a query in a persistent kernel; returns whether the query has more
 // work (false: finished). LOOP picks how much a turn does (the wavefront's
-// autotuner chooses per workload; all visit the leaves in the same order and
-// give the same hits):
+// autotuner chooses per workload; both visit the same nodes and leaves in the
+// same order):
 //   kLoopNodesThenLeaf  descend through interior nodes, then handle the leaf
 //                       reached, so the lanes of a warp move through each phase
 //                       together;
 //   kLoopOneStep        one node or one leaf, so lanes return to take new rays
-//                       sooner;
-//   kLoopSpeculative    descend through interior nodes, continuing past boxes
-//                       missed, and a closest-hit query that reaches a leaf of a
-//                       mesh while its next stack entry is an interior node keeps
-//                       (postpones) that leaf and goes on descending, until it
-//                       reaches a second leaf or has no interior node left; then
-//                       it handles the postponed leaf. The lanes of a warp then
-//                       spend the descent phase descending rather than waiting
-//                       (Aila and Laine, "Understanding the Efficiency of Ray
-//                       Traversal on GPUs", HPG 2009, speculative traversal).
-//                       Leaves are still handled in the order they are reached;
-//                       nodes descended past a postponed leaf are tested with the
-//                       distance bound from before it, so at most more nodes are
-//                       visited and the hits are the same.
-enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1, kLoopSpeculative = 2 };
-
-__device__ __forceinline__ std::uint32_t entryRef(uint2 e) { return e.x; }
-__device__ __forceinline__ std::uint32_t entryRef(unsigned e) { return e; }
-
-// Whether the stack's top entry is an interior node (not a leaf, not an
-// instance's exit marker), and if so pops it into `ref`.
-template <typename Stack>
-__device__ __forceinline__ bool popInteriorNode(TraceState& q, const Stack* stack, int stride)
-{
-    if (q.sp == 0) {
-        return false;
-    }
-    const std::uint32_t top = entryRef(stack[(q.sp - 1) * stride]);
-    if ((top & kLeafBit) != 0u || top == kExitMarker) {
-        return false;
-    }
-    --q.sp;
-    q.ref = top;
-    return true;
-}
+//                       sooner.
+enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1 };
 
 template <int LOOP, typename Stack>
 __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, Stack* stack,
@@ -698,57 +663,7 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
                                              TraversalCounts* counts, bool any)
 {
     int step = kStepDescend;
-    if constexpr (LOOP == kLoopSpeculative) {
-        // Descent phase: q.ref becomes a leaf to handle, or kNoPrim when a
-        // postponed leaf is to be handled before anything else.
-        for (;;) {
-            if ((q.ref & kLeafBit) == 0u) {
-                step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
-                if (step == kStepDescend) {
-                    continue;
-                }
-                if (step == kStepFinished) {
-                    return false;
-                }
-                if (q.pend != kNoPrim) {
-                    if (popInteriorNode(q, stack, stride)) {
-                        continue;
-                    }
-                    q.ref = kNoPrim;
-                    break;
-                }
-                if (!popNext(q, stack, stride)) {
-                    return false;
-                }
-                continue;
-            }
-            if (!any && q.pend == kNoPrim && q.inst_pos != kNoPrim) {
-                const std::uint32_t leaf = q.ref;
-                if (popInteriorNode(q, stack, stride)) {
-                    q.pend = leaf;
-                    continue;
-                }
-            }
-            break;
-        }
-        if (q.pend != kNoPrim) {
-            // The postponed leaf (of the current instance's mesh: no instance is
-            // entered) comes before the leaf the descent stopped at, if any.
-            const std::uint32_t next = q.ref;
-            q.ref = q.pend;
-            q.pend = kNoPrim;
-            step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
-            if (step == kStepFinished) {
-                return false;
-            }
-            if (next != kNoPrim) {
-                q.ref = next;
-                return true;
-            }
-            return popNext(q, stack, stride);
-        }
-        step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
-    } else if constexpr (LOOP == kLoopOneStep) {
+    if constexpr (LOOP == kLoopOneStep) {
         step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
                                         : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
     } else {

@@ -645,10 +645,7 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const
         }
         bool more = false;
         if (active) {
-            if (mode == 3) {
-                more = traceAdvance<kLoopSpeculative>(scene, q, SkipRule::none(), lane_refs, stride, STACK,
-                                                      error_flag, nullptr, any);
-            } else if (mode == 2) {
+            if (mode == 2) {
                 more = traceAdvance<kLoopOneStep>(scene, q, SkipRule::none(), lane_refs, stride, STACK, error_flag,
                                                   nullptr, any);
             } else {
@@ -698,13 +695,7 @@ cudaError_t wfPrepare(int stack)
         if (e == cudaSuccess) {
             e = allowStackMemory(extendKernel<S, kLoopOneStep>, S, kRef);
         }
-        if (e == cudaSuccess) {
-            e = allowStackMemory(shadowKernel<S, kLoopOneStep>, S, kRef);
-        }
-        if (e == cudaSuccess) {
-            e = allowStackMemory(extendKernel<S, kLoopSpeculative>, S, kRef);
-        }
-        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S, kLoopSpeculative>, S, kRef);
+        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S, kLoopOneStep>, S, kRef);
     });
 }
 
@@ -763,8 +754,6 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         constexpr int S = decltype(size)::value;
         if (launch.trace_loop == kLoopOneStep) {
             extendKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
-        } else if (launch.trace_loop == kLoopSpeculative) {
-            extendKernel<S, kLoopSpeculative><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         } else {
             extendKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         }
@@ -810,9 +799,6 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         if (launch.trace_loop == kLoopOneStep) {
             shadowKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
                                                                            binned_shadows);
-        } else if (launch.trace_loop == kLoopSpeculative) {
-            shadowKernel<S, kLoopSpeculative><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
-                                                                               binned_shadows);
         } else {
             shadowKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
                                                                                  binned_shadows);

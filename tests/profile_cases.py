@@ -8,7 +8,7 @@
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
 --scene icosphere6 or icosphere8 (displaced icospheres of 6 and 8 levels, 81,920 and
 1,310,720 triangles), max depth 10 (16 for icosphere8, as the bench frame), seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
-nodes then leaf, 1: one step, 2: speculative), --ray-sort its ray binning. With --autotune the launch shape is tuned first (as bench.py
+nodes then leaf, 1: one step), --ray-sort its ray binning. With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
 for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel). `resolve` resolves
@@ -41,7 +41,7 @@ def main() -> None:
     parser.add_argument("--autotune", action="store_true")
     parser.add_argument("--scene", choices=["trefoil", "icosphere6", "icosphere8"], default="trefoil")
     parser.add_argument("--depth", type=int, default=None, help="max depth (default 10; 16 for icosphere8)")
-    parser.add_argument("--trace-loop", type=int, choices=[0, 1, 2], default=None)
+    parser.add_argument("--trace-loop", type=int, choices=[0, 1], default=None)
     parser.add_argument("--ray-sort", type=int, choices=[0, 1, 2], default=None,
                         help="wavefront: pin ray binning (0 none, 1 extension rays, 2 shadow rays too)")
     parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
