@@ -513,9 +513,16 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
 {
     const std::uint32_t first = q.ref & kLeafFirstMask;
     const std::uint32_t count = ((q.ref >> 28) & 7u) + 1u;
-    if (q.inst_pos == kNoPrim) {
-        for (std::uint32_t k = 0; k < count; ++k) {
-            const std::uint32_t pos = first + k;
+    const bool in_mesh = q.inst_pos != kNoPrim;
+    // One loop and one triangle test serve TLAS leaves (spheres, scene
+    // triangles, instances) and mesh leaves (the current instance's triangles),
+    // which keeps the traversal's code small.
+    for (std::uint32_t k = 0; k < count; ++k) {
+        const std::uint32_t pos = first + k;
+        int kind = kObjTriangle;
+        std::uint32_t index = pos;
+        int mode = kSphereTestBoth;
+        if (!in_mesh) {
             const DevObject obj = s.objects[pos];
             if (pos == skip.light_object_pos) {
                 continue;
@@ -541,61 +548,39 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
                 q.ref = inst.root;
                 return kStepDescend;
             }
-            float t;
-            float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
-            bool h;
-            if (obj.kind == kObjTriangle) {
-                if (pos == skip.object_pos) {
+            kind = static_cast<int>(obj.kind);
+            index = obj.index;
+            if (pos == skip.object_pos) {
+                if (kind == kObjTriangle || skip.sphere_mode == kSphereSkipAll) {
                     continue;
                 }
-                const float4* tp = reinterpret_cast<const float4*>(s.triangles + obj.index);
-                if (counts != nullptr) {
-                    counts->triangles += 1;
-                }
-                h = q.r.usable &&
-                    intersectTriangle(q.r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q.tmin, q.tmax, t, b0, b1, b2);
-            } else {
-                int mode = kSphereTestBoth;
-                if (pos == skip.object_pos) {
-                    if (skip.sphere_mode == kSphereSkipAll) {
-                        continue;
-                    }
-                    mode = skip.sphere_mode;
-                }
-                if (counts != nullptr) {
-                    counts->spheres += 1;
-                }
-                h = intersectSphere(q.r, q.dir, s.spheres[obj.index], obj.kind == kObjSphereWide, q.tmin, q.tmax, mode, t);
+                mode = skip.sphere_mode;
             }
-            if (h) {
-                q.found = true;
-                q.tmax = t;
-                q.hit = {t, pos, obj.kind == kObjTriangle ? obj.index : kNoPrim, b0, b1, b2};
-                if (any) {
-                    return kStepFinished;
-                }
-            }
+        } else if (pos == skip.tri_pos && q.inst_pos == skip.object_pos) {
+            continue;
         }
-        return kStepPop;
-    }
-    if (q.r.usable) {
-        for (std::uint32_t k = 0; k < count; ++k) {
-            const std::uint32_t pos = first + k;
-            if (pos == skip.tri_pos && q.inst_pos == skip.object_pos) {
-                continue;
-            }
-            const float4* tp = reinterpret_cast<const float4*>(s.triangles + pos);
-            float t, b0, b1, b2;
-            if (counts != nullptr) {
+        float t;
+        float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;
+        bool h;
+        if (kind == kObjTriangle) {
+            const float4* tp = reinterpret_cast<const float4*>(s.triangles + index);
+            if (counts != nullptr && (!in_mesh || q.r.usable)) {
                 counts->triangles += 1;
             }
-            if (intersectTriangle(q.r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q.tmin, q.tmax, t, b0, b1, b2)) {
-                q.found = true;
-                q.tmax = t;
-                q.hit = {t, q.inst_pos, pos, b0, b1, b2};
-                if (any) {
-                    return kStepFinished;
-                }
+            h = q.r.usable &&
+                intersectTriangle(q.r, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), q.tmin, q.tmax, t, b0, b1, b2);
+        } else {
+            if (counts != nullptr) {
+                counts->spheres += 1;
+            }
+            h = intersectSphere(q.r, q.dir, s.spheres[index], kind == kObjSphereWide, q.tmin, q.tmax, mode, t);
+        }
+        if (h) {
+            q.found = true;
+            q.tmax = t;
+            q.hit = {t, in_mesh ? q.inst_pos : pos, kind == kObjTriangle ? index : kNoPrim, b0, b1, b2};
+            if (any) {
+                return kStepFinished;
             }
         }
     }
