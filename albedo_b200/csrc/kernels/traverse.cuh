@@ -129,8 +129,10 @@ ALB_DEV bool slabTest(float lox, float hix, float loy, float hiy, float loz, flo
     return lo <= hi;
 }
 
-// Three-input FP32 maximum and minimum (one instruction each on sm_100a). With
-// no NaN operand they are the plain maximum and minimum.
+// Three-input FP32 maximum and minimum (one instruction each on sm_100a). A NaN
+// operand is skipped as the two-input fmaxf/fminf chain skips it (checked on a
+// B200 against that chain over every triple of NaN, infinities, signed zeros,
+// a subnormal and ordinary values).
 __device__ __forceinline__ float max3f(float a, float b, float c)
 {
     float d;
@@ -361,7 +363,25 @@ struct TraceState {
     std::uint32_t inst_pos; // TLAS leaf position of the instance being traversed, or kNoPrim
     int sp;
     bool found;
+    // The ray changes space (entering or leaving an instance): r.o and r.inv
+    // hold the new origin and direction, and the next step sets the ray up from
+    // them. One set-up site keeps the traversal's code small.
+    bool resetup;
     TraceHit hit;
+
+    ALB_DEV void changeSpace(float3 o, float3 d)
+    {
+        r.o = o;
+        r.inv = d;
+        resetup = true;
+    }
+    ALB_DEV void settle()
+    {
+        if (resetup) {
+            r.setup(r.o, r.inv);
+            resetup = false;
+        }
+    }
 };
 
 // What a traversal step leaves to do next.
@@ -379,6 +399,7 @@ ALB_DEV bool traceBegin(const DevScene& s, TraceState& q, float3 origin, float3 
     q.tmin = tmin;
     q.tmax = tmax;
     q.found = false;
+    q.resetup = false;
     q.sp = 0;
     q.inst_pos = kNoPrim;
     q.ref = s.tlas_root;
@@ -543,7 +564,7 @@ __device__ __forceinline__ int leafStep(const DevScene& s, TraceState& q, const 
                     counts->instances += 1;
                     counts->reference_boxes += 1; // the BLAS root
                 }
-                q.r.setup(affinePoint(inst.to_object, q.origin), affineVector(inst.to_object, q.dir));
+                q.changeSpace(affinePoint(inst.to_object, q.origin), affineVector(inst.to_object, q.dir));
                 q.inst_pos = pos;
                 q.ref = inst.root;
                 return kStepDescend;
@@ -599,7 +620,7 @@ __device__ __forceinline__ bool popNext(TraceState& q, const uint2* stack, int s
         --q.sp;
         const uint2 e = stack[q.sp * stride];
         if (e.x == kExitMarker) {
-            q.r.setup(q.origin, q.dir);
+            q.changeSpace(q.origin, q.dir);
             q.inst_pos = kNoPrim;
             continue;
         }
@@ -622,7 +643,7 @@ __device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, in
         --q.sp;
         const unsigned ref = stack[q.sp * stride];
         if (ref == kExitMarker) {
-            q.r.setup(q.origin, q.dir);
+            q.changeSpace(q.origin, q.dir);
             q.inst_pos = kNoPrim;
             continue;
         }
@@ -647,6 +668,7 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
                                              int stride, int stack_size, unsigned int* error_flag,
                                              TraversalCounts* counts, bool any)
 {
+    q.settle();
     int step = kStepDescend;
     if constexpr (LOOP == kLoopOneStep) {
         step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
@@ -688,6 +710,7 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
         counts->reference_boxes += 1; // the TLAS root
     }
     for (;;) {
+        q.settle();
         const int step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
                                                   : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts,
                                                              any);
