@@ -1221,7 +1221,7 @@ int albedo_autotune_batch(const albedo_batch_item* items, int32_t count, albedo_
         TuneTimer timer;
         const std::vector<TuneKnob> knobs{{"trace_blocks_per_sm", {3, 4, 5}},
                                           {"fetch_batch", {16, 32, 64, 128}},
-                                          {"trace_loop", {0, 1}},
+                                          {"trace_loop", {0, 1, 2}},
                                           {"blocks_per_sm", {4, 8, 16}},
                                           {"iterations_per_graph", {2, 4, 8}},
                                           {"slot_count", {1 << 17, 1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22}},
@@ -1301,8 +1301,8 @@ int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape)
             shape->iterations_per_graph <= 0 || shape->slot_count <= 0) {
             throw std::invalid_argument{"wavefront shape values must be positive"};
         }
-        if (shape->trace_loop != 0 && shape->trace_loop != 1) {
-            throw std::invalid_argument{"the traversal turn shape must be 0 or 1"};
+        if (shape->trace_loop < 0 || shape->trace_loop > 2) {
+            throw std::invalid_argument{"the traversal turn shape must be 0, 1 or 2"};
         }
         if (shape->ray_sort < 0 || shape->ray_sort > 2) {
             throw std::invalid_argument{"ray binning must be 0, 1 or 2"};
@@ -1772,8 +1772,8 @@ int albedo_probe_trace_modes(const albedo_scene* scene, const float* rays, int64
         DeviceBuffer obj{n * sizeof(unsigned int)};
         DeviceBuffer tri{n * sizeof(unsigned int)};
         check(cudaMemset(counter.ptr, 0, sizeof(int)), "cudaMemset");
-        if (persistent < 0 || persistent > 2) {
-            throw std::invalid_argument{"persistent must be 0, 1 or 2"};
+        if (persistent < 0 || persistent > 3) {
+            throw std::invalid_argument{"persistent must be 0, 1, 2 or 3"};
         }
         check(launchTraceModes(scene->dev, d_rays.as<float>(), static_cast<int>(count), t_min, t_max, any != 0,
                                persistent, scene->stack_capacity, counter.as<int>(),

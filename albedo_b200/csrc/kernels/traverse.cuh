@@ -660,14 +660,35 @@ __device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, in
 //                       reached, so the lanes of a warp move through each phase
 //                       together;
 //   kLoopOneStep        one node or one leaf, so lanes return to take new rays
-//                       sooner.
-enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1 };
+//                       sooner;
+//   kLoopQuery          the whole query in one turn, through the out-of-line
+//                       traversal (a function of its own: the calling kernel's
+//                       state is saved around the call, and the traversal loop
+//                       has the registers to itself).
+enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1, kLoopQuery = 2 };
+
+template <bool COUNT, typename Stack>
+static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
+                                                        float& tmax, const SkipRule& skip, TraceHit& hit,
+                                                        Stack* stack, int stride, int stack_size,
+                                                        unsigned int* error_flag, TraversalCounts* counts, bool any);
 
 template <int LOOP, typename Stack>
 __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, const SkipRule& skip, Stack* stack,
                                              int stride, int stack_size, unsigned int* error_flag,
                                              TraversalCounts* counts, bool any)
 {
+    if constexpr (LOOP == kLoopQuery) {
+        float tmax = q.tmax;
+        TraceHit hit;
+        q.found = traceSceneOutOfLine<false>(s, q.origin, q.dir, q.tmin, tmax, skip, hit, stack, stride, stack_size,
+                                             error_flag, nullptr, any);
+        if (q.found) {
+            q.tmax = tmax;
+            q.hit = hit;
+        }
+        return false;
+    }
     q.settle();
     int step = kStepDescend;
     if constexpr (LOOP == kLoopOneStep) {

@@ -645,7 +645,10 @@ __global__ void __launch_bounds__(128, kTraceBlocksPerSm) traceModesKernel(const
         }
         bool more = false;
         if (active) {
-            if (mode == 2) {
+            if (mode == 3) {
+                more = traceAdvance<kLoopQuery>(scene, q, SkipRule::none(), lane_refs, stride, STACK, error_flag,
+                                                nullptr, any);
+            } else if (mode == 2) {
                 more = traceAdvance<kLoopOneStep>(scene, q, SkipRule::none(), lane_refs, stride, STACK, error_flag,
                                                   nullptr, any);
             } else {
@@ -695,7 +698,13 @@ cudaError_t wfPrepare(int stack)
         if (e == cudaSuccess) {
             e = allowStackMemory(extendKernel<S, kLoopOneStep>, S, kRef);
         }
-        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S, kLoopOneStep>, S, kRef);
+        if (e == cudaSuccess) {
+            e = allowStackMemory(shadowKernel<S, kLoopOneStep>, S, kRef);
+        }
+        if (e == cudaSuccess) {
+            e = allowStackMemory(extendKernel<S, kLoopQuery>, S, kRef);
+        }
+        return e != cudaSuccess ? e : allowStackMemory(shadowKernel<S, kLoopQuery>, S, kRef);
     });
 }
 
@@ -754,6 +763,8 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         constexpr int S = decltype(size)::value;
         if (launch.trace_loop == kLoopOneStep) {
             extendKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
+        } else if (launch.trace_loop == kLoopQuery) {
+            extendKernel<S, kLoopQuery><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         } else {
             extendKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch, binned);
         }
@@ -799,6 +810,9 @@ cudaError_t wfIteration(const WfJob* jobs, const WfBuffers& b, const WfLaunch& l
         if (launch.trace_loop == kLoopOneStep) {
             shadowKernel<S, kLoopOneStep><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
                                                                            binned_shadows);
+        } else if (launch.trace_loop == kLoopQuery) {
+            shadowKernel<S, kLoopQuery><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
+                                                                         binned_shadows);
         } else {
             shadowKernel<S, kLoopNodesThenLeaf><<<tg, 128, smemFor(S), stream>>>(jobs, b, error_flag, fetch,
                                                                                  binned_shadows);

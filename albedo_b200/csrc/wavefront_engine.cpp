@@ -119,7 +119,7 @@ WavefrontEngine::~WavefrontEngine()
 void WavefrontEngine::setShape(const WfShape& shape)
 {
     if (shape.blocks_per_sm <= 0 || shape.iterations_per_graph <= 0 || shape.trace_blocks_per_sm < 0 ||
-        shape.fetch_batch <= 0 || shape.trace_loop < 0 || shape.trace_loop > 1 || shape.ray_sort < 0 ||
+        shape.fetch_batch <= 0 || shape.trace_loop < 0 || shape.trace_loop > 2 || shape.ray_sort < 0 ||
         shape.ray_sort > 2) {
         throw std::invalid_argument{"wavefront launch shape values must be positive"};
     }

@@ -335,7 +335,8 @@ typedef struct albedo_tuning {
                                      closest-hit query's inlined and the shadow query's out of line
                                      (path estimator; 2 at 3 blocks per SM only) */
     int32_t trace_loop;           /* wavefront: 0 = a traversal turn descends nodes then handles a leaf,
-                                     1 = a turn is one node or one leaf (same steps, same results) */
+                                     1 = a turn is one node or one leaf, 2 = a turn is the whole query
+                                     (out-of-line traversal; same steps, same results) */
     int32_t ray_sort;             /* wavefront: 1 = the rays of each bounce are binned by job, direction
                                      octant and origin cell before they are traced, 2 = the shadow rays
                                      too (same results) */
@@ -361,7 +362,7 @@ int albedo_tuning_get(const albedo_scene* scene, albedo_tuning* out);
  * inline_traversal 0, 1 or 2, the last with 3 blocks per SM) or the
  * process's wavefront shape (scene NULL: blocks_per_sm, trace_blocks_per_sm,
  * fetch_batch, iterations_per_graph and slot_count, all positive, and
- * trace_loop 0 or 1, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the
+ * trace_loop 0, 1 or 2, ray_sort 0, 1 or 2). Timing fields are ignored. Images do not depend on the
  * shape. */
 int albedo_tuning_set(albedo_scene* scene, const albedo_tuning* shape);
 /* Iterations the last wavefront run took. */
@@ -416,7 +417,8 @@ int albedo_probe_read_sweep(const void* data, int64_t bytes, int32_t repeats, in
                             void* stream);
 /* Closest-hit (any = 0) or any-hit queries of given rays, traced as the
  * wavefront's persistent kernels trace them (persistent = 1: a turn descends
- * nodes then handles a leaf; 2: a turn is one step) or one query per thread
+ * nodes then handles a leaf; 2: a turn is one step; 3: a turn is the whole
+ * query, traced by the out-of-line traversal) or one query per thread
  * through the shared traversal (persistent = 0): raw hit flag, FP32 t
  * bits, object leaf position and triangle table position (0xFFFFFFFF if none),
  * so that tests can compare the two ways bit for bit. */

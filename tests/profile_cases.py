@@ -1,14 +1,14 @@
 """Fixed render cases for profiling under ncu: one render, nothing else.
 
     python tests/profile_cases.py megakernel --width 480 --height 270 --spp 64 [--autotune]
-                                   [--accumulation fp64|kahan]
+                                   [--accumulation fp64|kahan] [--mega-shape TILE,BLOCKS,INLINE]
     python tests/profile_cases.py wavefront --width 480 --height 270 --spp 16 [--autotune]
     python tests/profile_cases.py resolve --width 3840 --height 2160
 
 Both use the instanced trefoil scene (albedo_b200.scenes.trefoil_scene) unless
 --scene icosphere6 or icosphere8 (displaced icospheres of 6 and 8 levels, 81,920 and
 1,310,720 triangles), max depth 10 (16 for icosphere8, as the bench frame), seed 0. --trace-loop pins the wavefront traversal's turn shape (0:
-nodes then leaf, 1: one step), --ray-sort its ray binning. With --autotune the launch shape is tuned first (as bench.py
+nodes then leaf, 1: one step, 2: whole query out of line), --ray-sort its ray binning. With --autotune the launch shape is tuned first (as bench.py
 does); a warm-up render precedes the profiled one unless --no-warmup. The case
 prints how many launches of the render kernels come before the profiled render,
 for ncu's `-s` (pass `-k regex:<kernel>` to pick the kernel). `resolve` resolves
@@ -41,9 +41,11 @@ def main() -> None:
     parser.add_argument("--autotune", action="store_true")
     parser.add_argument("--scene", choices=["trefoil", "icosphere6", "icosphere8"], default="trefoil")
     parser.add_argument("--depth", type=int, default=None, help="max depth (default 10; 16 for icosphere8)")
-    parser.add_argument("--trace-loop", type=int, choices=[0, 1], default=None)
+    parser.add_argument("--trace-loop", type=int, choices=[0, 1, 2], default=None)
     parser.add_argument("--ray-sort", type=int, choices=[0, 1, 2], default=None,
                         help="wavefront: pin ray binning (0 none, 1 extension rays, 2 shadow rays too)")
+    parser.add_argument("--mega-shape", default=None,
+                        help="megakernel: pin TILE,BLOCKS,INLINE (tile width, blocks per SM, traversal placement)")
     parser.add_argument("--accumulation", choices=["fp64", "kahan"], default="fp64",
                         help="megakernel per-pixel sums: FP64 or Kahan-compensated FP32")
     args = parser.parse_args()
@@ -77,6 +79,9 @@ def main() -> None:
         acc = torch.zeros((args.width * args.height, 4), dtype=torch.float64, device="cuda")
         before = 0
         shape = None
+        if args.mega_shape is not None and method == ab.MEGAKERNEL:
+            tile, blocks, inline = (int(v) for v in args.mega_shape.split(","))
+            ab.set_tuning(scene, tile_width=tile, blocks_per_sm=blocks, inline_traversal=inline)
         if args.autotune:
             if method == ab.MEGAKERNEL:
                 shape = ab.autotune_megakernel(scene, job)

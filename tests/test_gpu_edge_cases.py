@@ -352,7 +352,9 @@ def test_renders_repeat_and_do_not_depend_on_the_launch_shape(trefoil_path):
                   dict(blocks_per_sm=8, trace_blocks_per_sm=5, fetch_batch=32, iterations_per_graph=4,
                        slot_count=1 << 16, trace_loop=1, ray_sort=1),
                   dict(blocks_per_sm=8, trace_blocks_per_sm=3, fetch_batch=64, iterations_per_graph=4,
-                       slot_count=1 << 20, trace_loop=0, ray_sort=2)):
+                       slot_count=1 << 20, trace_loop=0, ray_sort=2),
+                  dict(blocks_per_sm=8, trace_blocks_per_sm=5, fetch_batch=16, iterations_per_graph=4,
+                       slot_count=1 << 18, trace_loop=2)):
         ab.set_tuning(**shape)
         np.testing.assert_array_equal(render(scene, wave_job), wave)
     ab.wavefront_configure()

@@ -249,11 +249,12 @@ def trace_modes(scene, rays, any_hit, persistent, t_max=float("inf")):
 
 @pytest.mark.parametrize("which", ["room", "trefoil"])
 @pytest.mark.parametrize("any_hit", [False, True])
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_persistent_traversal_equals_the_per_thread_traversal(which, any_hit, mode, room_path, trefoil_path):
     """The wavefront's persistent kernels (warp fetch; a turn descends nodes then
-    handles a leaf, mode 1, or takes one step, mode 2; 4-byte stack entries that
-    keep no entry distance) reach the leaves in the same order as the per-thread
+    handles a leaf, mode 1, takes one step, mode 2, or traces the whole query out
+    of line, mode 3; 4-byte stack entries that keep no entry distance) reach the
+    leaves in the same order as the per-thread
     traversal the ray-query tests compare with the reference, and give the same
     hits: hit flags, FP32 t, object and triangle are identical bit for bit, for
     closest-hit and any-hit queries."""
