@@ -19,7 +19,7 @@ struct WfShape {
     int iterations_per_graph{4};  // iterations captured in one CUDA graph
     int trace_blocks_per_sm{0};   // persistent traversal kernels: blocks per SM, 0 = as many as fit
     int fetch_batch{32};          // queue entries a traversal warp claims at once
-    int trace_loop{0};            // traversal turn shape of the persistent kernels: 0 nodes then leaf, 1 one step,
+    int trace_loop{2};            // traversal turn shape of the persistent kernels: 0 nodes then leaf, 1 one step,
                                   // 2 the whole query through the out-of-line traversal
     int ray_sort{0};              // 1: bin each bounce's rays by coherence before they are traced; 2: the
                                   // shadow rays too
