@@ -405,9 +405,9 @@ def large_forms(scene, scene_path: Path, frame: Frame, flush, fp64_image, steps:
 
 
 def soup_form(tmp: Path, flush) -> dict:
-    """The 1M-triangle random soup at the large frame: megakernel (tuned on a
-    quarter of the frame) and wavefront (with the shape tuned on the icosphere
-    frame), one step each, and their errors against the FP64 oracle."""
+    """The 1M-triangle random soup at the large frame: megakernel and wavefront,
+    each tuned on the frame, one step each, and their errors against the FP64
+    oracle."""
     import torch
 
     import albedo_b200 as ab
@@ -423,13 +423,11 @@ def soup_form(tmp: Path, flush) -> dict:
         job = render_job(SOUP, method)
         acc = torch.zeros((SOUP.width * SOUP.height, 4), dtype=torch.float64, device="cuda")
         if method == ab.MEGAKERNEL:
-            # Tuned on a quarter of the frame (the 1920x1080 frame takes 7 s here).
-            quarter = ab.RenderJob(SOUP.width // 2, SOUP.height // 2, samples_per_axis=SOUP.samples_per_axis,
-                                   seed=SEED, max_depth=SOUP.max_depth, roulette_start=ROULETTE_START)
-            out["megakernel_autotune"] = ab.autotune_megakernel(scene, quarter)
+            # Tuned on the frame itself (the tuner renders it at a quarter of its samples).
+            out["megakernel_autotune"] = ab.autotune_megakernel(scene, job)
         else:
-            # The wavefront keeps the shape tuned on the icosphere frame.
-            out["wavefront_shape"] = ab.tuning()
+            # Tuned on the frame itself, as the megakernel.
+            out["wavefront_autotune"] = ab.autotune_batch([(scene, job, acc.data_ptr())])
         ms = timed_frames(scene, job, acc, flush, 1)
         out[label] = {"mpaths_per_s": SOUP.paths / (ms[0] / 1e3) / 1e6, "ms_per_frame": ms[0]}
         images[label] = acc.cpu().numpy()
