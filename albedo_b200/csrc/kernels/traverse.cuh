@@ -163,9 +163,11 @@ __device__ __forceinline__ float min3f(float a, float b, float c)
 //   - An infinite inverse (a zero or subnormal direction component) gives the
 //     clip's answer on that axis too, with one exception: for a -infinite
 //     inverse and an origin lying exactly on one of the slab's two planes (not
-//     both), the clip's NaN, left in place by its swap rule, rejects the box,
-//     and this test enters it. Entering a box more can only add primitive tests,
-//     never lose a hit.
+//     both), the clip's NaN, left in place by its swap rule, rejects the box
+//     (or, over an unbounded range, enters it at +infinity), and this test
+//     enters it at the other axes' entry. Entering a box more can only add
+//     primitive tests, never lose a hit. (Checked on the host over 8 M rays,
+//     tests/cpp/box_test.cpp.)
 // The four children of a node test independently.
 __device__ __forceinline__ bool slabTestOrdered(float nx, float fx, float ny, float fy, float nz, float fz,
                                                 const TravRay& r, float tmin, float tmax, float& entry)
