@@ -462,10 +462,10 @@ __device__ __forceinline__ void pushEntry(unsigned* slot, std::uint32_t ref, flo
 // reference reaches first and pushes the other hit children, last first, so
 // leaves are reached in the reference's depth-first near-first order.
 template <typename Stack>
-__device__ __forceinline__ int nodeStep(const DevScene& s, TraceState& q, Stack* stack, int stride, int stack_size,
-                                        unsigned int* error_flag, TraversalCounts* counts)
+__device__ __forceinline__ int nodeStep(const DevNode* nodes, TraceState& q, Stack* stack, int stride,
+                                        int stack_size, unsigned int* error_flag, TraversalCounts* counts)
 {
-    const float4* np = reinterpret_cast<const float4*>(s.nodes + q.ref);
+    const float4* np = reinterpret_cast<const float4*>(nodes + q.ref);
     const uint4 ch = __ldg(reinterpret_cast<const uint4*>(np + 6));
     const uint4 meta = __ldg(reinterpret_cast<const uint4*>(np + 7));
     const int present = static_cast<int>(meta.z);
@@ -669,7 +669,7 @@ __device__ __forceinline__ bool popNext(TraceState& q, const unsigned* stack, in
 //                       has the registers to itself).
 enum TraceLoop : int { kLoopNodesThenLeaf = 0, kLoopOneStep = 1, kLoopQuery = 2 };
 
-template <bool COUNT, typename Stack>
+template <bool COUNT, bool HOLD, typename Stack>
 static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
                                                         float& tmax, const SkipRule& skip, TraceHit& hit,
                                                         Stack* stack, int stride, int stack_size,
@@ -683,8 +683,8 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
     if constexpr (LOOP == kLoopQuery) {
         float tmax = q.tmax;
         TraceHit hit;
-        q.found = traceSceneOutOfLine<false>(s, q.origin, q.dir, q.tmin, tmax, skip, hit, stack, stride, stack_size,
-                                             error_flag, nullptr, any);
+        q.found = traceSceneOutOfLine<false, false>(s, q.origin, q.dir, q.tmin, tmax, skip, hit, stack, stride,
+                                                    stack_size, error_flag, nullptr, any);
         if (q.found) {
             q.tmax = tmax;
             q.hit = hit;
@@ -694,11 +694,11 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
     q.settle();
     int step = kStepDescend;
     if constexpr (LOOP == kLoopOneStep) {
-        step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
+        step = (q.ref & kLeafBit) == 0u ? nodeStep(s.nodes, q, stack, stride, stack_size, error_flag, counts)
                                         : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
     } else {
         while (step == kStepDescend && (q.ref & kLeafBit) == 0u) {
-            step = nodeStep(s, q, stack, stride, stack_size, error_flag, counts);
+            step = nodeStep(s.nodes, q, stack, stride, stack_size, error_flag, counts);
         }
         if (step == kStepDescend) {
             step = leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
@@ -716,7 +716,15 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
 // launch, so pushes never exceed `stack_size`. It takes one step (a node or a
 // leaf) per loop turn: inside the megakernel, the nested node/leaf loops of
 // traceAdvance measured 3.4x slower.
-template <typename Stack>
+//
+// HOLD keeps the node table's address in registers for the whole query. Read
+// through `s` at every node step instead, it comes from wherever the caller
+// keeps the scene (local memory, for a caller of the out-of-line copy) and is
+// reloaded after every stack push, a store the compiler cannot tell apart from
+// it: one more dependent load in front of every node fetch. Holding it measured
+// 2.8% faster in the megakernel (128 registers a thread) and 3-4% slower in the
+// wavefront's persistent kernels, whose 96-register budget then spills.
+template <bool HOLD, typename Stack>
 __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
                                                const SkipRule& skip, TraceHit& hit, Stack* stack, int stride,
                                                int stack_size, unsigned int* error_flag, TraversalCounts* counts,
@@ -732,11 +740,12 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
     if (counts != nullptr) {
         counts->reference_boxes += 1; // the TLAS root
     }
+    const DevNode* const held_nodes = s.nodes;
     for (;;) {
         q.settle();
-        const int step = (q.ref & kLeafBit) == 0u ? nodeStep(s, q, stack, stride, stack_size, error_flag, counts)
-                                                  : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts,
-                                                             any);
+        const int step = (q.ref & kLeafBit) == 0u
+                             ? nodeStep(HOLD ? held_nodes : s.nodes, q, stack, stride, stack_size, error_flag, counts)
+                             : leafStep(s, q, skip, stack, stride, stack_size, error_flag, counts, any);
         if (step == kStepFinished || (step == kStepPop && !popNext(q, stack, stride))) {
             break;
         }
@@ -752,13 +761,13 @@ __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin,
 // keeps the kernels that call it small enough for the instruction cache. COUNT
 // selects the copy that counts work (the counting kernels); the timed kernels'
 // copy has no counting code at all.
-template <bool COUNT, typename Stack>
+template <bool COUNT, bool HOLD, typename Stack>
 static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float3 origin, float3 dir, float tmin,
                                                         float& tmax, const SkipRule& skip, TraceHit& hit,
                                                         Stack* stack, int stride, int stack_size,
                                                         unsigned int* error_flag, TraversalCounts* counts, bool any)
 {
-    return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+    return traceSceneBody<HOLD>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
                           COUNT ? counts : nullptr, any);
 }
 
@@ -774,11 +783,11 @@ ALB_DEV bool traceQuery(const DevScene& s, float3 origin, float3 dir, float tmin
                         TraversalCounts* counts, bool any)
 {
     if constexpr (INLINE) {
-        return traceSceneBody(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
-                              COUNT ? counts : nullptr, any);
+        return traceSceneBody<true>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
+                                    COUNT ? counts : nullptr, any);
     } else {
-        return traceSceneOutOfLine<COUNT>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size,
-                                          error_flag, counts, any);
+        return traceSceneOutOfLine<COUNT, true>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size,
+                                                error_flag, counts, any);
     }
 }
 

@@ -292,7 +292,9 @@ void WavefrontEngine::render(const std::vector<WfJob>& jobs, int stack, unsigned
         }
         std::stable_sort(order.begin(), order.end(), [&](std::size_t a, std::size_t b) {
             const auto work = [&](const WfJob& j) {
-                return static_cast<long long>(j.samples_per_axis) * j.samples_per_axis * (j.max_depth + 1);
+                // In 64 bits: max_depth may be near INT_MAX.
+                return static_cast<long long>(j.samples_per_axis) * j.samples_per_axis *
+                       (static_cast<long long>(j.max_depth) + 1);
             };
             return work(jobs[a]) > work(jobs[b]);
         });
