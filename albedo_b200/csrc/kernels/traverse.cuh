@@ -722,7 +722,7 @@ __device__ __forceinline__ bool traceAdvance(const DevScene& s, TraceState& q, c
 // keeps the scene (local memory, for a caller of the out-of-line copy) and is
 // reloaded after every stack push, a store the compiler cannot tell apart from
 // it: one more dependent load in front of every node fetch. Holding it measured
-// 2.8% faster in the megakernel (128 registers a thread) and 3-4% slower in the
+// 2.7% faster in the megakernel (128 registers a thread) and 3-4% slower in the
 // wavefront's persistent kernels, whose 96-register budget then spills.
 template <bool HOLD, typename Stack>
 __device__ __forceinline__ bool traceSceneBody(const DevScene& s, float3 origin, float3 dir, float tmin, float& tmax,
@@ -768,7 +768,7 @@ static __device__ __noinline__ bool traceSceneOutOfLine(const DevScene& s, float
                                                         unsigned int* error_flag, TraversalCounts* counts, bool any)
 {
     return traceSceneBody<HOLD>(s, origin, dir, tmin, tmax, skip, hit, stack, stride, stack_size, error_flag,
-                          COUNT ? counts : nullptr, any);
+                                COUNT ? counts : nullptr, any);
 }
 
 // A query from a caller that keeps its state across the call (the megakernel),
