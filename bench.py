@@ -309,11 +309,16 @@ def run_reference(args, rank: int) -> None:
         total_s = sum(s["seconds"] for s in samples)
         value = total_paths / total_s / 1e6
         base = samples[-1]
+        cfg = config(LARGE, "reference CPU renderer (renderImage)", 1)
+        # The same frame and scene; each timed step renders it at 16 spp (Mpaths/s
+        # hardly depends on the sample count), which these fields state.
+        cfg["timed_samples_per_axis"] = REFERENCE_SAMPLES_PER_AXIS
+        cfg["timed_paths_per_step"] = LARGE.width * LARGE.height * REFERENCE_SAMPLES_PER_AXIS ** 2
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s * 1e3 / len(samples),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded scene files in the reference's formats)",
-                "config": config(LARGE, "reference CPU renderer (renderImage)", 1),
+                "config": cfg,
                 "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": base["cores"], "kind": "reference",
                                  "sample": "each step: " + base["sample"]},
                 "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
