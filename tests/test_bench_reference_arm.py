@@ -8,17 +8,19 @@ import json
 import os
 import subprocess
 import sys
+from pathlib import Path
 
 import pytest
 
-from conftest import ROOT
 from oracle import reference as ref
+
+BENCH = Path(__file__).resolve().parent.parent / "bench.py"
 
 pytestmark = pytest.mark.skipif(not ref.REF_LIBRARY.exists(), reason="reference library not built")
 
 
 def run_bench(*args, env=None):
-    return subprocess.run([sys.executable, str(ROOT / "bench.py"), *args], capture_output=True, text=True,
+    return subprocess.run([sys.executable, str(BENCH), *args], capture_output=True, text=True,
                           timeout=600, env={**os.environ, **(env or {})})
 
 
